@@ -1,0 +1,78 @@
+"""ctypes binding of ``libdamask_b200.so`` (the C-ABI declared in ``include/damask_b200.h``).
+
+The product path has no fallback: if the library cannot be loaded, every entry
+point raises.  The library is built in-tree by :mod:`damask_b200.build`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from pathlib import Path
+
+from .config import BCStruct, NumericsStruct, PhaseStruct, SolutionStruct
+
+LIB_PATH = Path(__file__).resolve().parent / 'libdamask_b200.so'
+
+EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materialpoint_forward',
+           'dmk_mech_update_coords', 'dmk_get_field', 'dmk_set_field', 'dmk_field_size', 'dmk_get_aims',
+           'dmk_constitutive_response', 'dmk_update_gamma', 'dmk_gamma_convolution', 'dmk_divergence_rms',
+           'dmk_dPdF', 'dmk_get_iteration_counts', 'dmk_get_counters', 'dmk_get_timings', 'dmk_destroy',
+           'dmk_last_error']
+
+_lib = None
+
+dp = C.POINTER(C.c_double)
+ip = C.POINTER(C.c_int)
+
+
+class DamaskError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f'{msg} (code {code})')
+        self.code = code
+
+
+def load(path: str | os.PathLike | None = None) -> C.CDLL:
+    """Load the CUDA library (once)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = Path(path) if path else LIB_PATH
+    if not p.exists():
+        raise RuntimeError(f'{p} is missing: build it with "python -m damask_b200.build" (no CPU fallback exists)')
+    lib = C.CDLL(str(p))
+    vp = C.c_void_p
+    sig = {
+        'dmk_mech_init': (C.c_int, [C.POINTER(vp), ip, dp, ip, C.c_int, dp, C.POINTER(PhaseStruct),
+                                    C.POINTER(NumericsStruct), C.c_int, C.c_int]),
+        'dmk_mech_forward': (C.c_int, [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                                       C.POINTER(BCStruct), C.POINTER(BCStruct), dp]),
+        'dmk_mech_solution': (C.c_int, [vp, C.POINTER(SolutionStruct)]),
+        'dmk_materialpoint_forward': (C.c_int, [vp]),
+        'dmk_mech_update_coords': (C.c_int, [vp]),
+        'dmk_get_field': (C.c_int, [vp, C.c_int, dp]),
+        'dmk_set_field': (C.c_int, [vp, C.c_int, dp]),
+        'dmk_field_size': (C.c_int, [vp, C.c_int]),
+        'dmk_get_aims': (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
+        'dmk_constitutive_response': (C.c_int, [vp, dp, C.c_double, dp, dp, dp, dp, ip]),
+        'dmk_update_gamma': (C.c_int, [vp, dp]),
+        'dmk_gamma_convolution': (C.c_int, [vp, dp, dp]),
+        'dmk_divergence_rms': (C.c_int, [vp, dp, dp]),
+        'dmk_dPdF': (C.c_int, [vp, C.c_double, dp]),
+        'dmk_get_iteration_counts': (C.c_int, [vp, ip]),
+        'dmk_get_counters': (C.c_int, [vp, C.POINTER(C.c_int64)]),
+        'dmk_get_timings': (C.c_int, [vp, dp]),
+        'dmk_destroy': (None, [vp]),
+        'dmk_last_error': (C.c_char_p, []),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = _lib.dmk_last_error().decode() if _lib is not None else 'library not loaded'
+        raise DamaskError(rc, msg or 'constitutive failure')

@@ -1,0 +1,873 @@
+// Host side of the damask_b200 C-ABI: context (device-resident per-voxel state,
+// cuFFT plans, solver scalars) and the grid_mechanical_spectral_basic_* entry points.
+#include "../../include/damask_b200.h"
+#include "kernels.cuh"
+#include "lattice.h"
+
+#include <cufft.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+using namespace dmk;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+
+#define CK(x)                                                                              \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return fail(DMK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+#define CKF(x)                                                                             \
+  do {                                                                                     \
+    cufftResult r_ = (x);                                                                  \
+    if (r_ != CUFFT_SUCCESS) return fail(DMK_ERR_CUFFT, std::string(#x) + " failed: " + std::to_string(int(r_))); \
+  } while (0)
+
+template <typename T>
+int dalloc(T** p, size_t n) {
+  cudaError_t e = cudaMalloc(reinterpret_cast<void**>(p), n * sizeof(T) + 256);
+  if (e != cudaSuccess) return fail(DMK_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+  return 0;
+}
+
+}  // namespace
+
+struct dmk_ctx {
+  int device = 0;
+  int nsm = 148;
+  int cells[3];
+  double geom[3];
+  int64_t N = 0;
+  double wgt = 0.0;
+  int NS = 0;
+  int precision = DMK_PRECISION_FP64;
+  dmk_numerics num;
+  HostPhase hp;
+  PhaseConst<12>* pc12 = nullptr;
+  PhaseConst<18>* pc18 = nullptr;
+  PhaseConst<24>* pc24 = nullptr;
+  Numerics nm;
+  Numerics2 nm2;
+  GammaConst gc;
+  cudaStream_t stream = nullptr;
+
+  // device fields (planes)
+  double *Fsol = nullptr, *r = nullptr, *F = nullptr, *F0 = nullptr, *Fp = nullptr, *Fp0 = nullptr, *Lp = nullptr,
+         *Lp0 = nullptr, *S = nullptr, *S0 = nullptr, *Fe = nullptr, *P = nullptr, *Pnew = nullptr, *Flast = nullptr,
+         *Fdot = nullptr, *state = nullptr, *state0 = nullptr;
+  double* spec = nullptr;       // FP64 spectrum (9 planes of complex)
+  float* specf = nullptr;       // FP32 spectrum (mixed)
+  float* Pf = nullptr;          // FP32 stress / residual planes (mixed)
+  double* partials = nullptr;   // constitutive / forward partial sums
+  double* sums = nullptr;
+  double* div_partials = nullptr;
+  int* status = nullptr;
+  int* iter = nullptr;
+  unsigned long long* counters = nullptr;
+  SolverScalars* sc = nullptr;
+  double* scratch = nullptr;    // host <-> device staging, grown on demand
+  size_t scratch_len = 0;
+  TangentOut tan{};
+  double* tan_out = nullptr;    // 243 doubles
+  long long* tan_idx = nullptr;
+  int tan_blocks = 0;
+  void* fft_work = nullptr;
+  cufftHandle plan_fwd = 0, plan_bwd = 0, plan_fwd_f = 0, plan_bwd_f = 0;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+  // host copy of the solver module state (grid_mech_spectral_basic.f90:30-45)
+  double F_aim[9], F_aim_lastinc[9], F_aimDot[9], P_aim[9], P_av[9];
+  double C_volAvg[81], C_volAvgLastInc[81], C_minMaxAvg[81], C_minMaxAvgLastInc[81], Scomp[81];
+  int stress_mask[9];
+  double q_rot[4];
+  double dt = 0.0;
+  int64_t last_counters[4] = {0, 0, 0, 0};
+  double last_ms[3] = {0, 0, 0};
+  bool iter_enabled = false;
+};
+
+namespace {
+
+Fields make_fields(dmk_ctx* c, const double* r) {
+  Fields f;
+  f.N = c->N;
+  f.Fsol = c->Fsol; f.r = r; f.F = c->F; f.F0 = c->F0; f.Fp = c->Fp; f.Fp0 = c->Fp0; f.Lp = c->Lp; f.Lp0 = c->Lp0;
+  f.S = c->S; f.S0 = c->S0; f.Fe = c->Fe; f.P = c->Pnew; f.state = c->state; f.state0 = c->state0;
+  f.partials = c->partials; f.status = c->status; f.iter = c->iter_enabled ? c->iter : nullptr;
+  f.counters = c->counters;
+  return f;
+}
+
+cudaError_t run_constitutive(dmk_ctx* c, const Fields& f, double dt, int apply) {
+  switch (c->NS) {
+    case 12: return launch_constitutive<12>(*c->pc12, c->nm, f, dt, apply, c->stream);
+    case 18: return launch_constitutive<18>(*c->pc18, c->nm, f, dt, apply, c->stream);
+    case 24: return launch_constitutive<24>(*c->pc24, c->nm, f, dt, apply, c->stream);
+  }
+  return cudaErrorInvalidValue;
+}
+cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o) {
+  switch (c->NS) {
+    case 12: return launch_dPdF<12>(*c->pc12, f, dt, o, 0, c->N, c->stream);
+    case 18: return launch_dPdF<18>(*c->pc18, f, dt, o, 0, c->N, c->stream);
+    case 24: return launch_dPdF<24>(*c->pc24, f, dt, o, 0, c->N, c->stream);
+  }
+  return cudaErrorInvalidValue;
+}
+cudaError_t run_pick(dmk_ctx* c, const Fields& f, double dt) {
+  switch (c->NS) {
+    case 12: return launch_tangent_pick<12>(*c->pc12, f, dt, c->tan_idx, c->tan_out, c->stream);
+    case 18: return launch_tangent_pick<18>(*c->pc18, f, dt, c->tan_idx, c->tan_out, c->stream);
+    case 24: return launch_tangent_pick<24>(*c->pc24, f, dt, c->tan_idx, c->tan_out, c->stream);
+  }
+  return cudaErrorInvalidValue;
+}
+
+int nblocks_const(const dmk_ctx* c) { return int((c->N + CONST_THREADS - 1) / CONST_THREADS); }
+
+template <int NS>
+void fill_phase_const(const HostPhase& hp, PhaseConst<NS>& pc) {
+  std::memcpy(pc.C66, hp.C66, sizeof pc.C66);
+  std::memcpy(pc.C, hp.C, sizeof pc.C);
+  for (int s = 0; s < NS; ++s) {
+    for (int k = 0; k < 9; ++k) {
+      pc.P[s][k] = hp.P[s][k];
+      pc.PnS[0][s][k] = hp.Ppos[s][k];
+      pc.PnS[1][s][k] = hp.Pneg[s][k];
+    }
+    for (int sense = 0; sense < 2; ++sense) {
+      const double* Pn = sense == 0 ? hp.Ppos[s].data() : hp.Pneg[s].data();
+      // tau = S : P_nS with S symmetric -> weights on (11,22,33,23,13,12)
+      double* p = pc.p6[sense][s];
+      p[0] = Pn[0]; p[1] = Pn[4]; p[2] = Pn[8];
+      p[3] = Pn[7] + Pn[5]; p[4] = Pn[6] + Pn[2]; p[5] = Pn[3] + Pn[1];
+      // Q(t,r) = sum_mn P_nS(m,n) C(m,n,t,r)
+      double Q[9];
+      for (int t = 0; t < 3; ++t)
+        for (int r = 0; r < 3; ++r) {
+          double acc = 0.0;
+          for (int n = 0; n < 3; ++n)
+            for (int m = 0; m < 3; ++m) acc += Pn[m + 3 * n] * hp.C[m + 3 * n + 9 * t + 27 * r];
+          Q[t + 3 * r] = acc;
+        }
+      double* q = pc.q6[sense][s];
+      q[0] = Q[0]; q[1] = Q[4]; q[2] = Q[8]; q[3] = 0.5 * (Q[7] + Q[5]); q[4] = 0.5 * (Q[6] + Q[2]); q[5] = 0.5 * (Q[3] + Q[1]);
+    }
+    pc.dg0[s] = hp.dg0[s];
+    pc.n[s] = hp.n[s];
+    pc.a[s] = hp.a[s];
+    pc.h0f[s] = hp.h0f[s];
+    pc.xiinf[s] = hp.xiinf[s];
+    pc.n_int[s] = (hp.n[s] == std::floor(hp.n[s]) && hp.n[s] >= 1.0 && hp.n[s] <= 64.0) ? int(hp.n[s]) : -1;
+    pc.a_int[s] = (hp.a[s] == std::floor(hp.a[s]) && hp.a[s] >= 0.0 && hp.a[s] <= 64.0) ? int(hp.a[s]) : -1;
+    for (int k = 0; k < NS; ++k) pc.h[s][k] = hp.h[s * NS + k];
+  }
+  pc.atol_xi = hp.atol_xi;
+  pc.atol_gamma = hp.atol_gamma;
+}
+
+// host rotations (rotations.f90:282-339, P = -1)
+void h_rotvec(const double* v, const double* q, double* o) {
+  const double A = q[0] * q[0] - (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  const double B = 2.0 * (q[1] * v[0] + q[2] * v[1] + q[3] * v[2]);
+  const double C = -2.0 * q[0];
+  const double cx = q[2] * v[2] - q[3] * v[1], cy = q[3] * v[0] - q[1] * v[2], cz = q[1] * v[1] - q[2] * v[0];
+  o[0] = A * v[0] + B * q[1] + C * cx;
+  o[1] = A * v[1] + B * q[2] + C * cy;
+  o[2] = A * v[2] + B * q[3] + C * cz;
+}
+void h_rot33(const double* qin, const double* T, double* R, bool active) {
+  const double q[4] = {qin[0], active ? -qin[1] : qin[1], active ? -qin[2] : qin[2], active ? -qin[3] : qin[3]};
+  double tmp[9];
+  for (int i = 0; i < 3; ++i) {
+    const double v[3] = {T[i], T[i + 3], T[i + 6]};
+    double o[3];
+    h_rotvec(v, q, o);
+    tmp[i] = o[0]; tmp[i + 3] = o[1]; tmp[i + 6] = o[2];
+  }
+  for (int j = 0; j < 3; ++j) {
+    const double v[3] = {tmp[3 * j], tmp[3 * j + 1], tmp[3 * j + 2]};
+    double o[3];
+    h_rotvec(v, q, o);
+    R[3 * j] = o[0]; R[3 * j + 1] = o[1]; R[3 * j + 2] = o[2];
+  }
+}
+void h_rot3333(const double* q, const double* T, double* R) {
+  std::memcpy(R, T, 81 * sizeof(double));
+  auto at = [&](int i, int j, int k, int l) -> double& { return R[i + 3 * j + 9 * k + 27 * l]; };
+  double v[3], o[3];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) {
+    for (int l = 0; l < 3; ++l) v[l] = at(i, j, k, l);
+    h_rotvec(v, q, o); for (int l = 0; l < 3; ++l) at(i, j, k, l) = o[l];
+  }
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int l = 0; l < 3; ++l) {
+    for (int k = 0; k < 3; ++k) v[k] = at(i, j, k, l);
+    h_rotvec(v, q, o); for (int k = 0; k < 3; ++k) at(i, j, k, l) = o[k];
+  }
+  for (int i = 0; i < 3; ++i) for (int k = 0; k < 3; ++k) for (int l = 0; l < 3; ++l) {
+    for (int j = 0; j < 3; ++j) v[j] = at(i, j, k, l);
+    h_rotvec(v, q, o); for (int j = 0; j < 3; ++j) at(i, j, k, l) = o[j];
+  }
+  for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) for (int l = 0; l < 3; ++l) {
+    for (int i = 0; i < 3; ++i) v[i] = at(i, j, k, l);
+    h_rotvec(v, q, o); for (int i = 0; i < 3; ++i) at(i, j, k, l) = o[i];
+  }
+}
+
+// utilities_maskedCompliance, grid_utilities.f90:74-127
+int masked_compliance(const double* q, const int* mask9 /* column-major, 1 = 'x' */, const double* C, double* S) {
+  bool sv[9];
+  int nred = 0;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) { sv[3 * i + j] = !mask9[i + 3 * j]; nred += sv[3 * i + j]; }
+  double t99[81];
+  std::fill(t99, t99 + 81, 0.0);
+  if (nred > 0) {
+    double Cr[81], M[81];
+    h_rot3333(q, C, Cr);
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) for (int l = 0; l < 3; ++l)
+      M[(3 * i + j) * 9 + 3 * k + l] = Cr[i + 3 * j + 9 * k + 27 * l];
+    std::vector<int> idx;
+    for (int i = 0; i < 9; ++i) if (sv[i]) idx.push_back(i);
+    std::vector<double> cr(nred * nred), sr(nred * nred);
+    for (int a = 0; a < nred; ++a) for (int b = 0; b < nred; ++b) cr[a * nred + b] = M[idx[a] * 9 + idx[b]];
+    if (invert_dense(cr.data(), sr.data(), nred)) return fail(DMK_ERR_STATE, "masked compliance: singular reduced stiffness");
+    // C * S == I check (grid_utilities.f90:106-118)
+    for (int a = 0; a < nred; ++a) for (int b = 0; b < nred; ++b) {
+      double s = 0.0;
+      for (int k = 0; k < nred; ++k) s += cr[a * nred + k] * sr[k * nred + b];
+      if (std::fabs(s - (a == b ? 1.0 : 0.0)) > 1.0e-12 || std::isnan(s))
+        return fail(DMK_ERR_STATE, "masked compliance: matrix inversion error");
+    }
+    for (int a = 0; a < nred; ++a) for (int b = 0; b < nred; ++b) t99[idx[a] * 9 + idx[b]] = sr[a * nred + b];
+  }
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) for (int l = 0; l < 3; ++l)
+    S[i + 3 * j + 9 * k + 27 * l] = t99[(3 * i + j) * 9 + 3 * k + l];
+  return 0;
+}
+
+int upload_scalars(dmk_ctx* c, bool reset_iter) {
+  SolverScalars h;
+  std::memset(&h, 0, sizeof h);
+  std::memcpy(h.F_aim, c->F_aim, sizeof h.F_aim);
+  std::memcpy(h.P_aim, c->P_aim, sizeof h.P_aim);
+  std::memcpy(h.P_av, c->P_av, sizeof h.P_av);
+  std::memcpy(h.Scomp, c->Scomp, sizeof h.Scomp);
+  std::memcpy(h.q_rot, c->q_rot, sizeof h.q_rot);
+  std::memcpy(h.stress_mask, c->stress_mask, sizeof h.stress_mask);
+  h.totalIter = reset_iter ? -1 : 0;
+  CK(cudaMemcpyAsync(c->sc, &h, sizeof h, cudaMemcpyHostToDevice, c->stream));
+  return 0;
+}
+
+// spectral_utilities_init scaledGeomSize (spectral_utilities.f90:181-197)
+void scaled_geom(const int* n, const double* g, int mode, double* out) {
+  const double sp[3] = {g[0] / n[0], g[1] / n[1], g[2] / n[2]};
+  auto argmin = [](const double* v) { int k = 0; for (int i = 1; i < 3; ++i) if (v[i] < v[k]) k = i; return k; };
+  auto argmax = [](const double* v) { int k = 0; for (int i = 1; i < 3; ++i) if (v[i] > v[k]) k = i; return k; };
+  for (int i = 0; i < 3; ++i) out[i] = g[i];
+  if (mode == 2) {
+    for (int j = 0; j < 3; ++j) if (j != argmin(sp) && j != argmax(sp)) for (int i = 0; i < 3; ++i) out[i] = g[i] / g[j] * double(n[j]);
+  } else if (mode == 0) {
+    for (int j = 0; j < 3; ++j) if (j != argmin(g) && j != argmax(g)) for (int i = 0; i < 3; ++i) out[i] = g[i] / g[j];
+  }
+}
+
+int make_plans(dmk_ctx* c) {
+  int n[3] = {c->cells[2], c->cells[1], c->cells[0]};
+  const int red0 = c->cells[0] / 2 + 1;
+  int inemb[3] = {c->cells[2], c->cells[1], c->cells[0]};
+  int onemb[3] = {c->cells[2], c->cells[1], red0};
+  const long long plane = (long long)red0 * c->cells[1] * c->cells[2];
+  size_t w1 = 0, w2 = 0, w3 = 0, w4 = 0;
+  CKF(cufftCreate(&c->plan_fwd));
+  CKF(cufftCreate(&c->plan_bwd));
+  CKF(cufftSetAutoAllocation(c->plan_fwd, 0));
+  CKF(cufftSetAutoAllocation(c->plan_bwd, 0));
+  CKF(cufftMakePlanMany(c->plan_fwd, 3, n, inemb, 1, int(c->N), onemb, 1, int(plane), CUFFT_D2Z, 9, &w1));
+  CKF(cufftMakePlanMany(c->plan_bwd, 3, n, onemb, 1, int(plane), inemb, 1, int(c->N), CUFFT_Z2D, 9, &w2));
+  if (c->precision == DMK_PRECISION_MIXED) {
+    CKF(cufftCreate(&c->plan_fwd_f));
+    CKF(cufftCreate(&c->plan_bwd_f));
+    CKF(cufftSetAutoAllocation(c->plan_fwd_f, 0));
+    CKF(cufftSetAutoAllocation(c->plan_bwd_f, 0));
+    CKF(cufftMakePlanMany(c->plan_fwd_f, 3, n, inemb, 1, int(c->N), onemb, 1, int(plane), CUFFT_R2C, 9, &w3));
+    CKF(cufftMakePlanMany(c->plan_bwd_f, 3, n, onemb, 1, int(plane), inemb, 1, int(c->N), CUFFT_C2R, 9, &w4));
+  }
+  const size_t w = std::max(std::max(w1, w2), std::max(w3, w4));
+  if (w) CK(cudaMalloc(&c->fft_work, w));
+  CKF(cufftSetWorkArea(c->plan_fwd, c->fft_work));
+  CKF(cufftSetWorkArea(c->plan_bwd, c->fft_work));
+  CKF(cufftSetStream(c->plan_fwd, c->stream));
+  CKF(cufftSetStream(c->plan_bwd, c->stream));
+  if (c->precision == DMK_PRECISION_MIXED) {
+    CKF(cufftSetWorkArea(c->plan_fwd_f, c->fft_work));
+    CKF(cufftSetWorkArea(c->plan_bwd_f, c->fft_work));
+    CKF(cufftSetStream(c->plan_fwd_f, c->stream));
+    CKF(cufftSetStream(c->plan_bwd_f, c->stream));
+  }
+  return 0;
+}
+
+// One constitutive sweep + commit of P (homogenization_mechanical_response + the P part of
+// utilities_constitutiveResponse).  On a failed sweep the previous P field is kept (the
+// reference skips mechanical_homogenize when any cell fails, homogenization.f90:343).
+int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int* status_out) {
+  CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+  Fields f = make_fields(c, r);
+  CK(cudaEventRecord(c->ev[0], c->stream));
+  CK(run_constitutive(c, f, dt, apply));
+  CK(cudaEventRecord(c->ev[1], c->stream));
+  int st = 0;
+  CK(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  c->last_ms[0] += ms;
+  if (st == 0) std::swap(c->P, c->Pnew);
+  else CK(launch_sum9(c->P, c->N, c->partials, c->stream));
+  *status_out = st;
+  return 0;
+}
+
+// dP/dF of every voxel from the stored state: C_volAvg and C_minMaxAvg (grid_utilities.f90:171-202)
+int ensure_scratch(dmk_ctx* c, int K);
+
+int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
+  Fields f = make_fields(c, nullptr);
+  TangentOut o = c->tan;
+  o.per_voxel = per_voxel_dev;
+  CK(run_dPdF(c, f, dt, o));
+  CK(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
+  CK(run_pick(c, f, dt));
+  double h[243];
+  CK(cudaMemcpyAsync(h, c->tan_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < 81; ++k) {
+    c->C_volAvg[k] = h[k];
+    c->C_minMaxAvg[k] = 0.5 * (h[81 + k] + h[162 + k]);
+  }
+  return 0;
+}
+
+void update_gamma_host(dmk_ctx* c, const double* C) {
+  for (int k = 0; k < 81; ++k) c->gc.Cref[k] = C[k] / c->wgt;
+}
+
+// D2Z of the committed P, fused divergence + Gamma, Z2D into r (FP64 or FP32 spectral path)
+int spectral_pass(dmk_ctx* c, bool fp32, int do_gamma, int do_div, void* out) {
+  const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
+  if (!fp32) {
+    CKF(cufftExecD2Z(c->plan_fwd, c->P, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
+    CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, do_gamma,
+                                do_div, c->stream));
+    if (do_gamma) CKF(cufftExecZ2D(c->plan_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), static_cast<double*>(out)));
+  } else {
+    CK(launch_to_float(c->P, c->Pf, 9 * c->N, c->nsm, c->stream));
+    CKF(cufftExecR2C(c->plan_fwd_f, c->Pf, reinterpret_cast<cufftComplex*>(c->specf)));
+    CK(launch_gamma_div<float>(c->specf, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, do_gamma,
+                               do_div, c->stream));
+    if (do_gamma) CKF(cufftExecC2R(c->plan_bwd_f, reinterpret_cast<cufftComplex*>(c->specf), static_cast<float*>(out)));
+  }
+  return 0;
+}
+
+int ensure_scratch(dmk_ctx* c, int K) {
+  const size_t need = size_t(K) * size_t(c->N);
+  if (need <= c->scratch_len) return 0;
+  if (c->scratch) { cudaStreamSynchronize(c->stream); cudaFree(c->scratch); c->scratch = nullptr; c->scratch_len = 0; }
+  int rc = dalloc(&c->scratch, need);
+  if (rc) return rc;
+  c->scratch_len = need;
+  return 0;
+}
+
+int h2d_planes(dmk_ctx* c, const double* host, double* dev_planes, int K) {
+  if (int rc = ensure_scratch(c, K)) return rc;
+  CK(cudaMemcpyAsync(c->scratch, host, sizeof(double) * K * c->N, cudaMemcpyHostToDevice, c->stream));
+  CK(launch_to_planes(c->scratch, dev_planes, c->N, K, c->stream));
+  return 0;
+}
+int d2h_planes(dmk_ctx* c, const double* dev_planes, double* host, int K) {
+  if (int rc = ensure_scratch(c, K)) return rc;
+  CK(launch_from_planes(dev_planes, c->scratch, c->N, K, c->stream));
+  CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * K * c->N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int response(dmk_ctx* c, double dt, int* status) {
+  int st = 0;
+  int rc = evaluate_constitutive(c, dt, nullptr, 0, &st);
+  if (rc) return rc;
+  CK(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 0, c->stream));
+  double pav[9];
+  CK(cudaMemcpyAsync(pav, reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, P_av), sizeof pav,
+                     cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  std::memcpy(c->P_av, pav, sizeof pav);
+  if (st == 0) {
+    rc = evaluate_tangent(c, dt, nullptr);
+    if (rc) return rc;
+  }
+  *status = st;
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* dmk_last_error(void) { return g_err.c_str(); }
+
+int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], const int* materialAt, int n_materials,
+                  const double* quaternions, const dmk_phase* phase, const dmk_numerics* num, int precision, int device) {
+  if (!out || !cells || !geomSize || !materialAt || !quaternions || !phase || !num) return fail(DMK_ERR_ARG, "null argument");
+  *out = nullptr;
+  for (int i = 0; i < 3; ++i)
+    if (cells[i] < 1 || !(geomSize[i] > 0.0)) return fail(DMK_ERR_ARG, "cells and geomSize must be positive");
+  if (precision != DMK_PRECISION_FP64 && precision != DMK_PRECISION_MIXED) return fail(DMK_ERR_ARG, "unknown precision");
+  if (num->derivative != 0) return fail(DMK_ERR_CONFIG, "only the continuous spectral derivative is on this path");
+  if (num->N_iter_max < 1 || num->N_iter_min < 1 || num->N_iter_min > num->N_iter_max)
+    return fail(DMK_ERR_CONFIG, "invalid N_iter_min/N_iter_max");
+  if (num->N_iter_Lp_max < 1 || num->N_iter_state_max < 1 || num->f_update_jacobi_Lp < 1 || !(num->r_cutback > 0.0) ||
+      !(num->r_cutback_min > 0.0) || !(num->r_increase > 0.0) || !(num->r_linesearch_Lp > 0.0))
+    return fail(DMK_ERR_CONFIG, "invalid phase.mechanical numerics");
+  dmk_ctx* c = new dmk_ctx();
+  int rc = build_host_phase(*phase, c->hp, g_err);
+  if (rc) { delete c; return DMK_ERR_CONFIG; }
+  c->NS = c->hp.Ns;
+  if (c->NS != 12 && c->NS != 18 && c->NS != 24) {
+    delete c;
+    return fail(DMK_ERR_CONFIG, "number of active slip systems must be 12, 18 or 24 on this path");
+  }
+  c->device = device;
+  c->precision = precision;
+  c->num = *num;
+  for (int i = 0; i < 3; ++i) { c->cells[i] = cells[i]; c->geom[i] = geomSize[i]; }
+  c->N = int64_t(cells[0]) * cells[1] * cells[2];
+  c->wgt = 1.0 / double(c->N);
+  const int64_t N = c->N;
+  for (int64_t v = 0; v < N; ++v)
+    if (materialAt[v] < 0 || materialAt[v] >= n_materials) { delete c; return fail(DMK_ERR_ARG, "material index out of range"); }
+
+  auto bail = [&](int code) { dmk_destroy(c); return code; };
+  if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(DMK_ERR_CUDA, "cudaSetDevice failed"); }
+  cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
+  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return fail(DMK_ERR_CUDA, "stream"); }
+  for (auto& e : c->ev) cudaEventCreate(&e);
+
+  c->nm.r_cutback_min = num->r_cutback_min; c->nm.r_cutback = num->r_cutback; c->nm.r_increase = num->r_increase;
+  c->nm.eps_rel_state = num->eps_rel_state; c->nm.N_iter_state_max = num->N_iter_state_max;
+  c->nm.N_iter_Lp_max = num->N_iter_Lp_max; c->nm.r_linesearch_Lp = num->r_linesearch_Lp;
+  c->nm.eps_rel_Lp = num->eps_rel_Lp; c->nm.eps_abs_Lp = num->eps_abs_Lp; c->nm.f_update_jacobi_Lp = num->f_update_jacobi_Lp;
+  c->nm2.N_iter_min = num->N_iter_min; c->nm2.N_iter_max = num->N_iter_max; c->nm2.cells0 = cells[0];
+  c->nm2.eps_abs_div = num->eps_abs_div; c->nm2.eps_rel_div = num->eps_rel_div;
+  c->nm2.eps_abs_P = num->eps_abs_P; c->nm2.eps_rel_P = num->eps_rel_P;
+  double sgs[3];
+  scaled_geom(cells, geomSize, num->divergence_correction, sgs);
+  for (int i = 0; i < 3; ++i) c->gc.rescale[i] = geomSize[i] / sgs[i];
+
+  switch (c->NS) {
+    case 12: c->pc12 = new PhaseConst<12>(); fill_phase_const<12>(c->hp, *c->pc12); break;
+    case 18: c->pc18 = new PhaseConst<18>(); fill_phase_const<18>(c->hp, *c->pc18); break;
+    case 24: c->pc24 = new PhaseConst<24>(); fill_phase_const<24>(c->hp, *c->pc24); break;
+  }
+
+  const int NST = 2 * c->NS;
+  const int64_t plane = int64_t(cells[0] / 2 + 1) * cells[1] * cells[2];
+  if ((rc = dalloc(&c->Fsol, 9 * N)) || (rc = dalloc(&c->r, 9 * N)) || (rc = dalloc(&c->F, 9 * N)) ||
+      (rc = dalloc(&c->F0, 9 * N)) || (rc = dalloc(&c->Fp, 9 * N)) || (rc = dalloc(&c->Fp0, 9 * N)) ||
+      (rc = dalloc(&c->Lp, 9 * N)) || (rc = dalloc(&c->Lp0, 9 * N)) || (rc = dalloc(&c->S, 6 * N)) ||
+      (rc = dalloc(&c->S0, 6 * N)) || (rc = dalloc(&c->Fe, 9 * N)) || (rc = dalloc(&c->P, 9 * N)) ||
+      (rc = dalloc(&c->Pnew, 9 * N)) || (rc = dalloc(&c->Flast, 9 * N)) || (rc = dalloc(&c->Fdot, 9 * N)) ||
+      (rc = dalloc(&c->state, NST * N)) || (rc = dalloc(&c->state0, NST * N)) ||
+      (rc = dalloc(&c->spec, 2 * 9 * plane)) ||
+      (rc = dalloc(&c->partials, 9 * (size_t)nblocks_const(c))) || (rc = dalloc(&c->sums, 16)) ||
+      (rc = dalloc(&c->div_partials, (size_t)gamma_div_blocks(cells[0], cells[1], cells[2]))) ||
+      (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
+      (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)))
+    return bail(rc);
+  if (precision == DMK_PRECISION_MIXED)
+    if ((rc = dalloc(&c->specf, 2 * 9 * plane)) || (rc = dalloc(&c->Pf, 9 * N))) return bail(rc);
+  c->tan_blocks = dPdF_blocks(N);
+  if ((rc = dalloc(&c->tan.partials, 81 * (size_t)c->tan_blocks)) || (rc = dalloc(&c->tan.nmax, c->tan_blocks)) ||
+      (rc = dalloc(&c->tan.nmin, c->tan_blocks)) || (rc = dalloc(&c->tan.norms, N)))
+    return bail(rc);
+  if ((rc = make_plans(c))) return bail(rc);
+
+  // mechanical_init (phase_mechanical.f90:249-266), computed per voxel on the device
+  {
+    int* dmat = nullptr;
+    double *dq = nullptr, *dxi = nullptr;
+    if ((rc = dalloc(&dmat, N)) || (rc = dalloc(&dq, 4 * size_t(n_materials))) || (rc = dalloc(&dxi, c->NS))) {
+      cudaFree(dmat); cudaFree(dq); cudaFree(dxi);
+      return bail(rc);
+    }
+    cudaError_t e = cudaMemcpyAsync(dmat, materialAt, sizeof(int) * N, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dq, quaternions, sizeof(double) * 4 * n_materials, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dxi, c->hp.xi0.data(), sizeof(double) * c->NS, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess)
+      e = launch_init_state(dmat, dq, dxi, c->NS, N, c->F, c->F0, c->Fsol, c->Flast, c->Fp, c->Fp0, c->Fe, c->state,
+                            c->state0, c->stream);
+    for (double* p : {c->Lp, c->Lp0, c->P, c->Pnew, c->Fdot, c->r})
+      if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * 9 * N, c->stream);
+    for (double* p : {c->S, c->S0})
+      if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * 6 * N, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    cudaFree(dmat); cudaFree(dq); cudaFree(dxi);
+    if (e != cudaSuccess) return bail(fail(DMK_ERR_CUDA, std::string("init: ") + cudaGetErrorString(e)));
+  }
+  // solver module state (grid_mech_spectral_basic.f90:30-45)
+  for (int k = 0; k < 9; ++k) {
+    c->F_aim[k] = c->F_aim_lastinc[k] = (k % 4 == 0) ? 1.0 : 0.0;
+    c->F_aimDot[k] = c->P_aim[k] = c->P_av[k] = 0.0;
+    c->stress_mask[k] = 1;
+  }
+  std::fill(c->C_volAvg, c->C_volAvg + 81, 0.0);
+  std::fill(c->C_volAvgLastInc, c->C_volAvgLastInc + 81, 0.0);
+  std::fill(c->C_minMaxAvg, c->C_minMaxAvg + 81, 0.0);
+  std::fill(c->C_minMaxAvgLastInc, c->C_minMaxAvgLastInc + 81, 0.0);
+  std::fill(c->Scomp, c->Scomp + 81, 0.0);
+  c->q_rot[0] = 1.0; c->q_rot[1] = c->q_rot[2] = c->q_rot[3] = 0.0;
+  if ((rc = upload_scalars(c, true))) return bail(rc);
+
+  // grid_mechanical_spectral_basic_init: constitutive response at F = I, dt = 0, then updateGamma
+  int st = 0;
+  if ((rc = response(c, 0.0, &st))) return bail(rc);
+  update_gamma_host(c, c->C_minMaxAvg);
+  *out = c;
+  return 0;
+}
+
+int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_old, double t_remaining,
+                     const dmk_bc* def, const dmk_bc* stress, const double q_rot[4]) {
+  if (!c || !def || !stress || !q_rot) return fail(DMK_ERR_ARG, "null argument");
+  if (cutBack) {
+    std::memcpy(c->C_volAvg, c->C_volAvgLastInc, sizeof c->C_volAvg);
+    std::memcpy(c->C_minMaxAvg, c->C_minMaxAvgLastInc, sizeof c->C_minMaxAvg);
+  } else {
+    std::memcpy(c->C_volAvgLastInc, c->C_volAvg, sizeof c->C_volAvg);
+    std::memcpy(c->C_minMaxAvgLastInc, c->C_minMaxAvg, sizeof c->C_minMaxAvg);
+    for (int k = 0; k < 9; ++k)
+      c->F_aimDot[k] = guess ? (stress->mask[k] ? 0.0 : (c->F_aim[k] - c->F_aim_lastinc[k]) / dt_old) : 0.0;
+    std::memcpy(c->F_aim_lastinc, c->F_aim, sizeof c->F_aim);
+    double m[9];
+    for (int k = 0; k < 9; ++k) m[k] = def->mask[k] ? 0.0 : def->values[k];
+    if (def->type == 1) {                      // L: F_aimDot += L F_aim_lastinc
+      for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) {
+          double s = 0.0;
+          for (int k = 0; k < 3; ++k) s += m[i + 3 * k] * c->F_aim_lastinc[k + 3 * j];
+          c->F_aimDot[i + 3 * j] += s;
+        }
+    } else if (def->type == 2) {               // dot_F
+      for (int k = 0; k < 9; ++k) c->F_aimDot[k] += m[k];
+    } else if (def->type == 3) {               // F at end of load case
+      for (int k = 0; k < 9; ++k)
+        c->F_aimDot[k] += def->mask[k] ? 0.0 : (def->values[k] - c->F_aim_lastinc[k]) / t_remaining;
+    } else {
+      return fail(DMK_ERR_ARG, "deformation BC type must be L, dot_F or F");
+    }
+  }
+  double avRate[9], aim[9];
+  h_rot33(q_rot, c->F_aimDot, avRate, true);
+  for (int k = 0; k < 9; ++k) c->F_aim[k] = c->F_aim_lastinc[k] + c->F_aimDot[k] * dt;
+  if (stress->type == 4)
+    for (int k = 0; k < 9; ++k) c->P_aim[k] = c->P_aim[k] + (stress->mask[k] ? 0.0 : (stress->values[k] - c->P_aim[k]) / t_remaining) * dt;
+  if (stress->type == 5)
+    for (int k = 0; k < 9; ++k) c->P_aim[k] = c->P_aim[k] + (stress->mask[k] ? 0.0 : stress->values[k]) * dt;
+  h_rot33(q_rot, c->F_aim, aim, true);
+  for (int k = 0; k < 9; ++k) c->stress_mask[k] = stress->mask[k] ? 1 : 0;
+  std::memcpy(c->q_rot, q_rot, sizeof c->q_rot);
+  c->dt = dt;
+  int rc = upload_scalars(c, true);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, avRate), avRate, sizeof avRate,
+                     cudaMemcpyHostToDevice, c->stream));
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_fwd), aim, sizeof aim,
+                     cudaMemcpyHostToDevice, c->stream));
+  const double* dsc = reinterpret_cast<const double*>(c->sc);
+  CK(launch_forward(c->Fsol, c->Flast, c->Fdot, c->N, cutBack, guess, dt, dt_old,
+                    dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->partials, c->sums, c->wgt,
+                    dsc + offsetof(SolverScalars, aim_fwd) / sizeof(double), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
+  if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
+  int rc = masked_compliance(c->q_rot, c->stress_mask, c->C_volAvg, c->Scomp);
+  if (rc) return rc;
+  if (c->num.update_gamma) update_gamma_host(c, c->C_minMaxAvg);
+  if ((rc = upload_scalars(c, true))) return rc;
+  CK(cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream));
+  c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
+  const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
+  const bool mixed = c->precision == DMK_PRECISION_MIXED;
+  bool fp32 = mixed;
+  int evals = 0, reason = 0, apply = 0;
+  const void* rprev = nullptr;
+  SolverScalars hs;
+  const int nspec = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
+  for (int it = 0;; ++it) {
+    int st = 0;
+    if ((rc = evaluate_constitutive(c, c->dt, static_cast<const double*>(rprev), apply, &st))) return rc;
+    ++evals;
+    CK(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 1, c->stream));
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    if ((rc = spectral_pass(c, fp32, 1, 1, fp32 ? static_cast<void*>(c->Pf) : static_cast<void*>(c->r)))) return rc;
+    CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, 1, c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    CK(cudaMemcpyAsync(&hs, c->sc, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+    c->last_ms[1] += ms;
+    reason = hs.reason;
+    if (fp32 && reason == 1) {
+      // The FP32 spectral residual meets the tolerance: correction sweep in FP64 on the
+      // same stress field (no new constitutive evaluation); its residual decides.
+      fp32 = false;
+      CK(cudaEventRecord(c->ev[2], c->stream));
+      if ((rc = spectral_pass(c, false, 1, 1, c->r))) return rc;
+      CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, 0, c->stream));
+      CK(cudaEventRecord(c->ev[3], c->stream));
+      CK(cudaMemcpyAsync(&hs, c->sc, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+      c->last_ms[1] += ms;
+      reason = hs.reason;
+    } else if (fp32) {
+      CK(launch_to_double(c->Pf, c->r, 9 * c->N, c->nsm, c->stream));
+    }
+    if (reason != 0) break;
+    if (it + 1 > snes_max_its) { reason = -1; break; }
+    rprev = c->r;   // F <- F - r is fused into the next constitutive sweep
+    apply = 1;
+  }
+  std::memcpy(c->F_aim, hs.F_aim, sizeof c->F_aim);
+  std::memcpy(c->P_av, hs.P_av, sizeof c->P_av);
+  out->converged = reason > 0;
+  out->iterationsNeeded = hs.totalIter;
+  out->stagConverged = 1;
+  out->residualEvals = evals;
+  out->err_div = hs.err_div;
+  out->err_BC = hs.err_BC;
+  std::memcpy(out->P_av, hs.P_av, sizeof out->P_av);
+  for (int k = 0; k < 9; ++k)
+    if (c->stress_mask[k]) c->P_aim[k] = c->P_av[k];
+  if (out->converged) {
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    if ((rc = evaluate_tangent(c, c->dt, nullptr))) return rc;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    c->last_ms[2] += ms;
+  }
+  unsigned long long hc[4];
+  CK(cudaMemcpyAsync(hc, c->counters, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_counters[0] = int64_t(evals) * c->N;
+  c->last_counters[1] = int64_t(hc[1]);
+  c->last_counters[2] = int64_t(hc[2]);
+  c->last_counters[3] = evals;
+  return 0;
+}
+
+int dmk_materialpoint_forward(dmk_ctx* c) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  const size_t b9 = sizeof(double) * 9 * c->N, b6 = sizeof(double) * 6 * c->N, bs = sizeof(double) * 2 * c->NS * c->N;
+  CK(cudaMemcpyAsync(c->F0, c->F, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->Fp0, c->Fp, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->Lp0, c->Lp, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->S0, c->S, b6, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->state0, c->state, bs, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_mech_update_coords(dmk_ctx* c) { return c ? 0 : fail(DMK_ERR_ARG, "null argument"); }
+
+int dmk_field_size(dmk_ctx* c, int field) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (field == DMK_FIELD_XI_SL || field == DMK_FIELD_GAMMA_SL) return c->NS;
+  if (field >= 0 && field <= DMK_FIELD_F_SOLVER) return 9;
+  return fail(DMK_ERR_ARG, "unknown field");
+}
+
+int dmk_get_field(dmk_ctx* c, int field, double* host) {
+  if (!c || !host) return fail(DMK_ERR_ARG, "null argument");
+  const int64_t N = c->N;
+  switch (field) {
+    case DMK_FIELD_F: return d2h_planes(c, c->F, host, 9);
+    case DMK_FIELD_P: return d2h_planes(c, c->P, host, 9);
+    case DMK_FIELD_FE: return d2h_planes(c, c->Fe, host, 9);
+    case DMK_FIELD_FP: return d2h_planes(c, c->Fp, host, 9);
+    case DMK_FIELD_LP: return d2h_planes(c, c->Lp, host, 9);
+    case DMK_FIELD_F_LASTINC: return d2h_planes(c, c->Flast, host, 9);
+    case DMK_FIELD_F_SOLVER: return d2h_planes(c, c->Fsol, host, 9);
+    case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NS);
+    case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NS);
+    case DMK_FIELD_S:
+      CK(launch_sym6_to9(c->S, c->scratch, N, c->stream));
+      CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      return 0;
+    case DMK_FIELD_FI:
+    case DMK_FIELD_LI:
+      for (int64_t v = 0; v < N; ++v)
+        for (int k = 0; k < 9; ++k) host[v * 9 + k] = (field == DMK_FIELD_FI && k % 4 == 0) ? 1.0 : 0.0;
+      return 0;
+  }
+  return fail(DMK_ERR_ARG, "unknown field");
+}
+
+int dmk_set_field(dmk_ctx* c, int field, const double* host) {
+  if (!c || !host) return fail(DMK_ERR_ARG, "null argument");
+  int rc = 0;
+  switch (field) {
+    case DMK_FIELD_F_SOLVER: rc = h2d_planes(c, host, c->Fsol, 9); break;
+    case DMK_FIELD_F_LASTINC: rc = h2d_planes(c, host, c->Flast, 9); break;
+    default: return fail(DMK_ERR_ARG, "field is not settable");
+  }
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_get_aims(dmk_ctx* c, double F_aim[9], double F_aim_lastinc[9], double F_aimDot[9], double P_aim[9],
+                 double C_volAvg[81], double C_volAvgLastInc[81], double C_minMaxAvg[81]) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (F_aim) std::memcpy(F_aim, c->F_aim, 9 * sizeof(double));
+  if (F_aim_lastinc) std::memcpy(F_aim_lastinc, c->F_aim_lastinc, 9 * sizeof(double));
+  if (F_aimDot) std::memcpy(F_aimDot, c->F_aimDot, 9 * sizeof(double));
+  if (P_aim) std::memcpy(P_aim, c->P_aim, 9 * sizeof(double));
+  if (C_volAvg) std::memcpy(C_volAvg, c->C_volAvg, 81 * sizeof(double));
+  if (C_volAvgLastInc) std::memcpy(C_volAvgLastInc, c->C_volAvgLastInc, 81 * sizeof(double));
+  if (C_minMaxAvg) std::memcpy(C_minMaxAvg, c->C_minMaxAvg, 81 * sizeof(double));
+  return 0;
+}
+
+int dmk_constitutive_response(dmk_ctx* c, const double* F, double dt, double* P, double P_av[9], double C_volAvg[81],
+                              double C_minMaxAvg[81], int* status) {
+  if (!c || !F || !P || !status) return fail(DMK_ERR_ARG, "null argument");
+  int rc = h2d_planes(c, F, c->Fsol, 9);
+  if (rc) return rc;
+  const double q0[4] = {1.0, 0.0, 0.0, 0.0};
+  std::memcpy(c->q_rot, q0, sizeof q0);
+  if ((rc = upload_scalars(c, true))) return rc;
+  c->iter_enabled = true;
+  rc = response(c, dt, status);
+  c->iter_enabled = false;
+  if (rc) return rc;
+  if ((rc = d2h_planes(c, c->P, P, 9))) return rc;
+  if (P_av) std::memcpy(P_av, c->P_av, 9 * sizeof(double));
+  if (C_volAvg) std::memcpy(C_volAvg, c->C_volAvg, 81 * sizeof(double));
+  if (C_minMaxAvg) std::memcpy(C_minMaxAvg, c->C_minMaxAvg, 81 * sizeof(double));
+  return 0;
+}
+
+int dmk_update_gamma(dmk_ctx* c, const double C[81]) {
+  if (!c || !C) return fail(DMK_ERR_ARG, "null argument");
+  update_gamma_host(c, C);
+  return 0;
+}
+
+int dmk_gamma_convolution(dmk_ctx* c, double* field, const double aim[9]) {
+  if (!c || !field || !aim) return fail(DMK_ERR_ARG, "null argument");
+  int rc = h2d_planes(c, field, c->P, 9);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_rot), aim, 9 * sizeof(double),
+                     cudaMemcpyHostToDevice, c->stream));
+  if ((rc = spectral_pass(c, false, 1, 0, c->r))) return rc;
+  return d2h_planes(c, c->r, field, 9);
+}
+
+int dmk_divergence_rms(dmk_ctx* c, const double* P, double* out) {
+  if (!c || !P || !out) return fail(DMK_ERR_ARG, "null argument");
+  int rc = h2d_planes(c, P, c->P, 9);
+  if (rc) return rc;
+  if ((rc = spectral_pass(c, false, 0, 1, nullptr))) return rc;
+  const int nb = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
+  std::vector<double> h(nb);
+  CK(cudaMemcpyAsync(h.data(), c->div_partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (double x : h) s += x;
+  double r = std::sqrt(s) * c->wgt;
+  if (c->cells[0] == 1) r *= 0.5;
+  *out = r;
+  return 0;
+}
+
+int dmk_dPdF(dmk_ctx* c, double dt, double* dPdF) {
+  if (!c || !dPdF) return fail(DMK_ERR_ARG, "null argument");
+  int rc = ensure_scratch(c, 81);
+  if (rc) return rc;
+  rc = evaluate_tangent(c, dt, c->scratch);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(dPdF, c->scratch, sizeof(double) * 81 * c->N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_get_iteration_counts(dmk_ctx* c, int* out) {
+  if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
+  std::vector<int> h(4 * c->N);
+  CK(cudaMemcpyAsync(h.data(), c->iter, sizeof(int) * 4 * c->N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int64_t v = 0; v < c->N; ++v)
+    for (int k = 0; k < 4; ++k) out[v * 4 + k] = h[k * c->N + v];
+  return 0;
+}
+
+int dmk_get_counters(dmk_ctx* c, int64_t out[4]) {
+  if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
+  for (int k = 0; k < 4; ++k) out[k] = c->last_counters[k];
+  return 0;
+}
+
+int dmk_get_timings(dmk_ctx* c, double out[3]) {
+  if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
+  for (int k = 0; k < 3; ++k) out[k] = c->last_ms[k];
+  return 0;
+}
+
+void dmk_destroy(dmk_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  for (cufftHandle p : {c->plan_fwd, c->plan_bwd, c->plan_fwd_f, c->plan_bwd_f})
+    if (p) cufftDestroy(p);
+  for (void* p : {(void*)c->Fsol, (void*)c->r, (void*)c->F, (void*)c->F0, (void*)c->Fp, (void*)c->Fp0, (void*)c->Lp,
+                  (void*)c->Lp0, (void*)c->S, (void*)c->S0, (void*)c->Fe, (void*)c->P, (void*)c->Pnew, (void*)c->Flast,
+                  (void*)c->Fdot, (void*)c->state, (void*)c->state0, (void*)c->spec, (void*)c->specf, (void*)c->Pf,
+                  (void*)c->partials, (void*)c->sums, (void*)c->div_partials, (void*)c->status, (void*)c->iter,
+                  (void*)c->counters, (void*)c->sc, (void*)c->scratch, (void*)c->tan_out, (void*)c->tan_idx,
+                  (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work})
+    if (p) cudaFree(p);
+  for (auto e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->stream) cudaStreamDestroy(c->stream);
+  delete c->pc12;
+  delete c->pc18;
+  delete c->pc24;
+  delete c;
+}
+
+}  // extern "C"

@@ -1,0 +1,534 @@
+// CUDA kernels of the damask_b200 hot path (sm_100a).
+//
+//  constitutive_kernel  one thread per voxel: fused Richardson field update
+//                       F <- F - r, phase restore, substep cutback, FPI state
+//                       integration, Lp Newton, P; per-block partial sums of P.
+//  gamma_div_kernel     one thread per Fourier point: divergence-RMS partial sums
+//                       and the Gamma-operator application (closed form) with the
+//                       DC term set to the aim, in one pass over the spectrum.
+//  dPdF_kernel          consistent tangent per voxel with fused volume average and
+//                       min/max Frobenius-norm selection.
+//  small kernels        aim/BC update, convergence test, layout transposes.
+#include "kernels.cuh"
+#include "constitutive.cuh"
+
+#include <cfloat>
+
+namespace dmk {
+
+// ------------------------------------------------------------------ constitutive
+template <int NS>
+__global__ void __launch_bounds__(CONST_THREADS)
+constitutive_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
+                    const __grid_constant__ Fields f, double dt, int apply_update) {
+  __shared__ double red[9 * (CONST_THREADS / 32)];
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t N = f.N;
+  double Psum[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  int status = 0, nstate = 0, newton = 0, nsub = 0;
+  if (v < N) {
+    double Fn[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double x = f.Fsol[k * N + v];
+      if (apply_update) {
+        x = x - f.r[k * N + v];
+        f.Fsol[k * N + v] = x;
+      }
+      Fn[k] = x;
+      f.F[k * N + v] = x;
+    }
+    status = constitutive_point<NS>(pc, nm, f, v, Fn, dt, nstate, newton, nsub);
+    if (status == 0) {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Psum[k] = f.P[k * N + v];
+    } else {
+      atomicMax(f.status, 2);                     // STATUS_FAIL_PHASE_MECHANICAL
+    }
+    if (f.iter) {
+      f.iter[v] = nstate;
+      f.iter[N + v] = newton;
+      f.iter[2 * N + v] = nsub;
+      f.iter[3 * N + v] = status;
+    }
+  }
+  // iteration counters (warp aggregated)
+  unsigned long long cs = nstate, cn = newton;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cs += __shfl_down_sync(0xffffffffu, cs, o);
+    cn += __shfl_down_sync(0xffffffffu, cn, o);
+  }
+  if ((threadIdx.x & 31) == 0 && f.counters) {
+    atomicAdd(&f.counters[1], cs);
+    atomicAdd(&f.counters[2], cn);
+  }
+  block_reduce_sum<9>(Psum, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) f.partials[int64_t(blockIdx.x) * 9 + k] = Psum[k];
+}
+
+template <int NS>
+cudaError_t launch_constitutive(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, double dt,
+                                int apply_update, cudaStream_t s) {
+  const int nb = int((f.N + CONST_THREADS - 1) / CONST_THREADS);
+  constitutive_kernel<NS><<<nb, CONST_THREADS, 0, s>>>(pc, nm, f, dt, apply_update);
+  return cudaGetLastError();
+}
+template cudaError_t launch_constitutive<12>(const PhaseConst<12>&, const Numerics&, const Fields&, double, int, cudaStream_t);
+template cudaError_t launch_constitutive<18>(const PhaseConst<18>&, const Numerics&, const Fields&, double, int, cudaStream_t);
+template cudaError_t launch_constitutive<24>(const PhaseConst<24>&, const Numerics&, const Fields&, double, int, cudaStream_t);
+
+// partial sums of a 9-plane field (used when the stale P field is kept after a failure)
+__global__ void __launch_bounds__(CONST_THREADS) sum9_kernel(const double* __restrict__ X, int64_t N, double* partials) {
+  __shared__ double red[9 * (CONST_THREADS / 32)];
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (v < N)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s[k] = X[k * N + v];
+  block_reduce_sum<9>(s, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) partials[int64_t(blockIdx.x) * 9 + k] = s[k];
+}
+cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s) {
+  const int nb = int((N + CONST_THREADS - 1) / CONST_THREADS);
+  sum9_kernel<<<nb, CONST_THREADS, 0, s>>>(X, N, partials);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ solver scalars
+__device__ void rotvec(const double* v, const double* q, double* o) {   // rotations.f90:776-791 (P = -1)
+  const double A = q[0] * q[0] - (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  const double B = 2.0 * (q[1] * v[0] + q[2] * v[1] + q[3] * v[2]);
+  const double C = -2.0 * q[0];
+  const double cx = q[2] * v[2] - q[3] * v[1], cy = q[3] * v[0] - q[1] * v[2], cz = q[1] * v[1] - q[2] * v[0];
+  o[0] = A * v[0] + B * q[1] + C * cx;
+  o[1] = A * v[1] + B * q[2] + C * cy;
+  o[2] = A * v[2] + B * q[3] + C * cz;
+}
+__device__ void rot33(const double* qin, const double* T, double* R, bool active) {   // rotations.f90:282-303
+  const double q[4] = {qin[0], active ? -qin[1] : qin[1], active ? -qin[2] : qin[2], active ? -qin[3] : qin[3]};
+  double tmp[9];
+  for (int i = 0; i < 3; ++i) {
+    const double v[3] = {T[i], T[i + 3], T[i + 6]};
+    double o[3];
+    rotvec(v, q, o);
+    tmp[i] = o[0]; tmp[i + 3] = o[1]; tmp[i + 6] = o[2];
+  }
+  for (int j = 0; j < 3; ++j) {
+    const double v[3] = {tmp[3 * j], tmp[3 * j + 1], tmp[3 * j + 2]};
+    double o[3];
+    rotvec(v, q, o);
+    R[3 * j] = o[0]; R[3 * j + 1] = o[1]; R[3 * j + 2] = o[2];
+  }
+}
+
+// After the constitutive sweep: P_av = <P> (rotated to the load frame),
+// deltaF_aim = S : (P_av - P_aim), F_aim -= deltaF_aim, err_BC, and the rotated
+// aim for the DC term of the Gamma convolution (form_residual, grid_mech_spectral_basic.f90:503-519).
+__global__ void aim_kernel(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim) {
+  __shared__ double acc[9][32];
+  const int t = threadIdx.x;
+  for (int k = 0; k < 9; ++k) {
+    double s = 0.0;
+    for (int b = t; b < nparts; b += 32) s += partials[int64_t(b) * 9 + k];
+    acc[k][t] = s;
+  }
+  __syncwarp();
+  if (t != 0) return;
+  double Pav[9];
+  for (int k = 0; k < 9; ++k) {
+    double s = 0.0;
+    for (int w = 0; w < 32; ++w) s += acc[k][w];
+    Pav[k] = s * wgt;
+  }
+  double R[9];
+  rot33(sc->q_rot, Pav, R, false);
+  for (int k = 0; k < 9; ++k) sc->P_av[k] = R[k];
+  if (!update_aim) return;
+  double d[9], dF[9];
+  for (int k = 0; k < 9; ++k) d[k] = sc->P_av[k] - sc->P_aim[k];
+  // math_mul3333xx33(S, d): dF(i,j) = sum_kl S(i,j,k,l) d(k,l)
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) {
+      double s = 0.0;
+      for (int l = 0; l < 3; ++l)
+        for (int k = 0; k < 3; ++k) s += sc->Scomp[i + 3 * j + 9 * k + 27 * l] * d[k + 3 * l];
+      dF[i + 3 * j] = s;
+    }
+  double e = 0.0;
+  for (int k = 0; k < 9; ++k) {
+    sc->F_aim[k] -= dF[k];
+    if (!sc->stress_mask[k]) e = fmax(e, fabs(d[k]));
+  }
+  sc->err_BC = e;
+  rot33(sc->q_rot, dF, sc->aim_rot, true);
+}
+
+// converged(), grid_mech_spectral_basic.f90:422-458, plus the SNES bookkeeping of the
+// Richardson iteration.  reason: 0 iterating, 1 converged, -1 diverged.
+__global__ void converge_kernel(SolverScalars* sc, const double* div_partials, int nparts, double wgt,
+                                const int* status, const Numerics2 nm2, int count_iteration) {
+  __shared__ double acc[32];
+  const int t = threadIdx.x;
+  double s = 0.0;
+  for (int b = t; b < nparts; b += 32) s += div_partials[b];
+  acc[t] = s;
+  __syncwarp();
+  if (t != 0) return;
+  double tot = 0.0;
+  for (int w = 0; w < 32; ++w) tot += acc[w];
+  double err_div = sqrt(tot) * wgt;
+  if (nm2.cells0 == 1) err_div *= 0.5;
+  sc->err_div = err_div;
+  sc->totalIter += count_iteration;
+  double pmax = 0.0;
+  for (int k = 0; k < 9; ++k) pmax = fmax(pmax, fabs(sc->P_av[k]));
+  const double divTol = fmax(pmax * nm2.eps_rel_div, nm2.eps_abs_div);
+  const double BCTol = fmax(pmax * nm2.eps_rel_P, nm2.eps_abs_P);
+  int reason = 0;
+  if (sc->totalIter >= nm2.N_iter_min && err_div / divTol < 1.0 && sc->err_BC / BCTol < 1.0 && *status == 0)
+    reason = 1;
+  else if (sc->totalIter >= nm2.N_iter_max)
+    reason = -1;
+  if (!isfinite(err_div)) reason = -1;
+  sc->status = *status;
+  sc->reason = reason;
+}
+
+cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s) {
+  aim_kernel<<<1, 32, 0, s>>>(sc, partials, nparts, wgt, update_aim);
+  return cudaGetLastError();
+}
+cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int nparts, double wgt, const int* status,
+                            const Numerics2& nm2, int count_iteration, cudaStream_t s) {
+  converge_kernel<<<1, 32, 0, s>>>(sc, div_partials, nparts, wgt, status, nm2, count_iteration);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ spectral
+// One thread per stored Fourier point (kx in [0, n0/2], ky, kz).  The spectrum of
+// component c is stored as plane c: [kz][ky][kx] with kx fastest (cuFFT D2Z layout).
+//
+// Gamma (spectral_utilities.f90:436-501, continuous derivative xi = i a, a = 2 pi k / L):
+// xiDyad = conj(-xi) (x) xi = -a a^T is real, the 6x6 real embedding of
+// A = C_ref : xiDyad is block diagonal with Re A = -K, K(l,m) = sum_jk C_ref(l,j,m,k) a_j a_k,
+// so Gamma_hat : P_hat = K^-1 (P_hat a) (x) a.  Points with |det Re A| <= 1e-16 (k = 0
+// and the even-grid Nyquist corner where all a_i vanish) are set to zero; k = 0 then
+// receives the aim.
+template <typename Real>
+__global__ void __launch_bounds__(SPEC_THREADS)
+gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                 const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
+                 double* __restrict__ div_partials, int do_gamma, int do_div) {
+  __shared__ double red[SPEC_THREADS / 32];
+  using C2 = typename std::conditional<sizeof(Real) == 8, double2, float2>::type;
+  C2* S = reinterpret_cast<C2*>(spec);
+  const int red0 = n0 / 2 + 1;
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double dsum = 0.0;
+  if (idx < plane) {
+    const int kx = int(idx % red0);
+    const int64_t rest = idx / red0;
+    const int ky = int(rest % n1);
+    const int kz = int(rest / n1);
+    const int sy = ky > n1 / 2 ? ky - n1 : ky;
+    const int sz = kz > n2 / 2 ? kz - n2 : kz;
+    const double TAU = 6.283185307179586;
+    double a[3];
+    a[0] = (n0 % 2 == 0 && kx == n0 / 2) ? 0.0 : TAU * double(kx) / L0;
+    a[1] = (n1 % 2 == 0 && ky == n1 / 2) ? 0.0 : TAU * double(sy) / L1;
+    a[2] = (n2 % 2 == 0 && kz == n2 / 2) ? 0.0 : TAU * double(sz) / L2;
+    double pr[9], pi[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const C2 z = S[c * plane + idx];
+      pr[c] = double(z.x);
+      pi[c] = double(z.y);
+    }
+    if (do_div) {
+      // |P_hat . conj(-xi) * rescale|^2, conj(-xi) = i a
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        double vr = 0.0, vi = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          const double w = a[m] * gc.rescale[m];
+          // (pr + i pi) * (i w) = -pi w + i pr w
+          vr = fma(-pi[l + 3 * m], w, vr);
+          vi = fma(pr[l + 3 * m], w, vi);
+        }
+        s = fma(vr, vr, s);
+        s = fma(vi, vi, s);
+      }
+      const double weight = (kx >= 1 && kx < red0 - 1) ? 2.0 : 1.0;
+      dsum = weight * s;
+    }
+    if (do_gamma) {
+      double rr[9], ri[9];
+      if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) { rr[c] = sc->aim_rot[c]; ri[c] = 0.0; }
+      } else {
+        // K(l,m) = sum_jk Cref(l,j,m,k) a_j a_k (symmetric)
+        double aa[9];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) aa[j + 3 * k] = a[j] * a[k];
+        double K[9];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            double s = 0.0;
+#pragma unroll
+            for (int k = 0; k < 3; ++k)
+#pragma unroll
+              for (int j = 0; j < 3; ++j) s = fma(gc.Cref[l + 3 * j + 9 * m + 27 * k], aa[j + 3 * k], s);
+            K[l + 3 * m] = s;
+          }
+        // det of Re A = -K
+        const double detK = det33(K);
+        if (fabs(detK) > 1.0e-16) {
+          double Ki[9];
+          Ki[0] = K[4] * K[8] - K[7] * K[5];
+          Ki[1] = -K[1] * K[8] + K[7] * K[2];
+          Ki[2] = K[1] * K[5] - K[4] * K[2];
+          Ki[3] = -K[3] * K[8] + K[6] * K[5];
+          Ki[4] = K[0] * K[8] - K[6] * K[2];
+          Ki[5] = -K[0] * K[5] + K[3] * K[2];
+          Ki[6] = K[3] * K[7] - K[6] * K[4];
+          Ki[7] = -K[0] * K[7] + K[6] * K[1];
+          Ki[8] = K[0] * K[4] - K[3] * K[1];
+          const double rdet = 1.0 / detK;
+          // v = P_hat a (complex 3-vector); u = K^-1 v
+          double vr[3], vi[3], ur[3], ui[3];
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            vr[l] = pr[l] * a[0] + pr[l + 3] * a[1] + pr[l + 6] * a[2];
+            vi[l] = pi[l] * a[0] + pi[l + 3] * a[1] + pi[l + 6] * a[2];
+          }
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            ur[l] = (Ki[l] * vr[0] + Ki[l + 3] * vr[1] + Ki[l + 6] * vr[2]) * rdet;
+            ui[l] = (Ki[l] * vi[0] + Ki[l + 3] * vi[1] + Ki[l + 6] * vi[2]) * rdet;
+          }
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) { rr[l + 3 * m] = ur[l] * a[m]; ri[l + 3 * m] = ui[l] * a[m]; }
+        } else {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) { rr[c] = 0.0; ri[c] = 0.0; }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        C2 z;
+        z.x = Real(rr[c]);
+        z.y = Real(ri[c]);
+        S[c * plane + idx] = z;
+      }
+    }
+  }
+  if (do_div) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < SPEC_THREADS / 32; ++w) s += red[w];
+      div_partials[blockIdx.x] = s;
+    }
+  }
+}
+
+template <typename Real>
+cudaError_t launch_gamma_div(Real* spec, int n0, int n1, int n2, const double L[3], const GammaConst& gc,
+                             const SolverScalars* sc, double* div_partials, int do_gamma, int do_div, cudaStream_t s) {
+  const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
+  const int nb = int((plane + SPEC_THREADS - 1) / SPEC_THREADS);
+  gamma_div_kernel<Real><<<nb, SPEC_THREADS, 0, s>>>(spec, plane, n0, n1, n2, L[0], L[1], L[2], gc, sc, div_partials,
+                                                     do_gamma, do_div);
+  return cudaGetLastError();
+}
+template cudaError_t launch_gamma_div<double>(double*, int, int, int, const double*, const GammaConst&, const SolverScalars*,
+                                              double*, int, int, cudaStream_t);
+template cudaError_t launch_gamma_div<float>(float*, int, int, int, const double*, const GammaConst&, const SolverScalars*,
+                                             double*, int, int, cudaStream_t);
+
+int gamma_div_blocks(int n0, int n1, int n2) {
+  const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
+  return int((plane + SPEC_THREADS - 1) / SPEC_THREADS);
+}
+
+// ------------------------------------------------------------------ field helpers
+// host layout [v][9] (Fortran (3,3,N)) <-> device planes [c][v]
+__global__ void to_planes_kernel(const double* __restrict__ in, double* __restrict__ out, int64_t N, int K) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  for (int k = 0; k < K; ++k) out[k * N + v] = in[v * K + k];
+}
+__global__ void from_planes_kernel(const double* __restrict__ in, double* __restrict__ out, int64_t N, int K) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  for (int k = 0; k < K; ++k) out[v * K + k] = in[k * N + v];
+}
+// symmetric 6 planes -> 9 column-major
+__global__ void sym6_to9_kernel(const double* __restrict__ in, double* __restrict__ out, int64_t N) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const double s[6] = {in[v], in[N + v], in[2 * N + v], in[3 * N + v], in[4 * N + v], in[5 * N + v]};
+  const double m[9] = {s[0], s[5], s[4], s[5], s[1], s[3], s[4], s[3], s[2]};
+  for (int k = 0; k < 9; ++k) out[v * 9 + k] = m[k];
+}
+cudaError_t launch_to_planes(const double* in, double* out, int64_t N, int K, cudaStream_t s) {
+  to_planes_kernel<<<int((N + 255) / 256), 256, 0, s>>>(in, out, N, K);
+  return cudaGetLastError();
+}
+cudaError_t launch_from_planes(const double* in, double* out, int64_t N, int K, cudaStream_t s) {
+  from_planes_kernel<<<int((N + 255) / 256), 256, 0, s>>>(in, out, N, K);
+  return cudaGetLastError();
+}
+cudaError_t launch_sym6_to9(const double* in, double* out, int64_t N, cudaStream_t s) {
+  sym6_to9_kernel<<<int((N + 255) / 256), 256, 0, s>>>(in, out, N);
+  return cudaGetLastError();
+}
+
+// forward of the solver field (grid_mech_spectral_basic.f90:312-346 with
+// utilities_calculateRate / utilities_forwardTensorField, grid_utilities.f90:245-297):
+// stage 1: Fdot (if not cut back), F_lastinc := F, F := F_lastinc + Fdot dt, partial sums of F
+__global__ void __launch_bounds__(CONST_THREADS)
+forward_kernel(double* __restrict__ Fsol, double* __restrict__ Flast, double* __restrict__ Fdot, int64_t N,
+               int cutBack, int guess, double dt, double dt_old, const double* __restrict__ avRate,
+               double* __restrict__ partials) {
+  __shared__ double red[9 * (CONST_THREADS / 32)];
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  if (v < N) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double fl = Flast[k * N + v], fd = Fdot[k * N + v];
+      if (!cutBack) {
+        const double f = Fsol[k * N + v];
+        fd = guess ? (f - fl) / dt_old : avRate[k];
+        fl = f;
+        Fdot[k * N + v] = fd;
+        Flast[k * N + v] = fl;
+      }
+      const double x = fl + fd * dt;
+      Fsol[k * N + v] = x;
+      s[k] = x;
+    }
+  }
+  block_reduce_sum<9>(s, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) partials[int64_t(blockIdx.x) * 9 + k] = s[k];
+}
+// reduce partials once (so that the shift kernel does not re-read them per block)
+__global__ void reduce_partials9_kernel(const double* partials, int nparts, double* out) {
+  const int k = threadIdx.x;
+  if (k >= 9) return;
+  double s = 0.0;
+  for (int b = 0; b < nparts; ++b) s += partials[int64_t(b) * 9 + k];
+  out[k] = s;
+}
+__global__ void shift2_kernel(double* __restrict__ Fsol, int64_t N, const double* __restrict__ sums, double wgt,
+                              const double* __restrict__ aim) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+#pragma unroll
+  for (int k = 0; k < 9; ++k) Fsol[k * N + v] -= sums[k] * wgt - aim[k];
+}
+// stage 2: F -= (<F> * wgt - aim)
+cudaError_t launch_forward(double* Fsol, double* Flast, double* Fdot, int64_t N, int cutBack, int guess, double dt,
+                           double dt_old, const double* avRate, double* partials, double* sums, double wgt,
+                           const double* aim, cudaStream_t s) {
+  const int nb = int((N + CONST_THREADS - 1) / CONST_THREADS);
+  forward_kernel<<<nb, CONST_THREADS, 0, s>>>(Fsol, Flast, Fdot, N, cutBack, guess, dt, dt_old, avRate, partials);
+  reduce_partials9_kernel<<<1, 32, 0, s>>>(partials, nb, sums);
+  shift2_kernel<<<int((N + 255) / 256), 256, 0, s>>>(Fsol, N, sums, wgt, aim);
+  return cudaGetLastError();
+}
+
+__global__ void copy_kernel(const double* __restrict__ a, double* __restrict__ b, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) b[i] = a[i];
+}
+__global__ void to_float_kernel(const double* __restrict__ a, float* __restrict__ b, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) b[i] = float(a[i]);
+}
+__global__ void to_double_kernel(const float* __restrict__ a, double* __restrict__ b, int64_t n) {
+  for (int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += int64_t(gridDim.x) * blockDim.x) b[i] = double(a[i]);
+}
+cudaError_t launch_copy(const double* a, double* b, int64_t n, int nsm, cudaStream_t s) {
+  copy_kernel<<<nsm * 8, 256, 0, s>>>(a, b, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s) {
+  to_float_kernel<<<nsm * 8, 256, 0, s>>>(a, b, n);
+  return cudaGetLastError();
+}
+cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s) {
+  to_double_kernel<<<nsm * 8, 256, 0, s>>>(a, b, n);
+  return cudaGetLastError();
+}
+
+}  // namespace dmk
+
+namespace dmk {
+
+// mechanical_init per voxel (phase_mechanical.f90:249-266) with V_e = I:
+// F = F0 = Fsol = F_lastinc = I, Fp = Fp0 = O%asMatrix() (qu2om, rotations.f90:399-423),
+// Fe = Fp^T, plastic state xi = xi_0, gamma = 0 (phenopowerlaw.f90:259-285).
+__global__ void init_state_kernel(const int* __restrict__ material, const double* __restrict__ quats,
+                                  const double* __restrict__ xi0, int NS, int64_t N, double* F, double* F0, double* Fsol,
+                                  double* Flast, double* Fp, double* Fp0, double* Fe, double* state, double* state0) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const double* q = quats + 4 * material[v];
+  const double qq = q[0] * q[0] - (q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  double m[9];   // om before the P = -1 transpose, column-major
+  m[0] = qq + 2.0 * q[1] * q[1];
+  m[4] = qq + 2.0 * q[2] * q[2];
+  m[8] = qq + 2.0 * q[3] * q[3];
+  m[3] = 2.0 * (q[1] * q[2] - q[0] * q[3]);
+  m[7] = 2.0 * (q[2] * q[3] - q[0] * q[1]);
+  m[2] = 2.0 * (q[3] * q[1] - q[0] * q[2]);
+  m[1] = 2.0 * (q[2] * q[1] + q[0] * q[3]);
+  m[5] = 2.0 * (q[3] * q[2] + q[0] * q[1]);
+  m[6] = 2.0 * (q[1] * q[3] + q[0] * q[2]);
+  double t[9];
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) t[i + 3 * j] = m[j + 3 * i];
+  const double c = cbrt(det33(t));
+  for (int k = 0; k < 9; ++k) {
+    const double fp = t[k] / c;
+    const double id = (k % 4 == 0) ? 1.0 : 0.0;
+    Fp[k * N + v] = fp;
+    Fp0[k * N + v] = fp;
+    F[k * N + v] = id; F0[k * N + v] = id; Fsol[k * N + v] = id; Flast[k * N + v] = id;
+  }
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j) Fe[(i + 3 * j) * N + v] = t[j + 3 * i] / c;
+  for (int s = 0; s < 2 * NS; ++s) {
+    const double x = s < NS ? xi0[s] : 0.0;
+    state[s * N + v] = x;
+    state0[s * N + v] = x;
+  }
+}
+cudaError_t launch_init_state(const int* material, const double* quats, const double* xi0, int NS, int64_t N, double* F,
+                              double* F0, double* Fsol, double* Flast, double* Fp, double* Fp0, double* Fe, double* state,
+                              double* state0, cudaStream_t s) {
+  init_state_kernel<<<int((N + 255) / 256), 256, 0, s>>>(material, quats, xi0, NS, N, F, F0, Fsol, Flast, Fp, Fp0, Fe,
+                                                         state, state0);
+  return cudaGetLastError();
+}
+
+}  // namespace dmk

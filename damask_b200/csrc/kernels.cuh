@@ -1,0 +1,81 @@
+// Kernel launch interface shared by the kernel and host translation units.
+#pragma once
+#include "dmk_device.cuh"
+
+namespace dmk {
+
+constexpr int CONST_THREADS = 128;   // constitutive block size (register-heavy FP64 threads)
+constexpr int SPEC_THREADS = 256;    // spectral pointwise kernels
+
+// Solver scalars living in device memory (grid_mech_spectral_basic.f90:30-45 module state
+// that the residual evaluation reads or updates).
+struct SolverScalars {
+  double F_aim[9];
+  double P_aim[9];
+  double P_av[9];
+  double Scomp[81];      // masked compliance S (grid_utilities.f90:74-127)
+  double q_rot[4];       // load-frame rotation
+  double aim_rot[9];     // rotation_BC%rotate(deltaF_aim, active) for the DC term
+  double avRate[9];      // forward: rotated F_aimDot
+  double aim_fwd[9];     // forward: rotated F_aim
+  int stress_mask[9];    // 1 = stress component not prescribed
+  double err_div, err_BC;
+  int totalIter;
+  int status;
+  int reason;
+};
+
+struct GammaConst {
+  double Cref[81];       // C_ref = C / wgt, column-major 3x3x3x3
+  double rescale[3];     // geomSize / scaledGeomSize
+};
+
+struct Numerics2 {
+  int N_iter_min, N_iter_max, cells0;
+  double eps_abs_div, eps_rel_div, eps_abs_P, eps_rel_P;
+};
+
+template <int NS>
+cudaError_t launch_constitutive(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, double dt,
+                                int apply_update, cudaStream_t s);
+cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s);
+cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s);
+cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int nparts, double wgt, const int* status,
+                            const Numerics2& nm2, int count_iteration, cudaStream_t s);
+template <typename Real>
+cudaError_t launch_gamma_div(Real* spec, int n0, int n1, int n2, const double L[3], const GammaConst& gc,
+                             const SolverScalars* sc, double* div_partials, int do_gamma, int do_div, cudaStream_t s);
+int gamma_div_blocks(int n0, int n1, int n2);
+cudaError_t launch_to_planes(const double* in, double* out, int64_t N, int K, cudaStream_t s);
+cudaError_t launch_from_planes(const double* in, double* out, int64_t N, int K, cudaStream_t s);
+cudaError_t launch_sym6_to9(const double* in, double* out, int64_t N, cudaStream_t s);
+cudaError_t launch_forward(double* Fsol, double* Flast, double* Fdot, int64_t N, int cutBack, int guess, double dt,
+                           double dt_old, const double* avRate, double* partials, double* sums, double wgt,
+                           const double* aim, cudaStream_t s);
+cudaError_t launch_init_state(const int* material, const double* quats, const double* xi0, int NS, int64_t N, double* F,
+                              double* F0, double* Fsol, double* Flast, double* Fp, double* Fp0, double* Fe, double* state,
+                              double* state0, cudaStream_t s);
+cudaError_t launch_copy(const double* a, double* b, int64_t n, int nsm, cudaStream_t s);
+cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s);
+cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
+
+// consistent tangent (dpdf.cu)
+struct TangentOut {
+  double* partials;      // per block: 81 sums of dPdF
+  double* nmax;          // per block: max Frobenius norm^2
+  double* nmin;
+  double* per_voxel;     // optional: 81 per voxel, voxel-major (Fortran layout)
+  double* norms;         // per voxel Frobenius norm^2
+};
+template <int NS>
+cudaError_t launch_dPdF(const PhaseConst<NS>& pc, const Fields& f, double dt, const TangentOut& o, int64_t first,
+                        int64_t count, cudaStream_t s);
+int dPdF_blocks(int64_t count);
+template <int NS>
+cudaError_t launch_tangent_pick(const PhaseConst<NS>& pc, const Fields& f, double dt, const long long* idx, double* out,
+                                cudaStream_t s);
+cudaError_t launch_tangent_finalize(const TangentOut& o, int nparts, double wgt,
+                                    double* out /* 81 vol, 81 max, 81 min, max/min norm */, long long* idx /* 2 */,
+                                    int64_t first, int64_t count, cudaStream_t s);
+
+}  // namespace dmk

@@ -1,0 +1,187 @@
+/*
+ * damask_b200 — C-ABI of the B200 (sm_100a) implementation of DAMASK's grid
+ * mechanical hot path: the basic spectral (FFT) fixed-point scheme with the
+ * Gamma-operator convolution, driving the per-voxel phenopowerlaw/Hooke
+ * constitutive update (FPI state integration, Lp Newton-Raphson, dP/dF).
+ *
+ * The entry points mirror the Fortran procedures the reference selects through
+ * procedure pointers in src/grid/DAMASK_grid.f90:110-119,171-206, so a
+ * Fortran host can bind them with ISO_C_BINDING.
+ *
+ * Conventions
+ *  - Plain C types only; all arrays are host pointers owned by the caller and
+ *    used only for the duration of the call.  Device memory (per-voxel state,
+ *    cuFFT plans, scratch) is owned by the context from init to destroy.
+ *  - 3x3 tensors are column-major (Fortran order: T11 T21 T31 T12 ...); fields
+ *    are voxel-major with x fastest, i.e. reshape(F,[3,3,cells1,cells2,cells3]).
+ *    4th-order tensors are column-major 3x3x3x3 (81 doubles).
+ *  - Every function returns a status: 0 on success, DMK_STATUS_* (mirroring
+ *    src/constants.f90:29-44) for constitutive failures, DMK_ERR_* otherwise.
+ *    Nothing is thrown across the ABI.
+ *  - A context is not re-entrant; call it from one host thread.
+ */
+#ifndef DAMASK_B200_H
+#define DAMASK_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes (constants.f90:29-44) */
+#define DMK_STATUS_OK 0
+#define DMK_STATUS_ITERATING 1
+#define DMK_STATUS_FAIL_PHASE_MECHANICAL 2
+#define DMK_STATUS_FAIL_STATE 3
+#define DMK_STATUS_FAIL_DELTASTATE 4
+#define DMK_STATUS_FAIL_STRESS 5
+#define DMK_STATUS_FAIL_LP_MAXIT 6
+#define DMK_STATUS_FAIL_LP_NAN 7
+#define DMK_STATUS_FAIL_LP_DGESV 8
+/* errors of this library */
+#define DMK_ERR_CUDA (-1)
+#define DMK_ERR_CUFFT (-2)
+#define DMK_ERR_CONFIG (-3)
+#define DMK_ERR_ARG (-4)
+#define DMK_ERR_STATE (-5)
+#define DMK_STATUS_TIMEOUT (-6)
+
+/* precision of the spectral part (FFT, Gamma, field update) */
+#define DMK_PRECISION_FP64 0
+#define DMK_PRECISION_MIXED 1
+
+/* Phase: Hooke elasticity + phenopowerlaw slip (SI units).
+   Keys as in material.yaml, phase_mechanical_elastic.f90:22-84 and
+   phase_mechanical_plastic_phenopowerlaw.f90:76-295; per-family arrays. */
+typedef struct {
+  int lattice;            /* 0 = cF, 1 = cI */
+  int n_families;         /* entries used in the per-family arrays */
+  int N_sl[4];
+  double C11, C12, C44;
+  double dot_gamma_0[4], n[4], a[4], h_0[4], xi_0[4], xi_inf[4], c_1[4], c_2[4], f_sat[4];
+  int n_h;                /* number of h_sl-sl interaction values */
+  double h_sl_sl[64];
+  int n_nonschmid;        /* cI family-1 non-Schmid coefficients a_non-Schmid (0..6) */
+  double a_nonschmid[6];
+  double atol_xi, atol_gamma;
+} dmk_phase;
+
+/* Numerical parameters: numerics.yaml keys (grid_mech_spectral_basic.f90:130-136,
+   spectral_utilities.f90:176-224, phase_mechanical.f90:281-295). */
+typedef struct {
+  int N_iter_min, N_iter_max;
+  double eps_abs_div, eps_rel_div, eps_abs_P, eps_rel_P;
+  int update_gamma;
+  int divergence_correction;   /* 0 none, 1 size, 2 grid+size */
+  int derivative;              /* 0 continuous */
+  double r_cutback_min, r_cutback, r_increase, eps_rel_state;
+  int N_iter_state_max;
+  int N_iter_Lp_max;
+  double r_linesearch_Lp, eps_rel_Lp, eps_abs_Lp;
+  int f_update_jacobi_Lp;
+  int N_iter_Li_max;
+  double r_linesearch_Li, eps_rel_Li, eps_abs_Li;
+  int f_update_jacobi_Li;
+} dmk_numerics;
+
+/* tBCmech (grid_utilities.f90:35-39): values/mask column-major, mask 1 = 'x' */
+typedef struct {
+  double values[9];
+  int mask[9];
+  int type;               /* 0 none, 1 L, 2 dot_F, 3 F, 4 P, 5 dot_P */
+} dmk_bc;
+
+/* tSolutionState (spectral_utilities.f90:77-83) plus diagnostics */
+typedef struct {
+  int iterationsNeeded;
+  int converged;
+  int stagConverged;
+  int residualEvals;
+  double err_div, err_BC;
+  double P_av[9];
+} dmk_solution_state;
+
+typedef struct dmk_ctx dmk_ctx;
+
+/* Field identifiers for dmk_get_field / dmk_set_field. */
+enum {
+  DMK_FIELD_F = 0,        /* phase F (3,3,N) */
+  DMK_FIELD_P = 1,        /* first Piola-Kirchhoff stress (3,3,N) */
+  DMK_FIELD_FE = 2,
+  DMK_FIELD_FP = 3,
+  DMK_FIELD_LP = 4,
+  DMK_FIELD_S = 5,
+  DMK_FIELD_XI_SL = 6,    /* (Ns,N) */
+  DMK_FIELD_GAMMA_SL = 7, /* (Ns,N) */
+  DMK_FIELD_F_LASTINC = 8,
+  DMK_FIELD_FI = 9,
+  DMK_FIELD_LI = 10,
+  DMK_FIELD_F_SOLVER = 11 /* solution field F of the spectral solver */
+};
+
+/* Create a context and run grid_mechanical_spectral_basic_init
+   (grid_mech_spectral_basic.f90:103-237; mechanical_init phase_mechanical.f90:184-338):
+   F := I, one constitutive sweep at dt = 0, Gamma reference stiffness := C_minMaxAvg.
+   materialAt: N entries, 0-based material index; quaternions: 4 per material (w,x,y,z).
+   precision: DMK_PRECISION_FP64 or DMK_PRECISION_MIXED. device: CUDA ordinal. */
+int dmk_mech_init(dmk_ctx** ctx, const int cells[3], const double geomSize[3], const int* materialAt,
+                  int n_materials, const double* quaternions, const dmk_phase* phase,
+                  const dmk_numerics* num, int precision, int device);
+
+/* grid_mechanical_spectral_basic_forward, grid_mech_spectral_basic.f90:284-355 */
+int dmk_mech_forward(dmk_ctx* ctx, int cutBack, int guess, double dt, double dt_old, double t_remaining,
+                     const dmk_bc* deformation, const dmk_bc* stress, const double q_rot[4]);
+
+/* grid_mechanical_spectral_basic_solution, grid_mech_spectral_basic.f90:243-277.
+   The residual is iterated as a Richardson fixed point F <- F - r(F). */
+int dmk_mech_solution(dmk_ctx* ctx, dmk_solution_state* out);
+
+/* materialpoint_forward -> mechanical_forward, phase_mechanical.f90:987-1002 */
+int dmk_materialpoint_forward(dmk_ctx* ctx);
+
+/* grid_mechanical_spectral_basic_updateCoords, grid_mech_spectral_basic.f90:361-372.
+   Nodal coordinates are an output-only quantity and are not produced on this path;
+   the call is accepted so that the host driver is unchanged. */
+int dmk_mech_update_coords(dmk_ctx* ctx);
+
+/* Field transfer to/from host buffers (Fortran layout). */
+int dmk_get_field(dmk_ctx* ctx, int field, double* host_out);
+int dmk_set_field(dmk_ctx* ctx, int field, const double* host_in);
+int dmk_field_size(dmk_ctx* ctx, int field);   /* doubles per voxel, or <0 */
+
+/* Restart contract (grid_mech_spectral_basic.f90:378-416): F_aim, F_aim_lastinc,
+   F_aimDot, P_aim (9 each), C_volAvg, C_volAvgLastInc, C_minMaxAvg (81 each). */
+int dmk_get_aims(dmk_ctx* ctx, double F_aim[9], double F_aim_lastinc[9], double F_aimDot[9],
+                 double P_aim[9], double C_volAvg[81], double C_volAvgLastInc[81], double C_minMaxAvg[81]);
+
+/* Operator-level entry points (unit parity).  Inputs/outputs are host arrays.
+   utilities_constitutiveResponse, grid_utilities.f90:133-207 */
+int dmk_constitutive_response(dmk_ctx* ctx, const double* F, double dt, double* P, double P_av[9],
+                              double C_volAvg[81], double C_minMaxAvg[81], int* status);
+/* utilities_updateGamma, spectral_utilities.f90:356-395 */
+int dmk_update_gamma(dmk_ctx* ctx, const double C[81]);
+/* utilities_GammaConvolution, spectral_utilities.f90:436-501 (in place) */
+int dmk_gamma_convolution(dmk_ctx* ctx, double* field, const double aim[9]);
+/* utilities_divergenceRMS, spectral_utilities.f90:650-691 */
+int dmk_divergence_rms(dmk_ctx* ctx, const double* P, double* out);
+/* phase_mechanical_dPdF, phase_mechanical.f90:1121-1242, for every voxel (81 per voxel) */
+int dmk_dPdF(dmk_ctx* ctx, double dt, double* dPdF);
+
+/* Per-voxel iteration counters of the last constitutive sweep: 4 ints per voxel
+   (integrateStateFPI iterations, integrateStress Newton iterations, substeps, status). */
+int dmk_get_iteration_counts(dmk_ctx* ctx, int* out);
+/* Totals of the last dmk_mech_solution: constitutive evaluations, state iterations,
+   Newton iterations, residual evaluations. */
+int dmk_get_counters(dmk_ctx* ctx, int64_t out[4]);
+/* Device time (ms) of the kernels of the last dmk_mech_solution, by stage:
+   constitutive, spectral (FFT + Gamma), other. */
+int dmk_get_timings(dmk_ctx* ctx, double out[3]);
+
+void dmk_destroy(dmk_ctx* ctx);
+const char* dmk_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif
