@@ -41,7 +41,8 @@ class NumericsStruct(C.Structure):
                 ('N_iter_Lp_max', C.c_int), ('r_linesearch_Lp', C.c_double), ('eps_rel_Lp', C.c_double),
                 ('eps_abs_Lp', C.c_double), ('f_update_jacobi_Lp', C.c_int),
                 ('N_iter_Li_max', C.c_int), ('r_linesearch_Li', C.c_double), ('eps_rel_Li', C.c_double),
-                ('eps_abs_Li', C.c_double), ('f_update_jacobi_Li', C.c_int)]
+                ('eps_abs_Li', C.c_double), ('f_update_jacobi_Li', C.c_int),
+                ('snes_type', C.c_int), ('anderson_m', C.c_int)]
 
 
 class BCStruct(C.Structure):
@@ -170,6 +171,23 @@ class Numerics:
     eps_rel_Li: float | None = None
     eps_abs_Li: float | None = None
     f_update_jacobi_Li: int | None = None
+    PETSc_options: str = ''
+    anderson_m: int = 8
+
+    @property
+    def snes_type(self) -> int:
+        """0 = Richardson (``-snes_type nrichardson``); 1 = Anderson-accelerated fixed point
+        (the reference's default ``-snes_type ngmres``, and ``anderson``)."""
+        toks = ('-snes_type ngmres ' + self.PETSc_options).split()
+        kind = 'ngmres'
+        for i, t in enumerate(toks[:-1]):
+            if t == '-snes_type':
+                kind = toks[i + 1]
+        if kind == 'nrichardson':
+            return 0
+        if kind in ('ngmres', 'anderson'):
+            return 1
+        raise ValueError(f'unsupported -snes_type {kind}')
 
     @classmethod
     def from_dict(cls, d: dict | None) -> 'Numerics':
@@ -186,6 +204,10 @@ class Numerics:
                           ('eps_abs_P', 'eps_abs_P'), ('eps_rel_P', 'eps_rel_P'), ('update_gamma', 'update_gamma')):
             if k_yaml in mech:
                 setattr(n, k, mech[k_yaml])
+        if 'PETSc_options' in mech:
+            n.PETSc_options = str(mech['PETSc_options'])
+        if 'anderson_m' in mech:
+            n.anderson_m = int(mech['anderson_m'])
         if 'divergence_correction' in fft:
             n.divergence_correction = fft['divergence_correction']
         if 'derivative' in fft:
@@ -216,6 +238,8 @@ class Numerics:
         if self.N_iter_Lp_max < 1: bad.append('N_iter_Lp_max')
         if self.N_iter_state_max < 1: bad.append('N_iter_state_max')
         if self.derivative != 'continuous': bad.append('derivative')
+        if not 1 <= self.anderson_m <= 32: bad.append('anderson_m')
+        self.snes_type
         if bad:
             raise ValueError('invalid numerics: ' + ' '.join(bad))
 
@@ -236,6 +260,8 @@ class Numerics:
         s.eps_rel_Li = self.eps_rel_Lp if self.eps_rel_Li is None else self.eps_rel_Li
         s.eps_abs_Li = self.eps_abs_Lp if self.eps_abs_Li is None else self.eps_abs_Li
         s.f_update_jacobi_Li = int(self.f_update_jacobi_Lp if self.f_update_jacobi_Li is None else self.f_update_jacobi_Li)
+        s.snes_type = self.snes_type
+        s.anderson_m = int(self.anderson_m)
         return s
 
 

@@ -96,6 +96,10 @@ struct dmk_ctx {
   int64_t last_counters[4] = {0, 0, 0, 0};
   double last_ms[3] = {0, 0, 0};
   bool iter_enabled = false;
+  // Anderson acceleration history (snes_type 1)
+  int aa_m = 0;
+  int aa_blocks = 0;
+  double *aa_dX = nullptr, *aa_dR = nullptr, *aa_Rprev = nullptr, *aa_partials = nullptr, *aa_out = nullptr;
 };
 
 namespace {
@@ -426,6 +430,50 @@ int response(dmk_ctx* c, double dt, int* status) {
   return 0;
 }
 
+constexpr int AA_CHUNK_HOST = 8;
+
+// Least-squares coefficients of the Anderson update (Walker & Ni 2011, type II):
+// gamma = argmin |r - dR gamma| from the normal equations G gamma = b on the slots
+// (oldest first), solved by Cholesky; while a pivot is not safely positive
+// (< 1e-13 of the largest diagonal) the oldest slot is dropped (gamma = 0 there).
+std::vector<double> anderson_coefficients(const std::vector<double>& G, int m, const std::vector<int>& slots,
+                                          const std::vector<double>& b) {
+  std::vector<double> gam(slots.size(), 0.0);
+  for (size_t first = 0; first < slots.size(); ++first) {
+    const size_t n = slots.size() - first;
+    std::vector<double> L(n * n, 0.0);
+    double dmax = 0.0;
+    for (size_t i = 0; i < n; ++i) dmax = std::max(dmax, G[size_t(slots[first + i]) * m + slots[first + i]]);
+    bool ok = dmax > 0.0;
+    for (size_t i = 0; ok && i < n; ++i)
+      for (size_t j = 0; j <= i; ++j) {
+        double sum = G[size_t(slots[first + i]) * m + slots[first + j]];
+        for (size_t k = 0; k < j; ++k) sum -= L[i * n + k] * L[j * n + k];
+        if (i == j) {
+          if (!(sum > 1.0e-13 * dmax)) { ok = false; break; }
+          L[i * n + i] = std::sqrt(sum);
+        } else {
+          L[i * n + j] = sum / L[j * n + j];
+        }
+      }
+    if (!ok) continue;
+    std::vector<double> y(n), x(n);
+    for (size_t i = 0; i < n; ++i) {
+      double sum = b[first + i];
+      for (size_t k = 0; k < i; ++k) sum -= L[i * n + k] * y[k];
+      y[i] = sum / L[i * n + i];
+    }
+    for (size_t i = n; i-- > 0;) {
+      double sum = y[i];
+      for (size_t k = i + 1; k < n; ++k) sum -= L[k * n + i] * x[k];
+      x[i] = sum / L[i * n + i];
+    }
+    for (size_t i = 0; i < n; ++i) gam[first + i] = x[i];
+    return gam;
+  }
+  return gam;
+}
+
 }  // namespace
 
 extern "C" {
@@ -506,6 +554,16 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   if ((rc = dalloc(&c->tan.partials, 81 * (size_t)c->tan_blocks)) || (rc = dalloc(&c->tan.nmax, c->tan_blocks)) ||
       (rc = dalloc(&c->tan.nmin, c->tan_blocks)) || (rc = dalloc(&c->tan.norms, N)))
     return bail(rc);
+  if (num->snes_type == 1) {
+    c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
+    c->aa_blocks = c->nsm * 4;
+    if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * 9 * N)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * 9 * N)) ||
+        (rc = dalloc(&c->aa_Rprev, 9 * N)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
+        (rc = dalloc(&c->aa_out, 4 * AA_MAX)))
+      return bail(rc);
+  } else if (num->snes_type != 0) {
+    return bail(fail(DMK_ERR_CONFIG, "snes_type must be 0 (Richardson) or 1 (Anderson)"));
+  }
   if ((rc = make_plans(c))) return bail(rc);
 
   // mechanical_init (phase_mechanical.f90:249-266), computed per voxel on the device
@@ -618,46 +676,87 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
   c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
   const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
   const bool mixed = c->precision == DMK_PRECISION_MIXED;
-  bool fp32 = mixed;
-  int evals = 0, reason = 0, apply = 0;
-  const void* rprev = nullptr;
-  SolverScalars hs;
+  const bool anderson = c->num.snes_type == 1;
+  const int m = c->aa_m;
+  const int64_t n9 = 9 * c->N;
   const int nspec = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
-  for (int it = 0;; ++it) {
+  bool fp32 = mixed;
+  int evals = 0, reason = 0;
+  SolverScalars hs;
+  int count = 0;                        // Anderson history pairs created so far
+  std::vector<double> G(size_t(m > 0 ? m : 1) * (m > 0 ? m : 1), 0.0), bvec;
+  std::vector<int> slots_b;             // slots that bvec refers to (oldest -> newest)
+  double dots[4 * AA_MAX];
+  int new_slot = -1;
+
+  // One residual evaluation at the current Fsol (apply: fuse F <- F - r into the sweep).
+  // Leaves r (FP64) and the convergence decision in hs; with Anderson also the inner
+  // products of the new residual with the history.
+  auto evaluate = [&](int apply) -> int {
     int st = 0;
-    if ((rc = evaluate_constitutive(c, c->dt, static_cast<const double*>(rprev), apply, &st))) return rc;
+    if (int e = evaluate_constitutive(c, c->dt, apply ? c->r : nullptr, apply, &st)) return e;
     ++evals;
     CK(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 1, c->stream));
-    CK(cudaEventRecord(c->ev[2], c->stream));
-    if ((rc = spectral_pass(c, fp32, 1, 1, fp32 ? static_cast<void*>(c->Pf) : static_cast<void*>(c->r)))) return rc;
-    CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, 1, c->stream));
-    CK(cudaEventRecord(c->ev[3], c->stream));
-    CK(cudaMemcpyAsync(&hs, c->sc, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
-    c->last_ms[1] += ms;
-    reason = hs.reason;
-    if (fp32 && reason == 1) {
-      // The FP32 spectral residual meets the tolerance: correction sweep in FP64 on the
-      // same stress field (no new constitutive evaluation); its residual decides.
-      fp32 = false;
+    for (int pass = 0; pass < 2; ++pass) {
+      const bool use32 = fp32 && pass == 0;
       CK(cudaEventRecord(c->ev[2], c->stream));
-      if ((rc = spectral_pass(c, false, 1, 1, c->r))) return rc;
-      CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, 0, c->stream));
+      if (int e = spectral_pass(c, use32, 1, 1, use32 ? static_cast<void*>(c->Pf) : static_cast<void*>(c->r))) return e;
+      if (use32) CK(launch_to_double(c->Pf, c->r, n9, c->nsm, c->stream));
+      CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, pass == 0 ? 1 : 0, c->stream));
       CK(cudaEventRecord(c->ev[3], c->stream));
+      int nsl = 0;
+      if (anderson && new_slot >= 0) {
+        slots_b.clear();
+        const int mk = std::min(count, m);
+        for (int q = count - mk; q < count; ++q) slots_b.push_back(q % m);
+        nsl = int(slots_b.size());
+        CK(launch_aa_dots(c->r, c->aa_Rprev, c->aa_dR, n9, new_slot, slots_b.data(), nsl, c->aa_partials,
+                          c->aa_blocks, c->aa_out, c->stream));
+        CK(cudaMemcpyAsync(dots, c->aa_out, sizeof(double) * 2 * AA_CHUNK_HOST * ((nsl + AA_CHUNK_HOST - 1) / AA_CHUNK_HOST),
+                           cudaMemcpyDeviceToHost, c->stream));
+      }
       CK(cudaMemcpyAsync(&hs, c->sc, sizeof hs, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
+      float ms = 0.f;
       CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
       c->last_ms[1] += ms;
-      reason = hs.reason;
-    } else if (fp32) {
-      CK(launch_to_double(c->Pf, c->r, 9 * c->N, c->nsm, c->stream));
+      if (nsl > 0) {
+        bvec.assign(nsl, 0.0);
+        for (int q = 0; q < nsl; ++q) {
+          const int ch = q / AA_CHUNK_HOST, k = q % AA_CHUNK_HOST;
+          const double g = dots[ch * 2 * AA_CHUNK_HOST + k], b = dots[ch * 2 * AA_CHUNK_HOST + AA_CHUNK_HOST + k];
+          G[size_t(new_slot) * m + slots_b[q]] = G[size_t(slots_b[q]) * m + new_slot] = g;
+          bvec[q] = b;
+        }
+      }
+      // FP32 spectral iterations that meet the tolerance get a correction sweep in FP64
+      // on the same stress field; its residual and decision replace the FP32 ones.
+      if (use32 && hs.reason == 1) { fp32 = false; continue; }
+      break;
     }
-    if (reason != 0) break;
-    if (it + 1 > snes_max_its) { reason = -1; break; }
-    rprev = c->r;   // F <- F - r is fused into the next constitutive sweep
-    apply = 1;
+    return 0;
+  };
+
+  if ((rc = evaluate(0))) return rc;
+  if (anderson) {
+    // b for the first Anderson step is empty (plain Richardson step)
+    bvec.clear();
+    slots_b.clear();
+  }
+  reason = hs.reason;
+  for (int it = 1; reason == 0; ++it) {
+    if (it > snes_max_its) { reason = -1; break; }
+    if (!anderson) {
+      if ((rc = evaluate(1))) return rc;
+    } else {
+      std::vector<double> gam = anderson_coefficients(G, m, slots_b, bvec);
+      new_slot = count % m;
+      CK(launch_aa_update(c->Fsol, c->r, c->aa_Rprev, c->aa_dX, c->aa_dR, n9, new_slot, slots_b.data(), gam.data(),
+                          int(slots_b.size()), c->aa_blocks, c->stream));
+      ++count;
+      if ((rc = evaluate(0))) return rc;
+    }
+    reason = hs.reason;
   }
   std::memcpy(c->F_aim, hs.F_aim, sizeof c->F_aim);
   std::memcpy(c->P_av, hs.P_av, sizeof c->P_av);
@@ -859,7 +958,8 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->Fdot, (void*)c->state, (void*)c->state0, (void*)c->spec, (void*)c->specf, (void*)c->Pf,
                   (void*)c->partials, (void*)c->sums, (void*)c->div_partials, (void*)c->status, (void*)c->iter,
                   (void*)c->counters, (void*)c->sc, (void*)c->scratch, (void*)c->tan_out, (void*)c->tan_idx,
-                  (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work})
+                  (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work,
+                  (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out})
     if (p) cudaFree(p);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);

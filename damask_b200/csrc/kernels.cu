@@ -12,6 +12,7 @@
 #include "kernels.cuh"
 #include "constitutive.cuh"
 
+#include <algorithm>
 #include <cfloat>
 
 namespace dmk {
@@ -528,6 +529,119 @@ cudaError_t launch_init_state(const int* material, const double* quats, const do
                               double* state0, cudaStream_t s) {
   init_state_kernel<<<int((N + 255) / 256), 256, 0, s>>>(material, quats, xi0, NS, N, F, F0, Fsol, Flast, Fp, Fp0, Fe,
                                                          state, state0);
+  return cudaGetLastError();
+}
+
+}  // namespace dmk
+
+namespace dmk {
+
+// ------------------------------------------------------------------ Anderson acceleration
+// After an evaluation with residual R: dR[slot] = R - Rprev (if write_slot >= 0), and the
+// inner products g_t = dR[slot].dR[t] and b_t = dR[t].R for up to AA_CHUNK history slots
+// per launch (per-block partial sums, reduced by the caller in block order).
+constexpr int AA_CHUNK = 8;
+struct AASlots {
+  int n;                 // slots in this chunk
+  int slot[AA_CHUNK];
+};
+
+__global__ void __launch_bounds__(256)
+aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, double* __restrict__ dR, int64_t n,
+               int write_slot, AASlots sl, double* __restrict__ partials) {
+  __shared__ double red[2 * AA_CHUNK][8];
+  double g[AA_CHUNK], b[AA_CHUNK];
+#pragma unroll
+  for (int q = 0; q < AA_CHUNK; ++q) { g[q] = 0.0; b[q] = 0.0; }
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const double r = R[e];
+    double dn = 0.0;
+    if (write_slot >= 0) {
+      dn = r - Rprev[e];
+      if (blockIdx.y == 0) dR[int64_t(write_slot) * n + e] = dn;
+    }
+#pragma unroll
+    for (int q = 0; q < AA_CHUNK; ++q) {
+      if (q < sl.n) {
+        const double d = (sl.slot[q] == write_slot) ? dn : dR[int64_t(sl.slot[q]) * n + e];
+        g[q] = fma(dn, d, g[q]);
+        b[q] = fma(d, r, b[q]);
+      }
+    }
+  }
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int q = 0; q < AA_CHUNK; ++q) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      g[q] += __shfl_down_sync(0xffffffffu, g[q], o);
+      b[q] += __shfl_down_sync(0xffffffffu, b[q], o);
+    }
+    if (lane == 0) { red[q][warp] = g[q]; red[AA_CHUNK + q][warp] = b[q]; }
+  }
+  __syncthreads();
+  if (threadIdx.x < 2 * AA_CHUNK) {
+    double s = 0.0;
+    for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
+    partials[int64_t(blockIdx.x) * 2 * AA_CHUNK + threadIdx.x] = s;
+  }
+}
+
+__global__ void aa_reduce_kernel(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
+  const int t = threadIdx.x;
+  if (t >= 2 * AA_CHUNK) return;
+  double s = 0.0;
+  for (int b = 0; b < nblocks; ++b) s += partials[int64_t(b) * 2 * AA_CHUNK + t];
+  out[t] = s;
+}
+
+cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,
+                           const int* slots, int nslots, double* partials, int nblocks, double* out, cudaStream_t s) {
+  // out: for each chunk c, 2*AA_CHUNK doubles (g then b)
+  int done = 0, chunk = 0;
+  do {
+    AASlots sl;
+    sl.n = std::min(AA_CHUNK, nslots - done);
+    for (int q = 0; q < AA_CHUNK; ++q) sl.slot[q] = q < sl.n ? slots[done + q] : 0;
+    // the first chunk writes dR[write_slot]; later chunks need dn for g, so they
+    // recompute it from R - Rprev without writing
+    const int ws = write_slot;
+    aa_dots_kernel<<<nblocks, 256, 0, s>>>(R, Rprev, dR, n, ws, sl, partials);
+    aa_reduce_kernel<<<1, 32, 0, s>>>(partials, nblocks, out + chunk * 2 * AA_CHUNK);
+    done += sl.n;
+    ++chunk;
+  } while (done < nslots);
+  return cudaGetLastError();
+}
+
+// X <- X - R - sum_t gamma_t (dX[t] - dR[t]);  dX[new_slot] = X_new - X_old;  Rprev = R
+struct AAUpdate {
+  int n;
+  int slot[32];
+  double gamma[32];
+};
+__global__ void __launch_bounds__(256)
+aa_update_kernel(double* __restrict__ X, const double* __restrict__ R, double* __restrict__ Rprev,
+                 double* __restrict__ dX, const double* __restrict__ dR, int64_t n, int new_slot,
+                 const __grid_constant__ AAUpdate u) {
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+    const double x = X[e], r = R[e];
+    double xn = x - r;
+    for (int q = 0; q < u.n; ++q) {
+      const int64_t off = int64_t(u.slot[q]) * n + e;
+      xn = fma(-u.gamma[q], dX[off] - dR[off], xn);
+    }
+    dX[int64_t(new_slot) * n + e] = xn - x;
+    X[e] = xn;
+    Rprev[e] = r;
+  }
+}
+cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* dX, const double* dR, int64_t n,
+                             int new_slot, const int* slots, const double* gamma, int nslots, int nblocks, cudaStream_t s) {
+  AAUpdate u;
+  u.n = nslots;
+  for (int q = 0; q < 32; ++q) { u.slot[q] = q < nslots ? slots[q] : 0; u.gamma[q] = q < nslots ? gamma[q] : 0.0; }
+  aa_update_kernel<<<nblocks, 256, 0, s>>>(X, R, Rprev, dX, dR, n, new_slot, u);
   return cudaGetLastError();
 }
 

@@ -59,6 +59,13 @@ cudaError_t launch_copy(const double* a, double* b, int64_t n, int nsm, cudaStre
 cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s);
 cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
 
+// Anderson acceleration of the fixed point (kernels.cu)
+constexpr int AA_MAX = 32;
+cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,
+                           const int* slots, int nslots, double* partials, int nblocks, double* out, cudaStream_t s);
+cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* dX, const double* dR, int64_t n,
+                             int new_slot, const int* slots, const double* gamma, int nslots, int nblocks, cudaStream_t s);
+
 // consistent tangent (dpdf.cu)
 struct TangentOut {
   double* partials;      // per block: 81 sums of dPdF

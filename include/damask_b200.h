@@ -83,6 +83,9 @@ typedef struct {
   int N_iter_Li_max;
   double r_linesearch_Li, eps_rel_Li, eps_abs_Li;
   int f_update_jacobi_Li;
+  int snes_type;               /* fixed-point iteration of the residual: 0 Richardson F <- F - r
+                                  (PETSc -snes_type nrichardson), 1 Anderson-accelerated */
+  int anderson_m;              /* Anderson history depth (1..32) */
 } dmk_numerics;
 
 /* tBCmech (grid_utilities.f90:35-39): values/mask column-major, mask 1 = 'x' */

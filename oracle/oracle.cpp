@@ -1079,6 +1079,43 @@ void form_residual(orc_ctx* c, std::vector<M3>& r) {
   gamma_convolution(c, r.data(), rot33(c->rot_q, deltaF_aim, true));
 }
 
+// Least-squares coefficients of the Anderson update: solve G_S gamma = b_S on the
+// slots S (oldest first) by Cholesky; while a pivot is not safely positive
+// (< 1e-13 of the largest diagonal), drop the oldest slot and retry.
+template <class BFn>
+std::vector<double> anderson_coefficients(const std::vector<double>& G, int m, std::vector<int>& slots, BFn bfn) {
+  std::vector<double> b(slots.size());
+  for (size_t q = 0; q < slots.size(); ++q) b[q] = bfn(slots[q]);
+  size_t first = 0;
+  while (first < slots.size()) {
+    const size_t n = slots.size() - first;
+    std::vector<double> L(n * n, 0.0);
+    double dmax = 0.0;
+    for (size_t i = 0; i < n; ++i) dmax = std::max(dmax, G[size_t(slots[first + i]) * m + slots[first + i]]);
+    bool ok = dmax > 0.0;
+    for (size_t i = 0; ok && i < n; ++i) {
+      for (size_t j = 0; j <= i; ++j) {
+        double sum = G[size_t(slots[first + i]) * m + slots[first + j]];
+        for (size_t k = 0; k < j; ++k) sum -= L[i * n + k] * L[j * n + k];
+        if (i == j) {
+          if (!(sum > 1.0e-13 * dmax)) { ok = false; break; }
+          L[i * n + i] = std::sqrt(sum);
+        } else {
+          L[i * n + j] = sum / L[j * n + j];
+        }
+      }
+    }
+    if (!ok) { ++first; continue; }
+    std::vector<double> y(n), x(n);
+    for (size_t i = 0; i < n; ++i) { double sum = b[first + i]; for (size_t k = 0; k < i; ++k) sum -= L[i * n + k] * y[k]; y[i] = sum / L[i * n + i]; }
+    for (size_t i = n; i-- > 0;) { double sum = y[i]; for (size_t k = i + 1; k < n; ++k) sum -= L[k * n + i] * x[k]; x[i] = sum / L[i * n + i]; }
+    std::vector<double> gam(slots.size(), 0.0);
+    for (size_t i = 0; i < n; ++i) gam[first + i] = x[i];
+    return gam;
+  }
+  return std::vector<double>(slots.size(), 0.0);
+}
+
 }  // namespace
 
 // ==================================================================== C API
@@ -1223,12 +1260,57 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
   };
   form_residual(c, r); evals++;
   if (!finite()) reason = -1; else reason = converged();
-  for (int it = 1; reason == 0 && it <= snes_max_its; ++it) {
-    for (long v = 0; v < c->N; ++v) c->Fsol[v] = sub(c->Fsol[v], r[v]);
-    form_residual(c, r); evals++;
-    if (!finite()) { reason = -1; break; }
-    reason = converged();
-    if (reason == 0 && it == snes_max_its) reason = -1;
+  if (c->num.snes_type == 0) {
+    for (int it = 1; reason == 0 && it <= snes_max_its; ++it) {
+      for (long v = 0; v < c->N; ++v) c->Fsol[v] = sub(c->Fsol[v], r[v]);
+      form_residual(c, r); evals++;
+      if (!finite()) { reason = -1; break; }
+      reason = converged();
+      if (reason == 0 && it == snes_max_its) reason = -1;
+    }
+  } else {
+    // Anderson-accelerated fixed point of X <- X - r(X) (Walker & Ni 2011, type II, depth m):
+    // gamma = argmin |r_k - dR gamma|, X_{k+1} = X_k - r_k - (dX - dR) gamma, where dX, dR hold
+    // the last m differences of iterates and residuals.
+    const int m = std::max(1, std::min(c->num.anderson_m, 32));
+    const long N = c->N;
+    std::vector<std::vector<M3>> dX(m, std::vector<M3>(N)), dR(m, std::vector<M3>(N));
+    std::vector<M3> Rprev(N);
+    std::vector<double> G(size_t(m) * m, 0.0);
+    int count = 0;
+    auto dot = [&](const std::vector<M3>& a, const std::vector<M3>& b) {
+      double s = 0.0;
+      for (long v = 0; v < N; ++v) for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) s += a[v].a[i][j] * b[v].a[i][j];
+      return s;
+    };
+    for (int it = 1; reason == 0 && it <= snes_max_its; ++it) {
+      const int mk = std::min(count, m);
+      std::vector<int> slots;                       // oldest -> newest
+      for (int q = count - mk; q < count; ++q) slots.push_back(q % m);
+      std::vector<double> gam = anderson_coefficients(G, m, slots, [&](int sl) { return dot(dR[sl], r); });
+      const int slot = count % m;
+      for (long v = 0; v < N; ++v) {
+        M3 xn = sub(c->Fsol[v], r[v]);
+        for (size_t q = 0; q < slots.size(); ++q) {
+          if (gam[q] == 0.0) continue;
+          xn = sub(xn, scl(gam[q], sub(dX[slots[q]][v], dR[slots[q]][v])));
+        }
+        dX[slot][v] = sub(xn, c->Fsol[v]);
+        c->Fsol[v] = xn;
+        Rprev[v] = r[v];
+      }
+      form_residual(c, r); evals++;
+      if (!finite()) { reason = -1; break; }
+      for (long v = 0; v < N; ++v) dR[slot][v] = sub(r[v], Rprev[v]);
+      ++count;
+      const int mk2 = std::min(count, m);
+      for (int q = count - mk2; q < count; ++q) {
+        const int t = q % m;
+        G[size_t(slot) * m + t] = G[size_t(t) * m + slot] = dot(dR[slot], dR[t]);
+      }
+      reason = converged();
+      if (reason == 0 && it == snes_max_its) reason = -1;
+    }
   }
   out->converged = reason > 0;
   out->iterationsNeeded = c->totalIter;

@@ -53,6 +53,8 @@ typedef struct {
   int N_iter_Li_max;
   double r_linesearch_Li, eps_rel_Li, eps_abs_Li;
   int f_update_jacobi_Li;
+  int snes_type;               /* 0 Richardson (nrichardson), 1 Anderson-accelerated */
+  int anderson_m;              /* Anderson history depth */
 } orc_numerics;
 
 typedef struct {
