@@ -1,0 +1,354 @@
+#!/usr/bin/env python
+"""Benchmark of DAMASK's grid mechanical hot path on B200.
+
+Metric: material-point updates/s (one update = one constitutive evaluation of one
+voxel inside one residual evaluation of the basic spectral scheme) on the 256^3
+bcc RVE (2000 Voronoi grains, seed 3, phenopowerlaw N_sl [12,12], uniaxial
+tension dot_F_xx = 1e-3/s to 10 % in 100 increments).  One step = one load
+increment (forward, the fixed-point solve to convergence, materialpoint forward).
+
+  python bench.py [--gpus N --steps K --warmup W]     # this implementation
+  python bench.py --impl reference ...                  # CPU restatement (oracle) on host cores
+
+Multi-GPU (torchrun, one rank per GPU): the path is run as independent replicas,
+one RVE per GPU, with no collective in the data path ("weak" scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+WORKLOAD = 'grid256_bcc24_2000g'
+METRIC = 'material-point updates/s at 256^3: mixed vs FP64 GPU, P within 1e-5 of FP64'
+FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (CUDA cores), datasheet figure
+
+
+def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> float:
+    """Static arithmetic count of the constitutive kernel (see DESIGN.md, FP64 FLOPs):
+    per Newton iteration 1458 + 173 Ns, per state iteration 2 Ns^2 + 57 Ns + 400,
+    per update 2 Ns^2 + 28 Ns (initial dotState)."""
+    return newton * (1458 + 173 * ns) + state * (2 * ns * ns + 57 * ns + 400) + updates * (2 * ns * ns + 28 * ns)
+
+
+def bc_bytes() -> int:
+    """Host bytes passed to the device per increment: two boundary-condition structs and the rotation."""
+    import ctypes
+    from damask_b200.config import BCStruct
+    return 2 * ctypes.sizeof(BCStruct) + 4 * 8
+
+
+def constitutive_bytes(ns: int) -> int:
+    """Algorithmic HBM bytes per update of the constitutive kernel (Anderson form):
+    reads F, F0, Fp0, Lp (9 doubles each), S0 (6), state0 (2 Ns); writes F, P, Fp, Lp, Fe
+    (9 each), S (6), state (2 Ns)."""
+    return 8 * (4 * 9 + 6 + 2 * ns) + 8 * (5 * 9 + 6 + 2 * ns)
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ('clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,'
+              'clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,'
+              'clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu: int):
+        self.gpu = gpu
+        self.proc = None
+        self.lines: list[str] = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), f'--query-gpu={self.FIELDS}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+            return
+        self._t = threading.Thread(target=self._read, daemon=True)
+        self._t.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        if self._t:
+            self._t.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(',')]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for n, v in zip(names, parts[3:7]):
+                if v.lower().startswith('active'):
+                    reasons.add(n)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': max(smax) if smax else None,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=600),
+                                device_id=torch.device('cuda', local))
+    return world, rank, local
+
+
+def allreduce_max(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def allreduce_sum(x: float, world: int) -> float:
+    if world == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def barrier(world: int):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def load_peaks() -> dict:
+    p = ROOT / 'MEASURED_PEAKS.json'
+    if p.exists():
+        d = json.loads(p.read_text())
+        return {'hbm_gbs': float(d['hbm_gbs']), 'source': 'measured'}
+    return {'hbm_gbs': 6650.0, 'source': 'fallback'}
+
+
+def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, local: int, cells=None) -> dict:
+    from damask_b200 import workloads
+    from damask_b200.grid import IncrementDriver, SpectralBasic
+
+    rve, phase, lcs, num = workloads.make(WORKLOAD, cells)
+    solver = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision,
+                           device=local)
+    drv = IncrementDriver(solver, lcs)
+    p_av = []
+
+    def one_step(e2e_buf=None):
+        c0, t0 = solver.total_counters.copy(), solver.total_ms.copy()
+        recs = drv.step()
+        c = solver.total_counters - c0
+        tm = solver.total_ms - t0
+        if e2e_buf is not None:
+            solver.get_field('P', out=e2e_buf)
+        p_av.extend(r.P_av for r in recs)
+        return recs, c, tm
+
+    for _ in range(warmup):
+        one_step()
+    # timed region: inputs resident in HBM, device time on the solver's stream
+    barrier(world)
+    clocks = ClockSampler(local)
+    clocks.start()
+    launches0 = solver.launches()
+    solver.timer_start()
+    upd = newton = state = evals = 0
+    const_ms = 0.0
+    for _ in range(steps):
+        recs, c, tm = one_step()
+        upd += c[0]
+        state += c[1]
+        newton += c[2]
+        evals += c[3]
+        const_ms += tm[0]
+    ms = solver.timer_stop()
+    launches = solver.launches() - launches0
+    clk = clocks.stop()
+    barrier(world)
+    # end to end through the public API: per step the BCs go in from host memory
+    # and the stress field P comes back into pinned host memory
+    import torch
+    pinned = torch.empty((solver.N, 9), dtype=torch.float64, pin_memory=True).numpy()
+    barrier(world)
+    solver.timer_start()
+    upd_e2e = 0
+    for _ in range(steps):
+        recs, c, _tm = one_step(e2e_buf=pinned)
+        upd_e2e += c[0]
+    ms_e2e = solver.timer_stop()
+    barrier(world)
+    out = {'updates': upd, 'ms': ms, 'newton': newton, 'state': state, 'evals': evals, 'const_ms': const_ms,
+           'launches': launches, 'clocks': clk, 'updates_e2e': upd_e2e, 'ms_e2e': ms_e2e, 'N': solver.N,
+           'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8}
+    solver.close()
+    return out
+
+
+def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None) -> dict:
+    """The CPU restatement on the same material and load, on a 48^3 cut of the
+    workload's statistics (13 grains, seed 3), first increments; ~10-30 s of work."""
+    from damask_b200 import workloads
+    from damask_b200.grid import IncrementDriver
+    from damask_b200.synthetic import voronoi_rve
+    from oracle.oracle import OracleSpectralBasic
+
+    threads = threads or os.cpu_count() or 1
+    cells = (48, 48, 48)
+    rve = voronoi_rve(cells, workloads.SIZE_1MM, 13, 3)
+    phase = workloads.bcc_24()
+    lcs = workloads.tension_x(100.0, 100)
+    o = OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, workloads.numerics_default(),
+                            threads=threads)
+    drv = IncrementDriver(o, lcs)
+    for _ in range(warmup):
+        drv.step()
+    t0 = time.perf_counter()
+    upd = 0
+    for _ in range(steps):
+        for r in drv.step():
+            upd += r.residual_evals * o.N
+    dt = time.perf_counter() - t0
+    o.close()
+    return {'value': upd / dt, 'seconds': dt, 'cores': threads, 'updates': upd,
+            'sample': f'oracle (C++ FP64, OpenMP) on a 48^3 RVE, 13 grains, same bcc-24 material and tension load, '
+                      f'increments {warmup + 1}..{warmup + steps}'}
+
+
+def _json_default(o):
+    if isinstance(o, np.integer):
+        return int(o)
+    if isinstance(o, np.floating):
+        return float(o)
+    raise TypeError(type(o))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=3)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
+    ap.add_argument('--cells', type=str, default=None, help='override grid (testing only)')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--precision', choices=['both', 'mixed', 'fp64'], default='both',
+                    help='run one precision only (profiling); the bench line needs both')
+    args = ap.parse_args()
+    world, rank, local = dist_setup()
+    warmup = max(3, args.warmup)
+    cells = tuple(int(x) for x in args.cells.split(',')) if args.cells else None
+
+    if args.impl == 'reference':
+        if rank != 0:
+            return
+        s = cpu_sample(steps=max(1, args.steps), warmup=0)
+        line = {'metric': METRIC, 'value': s['value'], 'unit': 'updates/s', 'n_gpus': args.gpus, 'steps': args.steps,
+                'warmup': 0, 'ms_per_step': 1e3 * s['seconds'] / max(1, args.steps), 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'impl': 'reference',
+                'config': {'workload': 'bcc-24 phenopowerlaw RVE, tension 1e-3/s (48^3 bounded sample of the '
+                                       '256^3/2000-grain workload)', 'solver': 'Anderson fixed point'},
+                'cpu_baseline': {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port',
+                                 'sample': s['sample']},
+                'e2e': {'value': s['value'], 'unit': 'updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
+        print(json.dumps(line, default=_json_default), flush=True)
+        return
+
+    res = {}
+    precs = ('mixed', 'fp64') if args.precision == 'both' else (args.precision,)
+    for prec in precs:
+        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells)
+    mx = res.get('mixed', res.get('fp64'))
+    fp = res.get('fp64', mx)
+    ms_max = allreduce_max(mx['ms'], world)
+    upd_tot = allreduce_sum(mx['updates'], world)
+    value = upd_tot / (ms_max * 1e-3)
+    fp_ms = allreduce_max(fp['ms'], world)
+    fp_value = allreduce_sum(fp['updates'], world) / (fp_ms * 1e-3)
+    e2e_ms = allreduce_max(mx['ms_e2e'], world)
+    e2e_value = allreduce_sum(mx['updates_e2e'], world) / (e2e_ms * 1e-3)
+    # agreement of the volume-averaged stress of the mixed and FP64 runs, increment by increment
+    rel = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(mx['p_av'], fp['p_av'])]
+    peaks = load_peaks()
+    ns = mx['ns']
+    bpu = constitutive_bytes(ns)
+    avg_launch_ms = mx['const_ms'] / max(1, mx['evals'])
+    achieved_gbs = bpu * mx['N'] / (avg_launch_ms * 1e-3) / 1e9
+    flops = constitutive_flops(ns, mx['newton'], mx['state'], mx['updates'])
+    fp64_tflops = flops / (mx['const_ms'] * 1e-3) / 1e12
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        s = cpu_sample()
+        cpu = {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port', 'sample': s['sample']}
+    line = {
+        'metric': METRIC, 'value': value, 'unit': 'updates/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': warmup, 'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'f64 constitutive, f32 spectral (mixed)', 'data': 'synthetic',
+        'config': {'workload': f'{WORKLOAD}: 256^3 grid, 2000 Voronoi grains (seed 3), bcc N_sl [12,12], '
+                               'tension dot_F_xx 1e-3/s, 100 increments to 10 %' if cells is None else
+                               f'{WORKLOAD} at {cells}',
+                   'solver': 'basic spectral, Anderson fixed point (m=8)', 'precision': 'mixed',
+                   'parallelism': f'replicas x{world}', 'l2': 'inputs larger than L2 (per-voxel state ~30 GB)',
+                   'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
+        'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
+        'mixed_over_fp64': value / fp_value,
+        'mixed_vs_fp64_P_av_rel_err_max': max(rel) if rel else None,
+        'roofline': {'bound': 'hbm', 'kernel': 'constitutive_kernel<24>', 'achieved': achieved_gbs,
+                     'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved_gbs / peaks['hbm_gbs'],
+                     'peak_source': peaks['source'], 'traffic': None, 'bytes_per_update': bpu,
+                     'fp64_tflops': fp64_tflops, 'fp64_frac_of_nominal': fp64_tflops / FP64_NOMINAL_TFLOPS,
+                     'avg_launch_ms': avg_launch_ms},
+        'cpu_baseline': cpu,
+        'e2e': {'value': e2e_value, 'unit': 'updates/s', 'h2d_bytes_per_step': bc_bytes(),
+                'd2h_bytes_per_step': mx['d2h_bytes']},
+        'gpu_launches': mx['launches'],
+        'clocks': mx['clocks'],
+        'iterations': {'newton_per_update': mx['newton'] / max(1, mx['updates']),
+                       'state_per_update': mx['state'] / max(1, mx['updates']),
+                       'residual_evals': mx['evals']},
+    }
+    print(json.dumps(line, default=_json_default), flush=True)
+
+
+if __name__ == '__main__':
+    main()

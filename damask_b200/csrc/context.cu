@@ -29,6 +29,12 @@ int fail(int code, const std::string& msg) {
     cudaError_t e_ = (x);                                                                  \
     if (e_ != cudaSuccess) return fail(DMK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
   } while (0)
+#define CKL(x)                                                                             \
+  do {                                                                                     \
+    cudaError_t e_ = (x);                                                                  \
+    if (e_ != cudaSuccess) return fail(DMK_ERR_CUDA, std::string(#x) + ": " + cudaGetErrorString(e_)); \
+    ++c->launches;                                                                         \
+  } while (0)
 #define CKF(x)                                                                             \
   do {                                                                                     \
     cufftResult r_ = (x);                                                                  \
@@ -96,6 +102,8 @@ struct dmk_ctx {
   int64_t last_counters[4] = {0, 0, 0, 0};
   double last_ms[3] = {0, 0, 0};
   bool iter_enabled = false;
+  int64_t launches = 0;                  // kernels of this library launched by the context
+  cudaEvent_t tev[2] = {nullptr, nullptr};
   // Anderson acceleration history (snes_type 1)
   int aa_m = 0;
   int aa_blocks = 0;
@@ -332,7 +340,7 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
   CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
   Fields f = make_fields(c, r);
   CK(cudaEventRecord(c->ev[0], c->stream));
-  CK(run_constitutive(c, f, dt, apply));
+  CKL(run_constitutive(c, f, dt, apply));
   CK(cudaEventRecord(c->ev[1], c->stream));
   int st = 0;
   CK(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -341,7 +349,7 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
   c->last_ms[0] += ms;
   if (st == 0) std::swap(c->P, c->Pnew);
-  else CK(launch_sum9(c->P, c->N, c->partials, c->stream));
+  else CKL(launch_sum9(c->P, c->N, c->partials, c->stream));
   *status_out = st;
   return 0;
 }
@@ -353,9 +361,10 @@ int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
   Fields f = make_fields(c, nullptr);
   TangentOut o = c->tan;
   o.per_voxel = per_voxel_dev;
-  CK(run_dPdF(c, f, dt, o));
-  CK(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
-  CK(run_pick(c, f, dt));
+  CKL(run_dPdF(c, f, dt, o));
+  CKL(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
+  c->launches += 1;   // finalize + first-index kernels
+  CKL(run_pick(c, f, dt));
   double h[243];
   CK(cudaMemcpyAsync(h, c->tan_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
@@ -379,7 +388,7 @@ int spectral_pass(dmk_ctx* c, bool fp32, int do_gamma, int do_div, void* out) {
                                 do_div, c->stream));
     if (do_gamma) CKF(cufftExecZ2D(c->plan_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), static_cast<double*>(out)));
   } else {
-    CK(launch_to_float(c->P, c->Pf, 9 * c->N, c->nsm, c->stream));
+    CKL(launch_to_float(c->P, c->Pf, 9 * c->N, c->nsm, c->stream));
     CKF(cufftExecR2C(c->plan_fwd_f, c->Pf, reinterpret_cast<cufftComplex*>(c->specf)));
     CK(launch_gamma_div<float>(c->specf, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, do_gamma,
                                do_div, c->stream));
@@ -401,12 +410,12 @@ int ensure_scratch(dmk_ctx* c, int K) {
 int h2d_planes(dmk_ctx* c, const double* host, double* dev_planes, int K) {
   if (int rc = ensure_scratch(c, K)) return rc;
   CK(cudaMemcpyAsync(c->scratch, host, sizeof(double) * K * c->N, cudaMemcpyHostToDevice, c->stream));
-  CK(launch_to_planes(c->scratch, dev_planes, c->N, K, c->stream));
+  CKL(launch_to_planes(c->scratch, dev_planes, c->N, K, c->stream));
   return 0;
 }
 int d2h_planes(dmk_ctx* c, const double* dev_planes, double* host, int K) {
   if (int rc = ensure_scratch(c, K)) return rc;
-  CK(launch_from_planes(dev_planes, c->scratch, c->N, K, c->stream));
+  CKL(launch_from_planes(dev_planes, c->scratch, c->N, K, c->stream));
   CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * K * c->N, cudaMemcpyDeviceToHost, c->stream));
   CK(cudaStreamSynchronize(c->stream));
   return 0;
@@ -416,7 +425,7 @@ int response(dmk_ctx* c, double dt, int* status) {
   int st = 0;
   int rc = evaluate_constitutive(c, dt, nullptr, 0, &st);
   if (rc) return rc;
-  CK(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 0, c->stream));
+  CKL(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 0, c->stream));
   double pav[9];
   CK(cudaMemcpyAsync(pav, reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, P_av), sizeof pav,
                      cudaMemcpyDeviceToHost, c->stream));
@@ -659,9 +668,10 @@ int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_ol
   CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_fwd), aim, sizeof aim,
                      cudaMemcpyHostToDevice, c->stream));
   const double* dsc = reinterpret_cast<const double*>(c->sc);
-  CK(launch_forward(c->Fsol, c->Flast, c->Fdot, c->N, cutBack, guess, dt, dt_old,
+  CKL(launch_forward(c->Fsol, c->Flast, c->Fdot, c->N, cutBack, guess, dt, dt_old,
                     dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->partials, c->sums, c->wgt,
                     dsc + offsetof(SolverScalars, aim_fwd) / sizeof(double), c->stream));
+  c->launches += 2;   // forward, partial reduction, shift
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -696,13 +706,13 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
     int st = 0;
     if (int e = evaluate_constitutive(c, c->dt, apply ? c->r : nullptr, apply, &st)) return e;
     ++evals;
-    CK(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 1, c->stream));
+    CKL(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 1, c->stream));
     for (int pass = 0; pass < 2; ++pass) {
       const bool use32 = fp32 && pass == 0;
       CK(cudaEventRecord(c->ev[2], c->stream));
       if (int e = spectral_pass(c, use32, 1, 1, use32 ? static_cast<void*>(c->Pf) : static_cast<void*>(c->r))) return e;
-      if (use32) CK(launch_to_double(c->Pf, c->r, n9, c->nsm, c->stream));
-      CK(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, pass == 0 ? 1 : 0, c->stream));
+      if (use32) CKL(launch_to_double(c->Pf, c->r, n9, c->nsm, c->stream));
+      CKL(launch_converge(c->sc, c->div_partials, nspec, c->wgt, c->status, c->nm2, pass == 0 ? 1 : 0, c->stream));
       CK(cudaEventRecord(c->ev[3], c->stream));
       int nsl = 0;
       if (anderson && new_slot >= 0) {
@@ -710,8 +720,9 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
         const int mk = std::min(count, m);
         for (int q = count - mk; q < count; ++q) slots_b.push_back(q % m);
         nsl = int(slots_b.size());
-        CK(launch_aa_dots(c->r, c->aa_Rprev, c->aa_dR, n9, new_slot, slots_b.data(), nsl, c->aa_partials,
+        CKL(launch_aa_dots(c->r, c->aa_Rprev, c->aa_dR, n9, new_slot, slots_b.data(), nsl, c->aa_partials,
                           c->aa_blocks, c->aa_out, c->stream));
+        c->launches += 2 * ((nsl + AA_CHUNK_HOST - 1) / AA_CHUNK_HOST) - 1;   // dots + reduce per chunk
         CK(cudaMemcpyAsync(dots, c->aa_out, sizeof(double) * 2 * AA_CHUNK_HOST * ((nsl + AA_CHUNK_HOST - 1) / AA_CHUNK_HOST),
                            cudaMemcpyDeviceToHost, c->stream));
       }
@@ -751,7 +762,7 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
     } else {
       std::vector<double> gam = anderson_coefficients(G, m, slots_b, bvec);
       new_slot = count % m;
-      CK(launch_aa_update(c->Fsol, c->r, c->aa_Rprev, c->aa_dX, c->aa_dR, n9, new_slot, slots_b.data(), gam.data(),
+      CKL(launch_aa_update(c->Fsol, c->r, c->aa_Rprev, c->aa_dX, c->aa_dR, n9, new_slot, slots_b.data(), gam.data(),
                           int(slots_b.size()), c->aa_blocks, c->stream));
       ++count;
       if ((rc = evaluate(0))) return rc;
@@ -823,7 +834,7 @@ int dmk_get_field(dmk_ctx* c, int field, double* host) {
     case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NS);
     case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NS);
     case DMK_FIELD_S:
-      CK(launch_sym6_to9(c->S, c->scratch, N, c->stream));
+      CKL(launch_sym6_to9(c->S, c->scratch, N, c->stream));
       CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
       return 0;
@@ -941,6 +952,29 @@ int dmk_get_counters(dmk_ctx* c, int64_t out[4]) {
   return 0;
 }
 
+int dmk_get_launches(dmk_ctx* c, int64_t* out) {
+  if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
+  *out = c->launches;
+  return 0;
+}
+
+int dmk_timer_start(dmk_ctx* c) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (!c->tev[0]) { CK(cudaEventCreate(&c->tev[0])); CK(cudaEventCreate(&c->tev[1])); }
+  CK(cudaEventRecord(c->tev[0], c->stream));
+  return 0;
+}
+
+int dmk_timer_stop(dmk_ctx* c, double* ms) {
+  if (!c || !ms || !c->tev[0]) return fail(DMK_ERR_ARG, "timer not started");
+  CK(cudaEventRecord(c->tev[1], c->stream));
+  CK(cudaEventSynchronize(c->tev[1]));
+  float f = 0.f;
+  CK(cudaEventElapsedTime(&f, c->tev[0], c->tev[1]));
+  *ms = f;
+  return 0;
+}
+
 int dmk_get_timings(dmk_ctx* c, double out[3]) {
   if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
   for (int k = 0; k < 3; ++k) out[k] = c->last_ms[k];
@@ -962,6 +996,8 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out})
     if (p) cudaFree(p);
   for (auto e : c->ev)
+    if (e) cudaEventDestroy(e);
+  for (auto e : c->tev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
   delete c->pc12;

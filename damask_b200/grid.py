@@ -59,6 +59,10 @@ class SpectralBasic:
         self.init_seconds = time.perf_counter() - t0
         self.ctx = ctx
         self.n_slip = phase.n_slip
+        # running totals over all solution calls: updates, state iterations, Newton
+        # iterations, residual evaluations; and device ms by stage
+        self.total_counters = np.zeros(4, dtype=np.int64)
+        self.total_ms = np.zeros(3)
 
     # -- the plugin procedures ------------------------------------------------------------------
     def forward(self, cutBack: bool, guess: bool, Delta_t: float, Delta_t_old: float, t_remaining: float,
@@ -71,6 +75,8 @@ class SpectralBasic:
     def solution(self) -> SolutionStruct:
         out = SolutionStruct()
         _lib.check(self.lib.dmk_mech_solution(self.ctx, C.byref(out)))
+        self.total_counters += self.counters()
+        self.total_ms += self.timings()
         return out
 
     def materialpoint_forward(self) -> None:
@@ -107,6 +113,19 @@ class SpectralBasic:
         out = np.zeros(3)
         _lib.check(self.lib.dmk_get_timings(self.ctx, _dp(out)))
         return out
+
+    def launches(self) -> int:
+        out = C.c_int64()
+        _lib.check(self.lib.dmk_get_launches(self.ctx, C.byref(out)))
+        return out.value
+
+    def timer_start(self) -> None:
+        _lib.check(self.lib.dmk_timer_start(self.ctx))
+
+    def timer_stop(self) -> float:
+        ms = C.c_double()
+        _lib.check(self.lib.dmk_timer_stop(self.ctx, C.byref(ms)))
+        return ms.value
 
     # -- operator-level entry points --------------------------------------------------------------
     def constitutive_response(self, F: np.ndarray, dt: float):
@@ -172,59 +191,93 @@ class IncrementStats:
     P_av: np.ndarray = field(default_factory=lambda: np.zeros((3, 3)))
 
 
-def run_load_cases(solver, loadcases: list[LoadCase], N_cutback_max: int = 3, max_increments: int | None = None,
-                   on_increment=None, sync=None) -> list[IncrementStats]:
-    """The increment loop of DAMASK_grid (DAMASK_grid.f90:288-460) for one mechanical field.
+class IncrementDriver:
+    """The increment loop of DAMASK_grid (DAMASK_grid.f90:288-460) for one mechanical field,
+    one increment per :meth:`step` call.
 
-    ``solver`` provides forward/solution/materialpoint_forward/update_coords.  Returns one
-    record per converged (sub)increment.  Raises NotConverged like IO_error(950).
+    ``solver`` provides forward/solution/materialpoint_forward/update_coords.  A step
+    runs all (sub)increments of one load-case increment including the global cutback
+    (time step halved up to ``N_cutback_max`` times); it raises NotConverged like
+    IO_error(950).
     """
     sub_step_factor = 2
-    t = 0.0
-    Delta_t = 1.0
-    cut_back_level = 0
-    cut_back = False
-    total = 0
+
+    def __init__(self, solver, loadcases: list[LoadCase], N_cutback_max: int = 3, sync=None):
+        self.solver = solver
+        self.loadcases = loadcases
+        self.N_cutback_max = N_cutback_max
+        self.sync = sync
+        self.t = 0.0
+        self.Delta_t = 1.0
+        self.cut_back_level = 0
+        self.cut_back = False
+        self.total = 0
+        self._l = 0
+        self._inc = 0
+        self._t_0 = 0.0
+        self._guess = loadcases[0].estimate_rate if loadcases else True
+
+    @property
+    def done(self) -> bool:
+        return self._l >= len(self.loadcases)
+
+    def step(self) -> list[IncrementStats]:
+        if self.done:
+            return []
+        lc = self.loadcases[self._l]
+        if self._inc == 0:
+            self._t_0 = self.t
+            self._guess = lc.estimate_rate
+        self._inc += 1
+        inc = self._inc
+        self.total += 1
+        out: list[IncrementStats] = []
+        ssf = self.sub_step_factor
+        Delta_t_prev = self.Delta_t
+        self.Delta_t = lc.t * geometric_fraction(lc.r, inc, lc.N) * float(ssf) ** (-float(self.cut_back_level))
+        step_fraction = 0
+        while step_fraction < ssf ** self.cut_back_level:
+            t_remaining = lc.t + self._t_0 - self.t
+            self.t = self.t + self.Delta_t
+            step_fraction += 1
+            t0 = time.perf_counter()
+            self.solver.forward(self.cut_back, self._guess, self.Delta_t, Delta_t_prev, t_remaining, lc)
+            if not self.cut_back:
+                self.solver.materialpoint_forward()
+            sol = self.solver.solution()
+            if self.sync is not None:
+                self.sync()
+            dt_wall = time.perf_counter() - t0
+            if sol.converged and sol.stagConverged:
+                self.solver.update_coords()
+                Delta_t_prev = self.Delta_t
+                self.cut_back = False
+                self._guess = True
+                out.append(IncrementStats(self.total, self.t, self.cut_back_level, True, sol.iterationsNeeded,
+                                          sol.residualEvals, dt_wall, np.array(sol.P_av[:]).reshape(3, 3, order='F')))
+            elif self.cut_back_level < self.N_cutback_max:
+                self.cut_back = True
+                step_fraction = (step_fraction - 1) * ssf
+                self.cut_back_level += 1
+                self.t = self.t - self.Delta_t
+                self.Delta_t = self.Delta_t / float(ssf)
+            else:
+                raise NotConverged(f'increment {self.total} did not converge after {self.N_cutback_max} cutbacks')
+        self.cut_back_level = max(0, self.cut_back_level - 1)
+        if self._inc >= lc.N:
+            self._l += 1
+            self._inc = 0
+        return out
+
+
+def run_load_cases(solver, loadcases: list[LoadCase], N_cutback_max: int = 3, max_increments: int | None = None,
+                   on_increment=None, sync=None) -> list[IncrementStats]:
+    """Run the whole load-case list (or its first ``max_increments`` increments)."""
+    drv = IncrementDriver(solver, loadcases, N_cutback_max, sync)
     stats: list[IncrementStats] = []
-    for lc in loadcases:
-        t_0 = t
-        guess = lc.estimate_rate
-        for inc in range(1, lc.N + 1):
-            if max_increments is not None and total >= max_increments:
-                return stats
-            total += 1
-            Delta_t_prev = Delta_t
-            Delta_t = lc.t * geometric_fraction(lc.r, inc, lc.N) * float(sub_step_factor) ** (-float(cut_back_level))
-            step_fraction = 0
-            while step_fraction < sub_step_factor ** cut_back_level:
-                t_remaining = lc.t + t_0 - t
-                t = t + Delta_t
-                step_fraction += 1
-                t0 = time.perf_counter()
-                solver.forward(cut_back, guess, Delta_t, Delta_t_prev, t_remaining, lc)
-                if not cut_back:
-                    solver.materialpoint_forward()
-                sol = solver.solution()
-                if sync is not None:
-                    sync()
-                dt_wall = time.perf_counter() - t0
-                if sol.converged and sol.stagConverged:
-                    solver.update_coords()
-                    Delta_t_prev = Delta_t
-                    cut_back = False
-                    guess = True
-                    rec = IncrementStats(total, t, cut_back_level, True, sol.iterationsNeeded, sol.residualEvals,
-                                         dt_wall, np.array(sol.P_av[:]).reshape(3, 3, order='F'))
-                    stats.append(rec)
-                    if on_increment is not None:
-                        on_increment(rec)
-                elif cut_back_level < N_cutback_max:
-                    cut_back = True
-                    step_fraction = (step_fraction - 1) * sub_step_factor
-                    cut_back_level += 1
-                    t = t - Delta_t
-                    Delta_t = Delta_t / float(sub_step_factor)
-                else:
-                    raise NotConverged(f'increment {total} did not converge after {N_cutback_max} cutbacks')
-            cut_back_level = max(0, cut_back_level - 1)
+    while not drv.done and (max_increments is None or drv.total < max_increments):
+        for rec in drv.step():
+            stats.append(rec)
+            if on_increment is not None:
+                on_increment(rec)
     return stats

@@ -181,6 +181,13 @@ int dmk_get_counters(dmk_ctx* ctx, int64_t out[4]);
    constitutive, spectral (FFT + Gamma), other. */
 int dmk_get_timings(dmk_ctx* ctx, double out[3]);
 
+/* Number of kernels of this library launched by the context so far. */
+int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
+/* Device timer on the context's stream: CUDA events recorded at start and stop;
+   stop waits for the stream and returns the elapsed milliseconds. */
+int dmk_timer_start(dmk_ctx* ctx);
+int dmk_timer_stop(dmk_ctx* ctx, double* ms);
+
 void dmk_destroy(dmk_ctx* ctx);
 const char* dmk_last_error(void);
 
