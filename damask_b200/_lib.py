@@ -17,7 +17,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_mech_update_coords', 'dmk_get_field', 'dmk_set_field', 'dmk_field_size', 'dmk_get_aims',
            'dmk_constitutive_response', 'dmk_update_gamma', 'dmk_gamma_convolution', 'dmk_divergence_rms',
            'dmk_dPdF', 'dmk_get_iteration_counts', 'dmk_get_counters', 'dmk_get_timings', 'dmk_destroy',
-           'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop']
+           'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop', 'dmk_phase_schmid',
+           'dmk_phase_interaction']
 
 _lib = None
 
@@ -64,6 +65,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_get_launches': (C.c_int, [vp, C.POINTER(C.c_int64)]),
         'dmk_timer_start': (C.c_int, [vp]),
         'dmk_timer_stop': (C.c_int, [vp, dp]),
+        'dmk_phase_schmid': (C.c_int, [C.POINTER(PhaseStruct), C.c_int, dp]),
+        'dmk_phase_interaction': (C.c_int, [C.POINTER(PhaseStruct), dp]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

@@ -952,6 +952,26 @@ int dmk_get_counters(dmk_ctx* c, int64_t out[4]) {
   return 0;
 }
 
+int dmk_phase_schmid(const dmk_phase* phase, int sense, double* out) {
+  if (!phase || !out || (sense != 1 && sense != -1)) return fail(DMK_ERR_ARG, "invalid argument");
+  HostPhase hp;
+  std::string err;
+  if (build_host_phase(*phase, hp, err)) return fail(DMK_ERR_CONFIG, err);
+  const auto& P = sense > 0 ? hp.Ppos : hp.Pneg;
+  for (int s = 0; s < hp.Ns; ++s)
+    for (int k = 0; k < 9; ++k) out[9 * s + k] = P[s][k];
+  return hp.Ns;
+}
+
+int dmk_phase_interaction(const dmk_phase* phase, double* h) {
+  if (!phase || !h) return fail(DMK_ERR_ARG, "invalid argument");
+  HostPhase hp;
+  std::string err;
+  if (build_host_phase(*phase, hp, err)) return fail(DMK_ERR_CONFIG, err);
+  std::copy(hp.h.begin(), hp.h.end(), h);
+  return hp.Ns;
+}
+
 int dmk_get_launches(dmk_ctx* c, int64_t* out) {
   if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
   *out = c->launches;

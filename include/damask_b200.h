@@ -181,6 +181,14 @@ int dmk_get_counters(dmk_ctx* ctx, int64_t out[4]);
    constitutive, spectral (FFT + Gamma), other. */
 int dmk_get_timings(dmk_ctx* ctx, double out[3]);
 
+/* Host-only phase constants (no device needed), crystal_SchmidMatrix_slip
+   (crystal.f90:1348-1454) and crystal_interaction_SlipBySlip (crystal.f90:591-902):
+   Schmid matrices of the active slip systems (column-major, 9 per system; sense +1/-1,
+   with the non-Schmid terms of the phase) and the Ns x Ns hardening matrix (row =
+   reacting system).  Return the number of systems Ns, or an error code < 0. */
+int dmk_phase_schmid(const dmk_phase* phase, int sense, double* out);
+int dmk_phase_interaction(const dmk_phase* phase, double* h);
+
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 /* Device timer on the context's stream: CUDA events recorded at start and stop;

@@ -1,0 +1,69 @@
+"""Generate ``golden.npz`` from the reference's own Python package.
+
+Run here (where the reference tree is mounted), not on the test machines:
+
+    python tests/golden/make_golden.py /root/reference
+
+The reference package is imported piecewise: its optional I/O dependencies
+(h5py, vtk, matplotlib) are replaced by inert stand-ins because none of the
+functions used here touches them.  Fixtures written:
+
+* ``schmid_cF``, ``schmid_cI``: Schmid matrices ``Crystal.Schmid(N_slip='*')``
+  (``python/damask/_crystal.py``), all slip systems, shape (n, 3, 3);
+* ``seeds_0``, ``quats_0``: 20 seed points in a 1 mm cube and 20 orientations drawn
+  from one generator ``default_rng(0)`` (``seeds.from_random``, ``Rotation.from_random``);
+* ``div_field``, ``div_rms``: a seeded random tensor field on an 8x6x4 grid of size
+  (1, 2, 3) mm and the RMS of its spectral divergence ``grid.divergence``
+  (``python/damask/grid.py:143-167``).
+"""
+import importlib
+import sys
+import types
+from pathlib import Path
+
+import numpy as np
+
+
+def import_reference(root: str):
+    sys.path.insert(0, str(Path(root) / 'python'))
+
+    class _Inert(types.ModuleType):
+        def __getattr__(self, name):
+            if name.startswith('__'):
+                raise AttributeError(name)
+            return type(name, (), {})
+
+    for name in ('h5py', 'vtk', 'vtkmodules', 'matplotlib', 'matplotlib.pyplot', 'PIL'):
+        m = _Inert(name)
+        m.__path__ = []
+        sys.modules[name] = m
+    pkg = types.ModuleType('damask')
+    pkg.__path__ = [str(Path(root) / 'python' / 'damask')]
+    pkg.version = '0'
+    sys.modules['damask'] = pkg
+    rot = importlib.import_module('damask._rotation')
+    pkg.Rotation = rot.Rotation
+    return (rot, importlib.import_module('damask.seeds'), importlib.import_module('damask._crystal'),
+            importlib.import_module('damask.grid'))
+
+
+def main(root: str) -> None:
+    rot, seeds, crystal, grid = import_reference(root)
+    out = {}
+    out['schmid_cF'] = crystal.Crystal(lattice='cF').Schmid(N_slip='*')
+    out['schmid_cI'] = crystal.Crystal(lattice='cI').Schmid(N_slip='*')
+    rng = np.random.default_rng(0)
+    out['seeds_0'] = seeds.from_random([1.0e-3] * 3, 20, rng=rng)
+    out['quats_0'] = rot.Rotation.from_random(20, rng=rng).quaternion
+    size = np.array([1.0e-3, 2.0e-3, 3.0e-3])
+    f = np.random.default_rng(7).normal(size=(8, 6, 4, 3, 3)) * 1.0e8
+    d = grid.divergence(size, f)
+    out['div_field'] = f
+    out['div_size'] = size
+    out['div_rms'] = np.sqrt(np.mean(np.sum(d ** 2, axis=-1)))
+    np.savez_compressed(Path(__file__).with_name('golden.npz'), **out)
+    print({k: np.shape(v) for k, v in out.items()})
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')

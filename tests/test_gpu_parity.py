@@ -1,0 +1,132 @@
+"""CUDA path (libdamask_b200.so, through the C-ABI) against the oracle on the same inputs.
+
+Tolerances: FP64 results within 1e-9 relative (per voxel, relative to the field's
+maximum) with equal fixed-point iteration counts; the mixed-precision form within
+1e-5 relative in the volume-averaged stress.
+"""
+import numpy as np
+import pytest
+
+from damask_b200 import synthetic, workloads
+from damask_b200.grid import SpectralBasic, run_load_cases
+
+from conftest import rel
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-9
+
+
+def pair(oracle_lib, cells, grains, seed=0, phase=None, num=None, size=workloads.SIZE_1MM, precision='fp64'):
+    rve = synthetic.voronoi_rve(cells, size, grains, seed)
+    phase = phase or workloads.fcc_al()
+    num = num or workloads.numerics_default()
+    g = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision)
+    o = oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, threads=4)
+    return g, o
+
+
+def test_init_sweep(gpu, oracle_lib):
+    g, o = pair(oracle_lib, (8, 8, 8), 5)
+    for name in ('F_p', 'F_e', 'xi_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < 1e-14
+    ag, ao = g.aims(), o.aims()
+    assert rel(ag['C_minMaxAvg'], ao['C_minMaxAvg']) < 1e-12
+    assert rel(ag['C_volAvg'], ao['C_volAvg']) < 1e-12
+    g.close()
+
+
+@pytest.mark.parametrize('phase', [workloads.fcc_al(), workloads.bcc_24()], ids=['fcc12', 'bcc24'])
+def test_constitutive_response_and_tangent(gpu, oracle_lib, phase):
+    """utilities_constitutiveResponse and phase_mechanical_dPdF in the plastic range."""
+    g, o = pair(oracle_lib, (6, 5, 4), 4, phase=phase)
+    rng = np.random.default_rng(11)
+    F = np.eye(3) + np.diag([4e-3, -1.5e-3, -1.5e-3])
+    Fs = np.tile(F.reshape(-1, order='F'), (g.N, 1)) + 2e-4 * rng.normal(size=(g.N, 9))
+    Pg, Pavg, Cvg, Cmg, stg = g.constitutive_response(Fs, 1.0)
+    Po, Pavo, Cvo, Cmo, sto = o.constitutive_response(Fs, 1.0)
+    assert stg == sto == 0
+    assert np.abs(Po).max() > 5e7                 # plastic
+    assert rel(Pg, Po) < TOL and rel(Pavg, Pavo) < TOL
+    assert rel(Cvg, Cvo) < TOL and rel(Cmg, Cmo) < TOL
+    for name in ('F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'F_e'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    assert rel(g.dPdF(1.0), o.dPdF(1.0)) < TOL
+    it = g.iteration_counts()
+    assert it[:, 0].min() >= 1 and it[:, 1].min() >= 1 and np.all(it[:, 3] == 0)
+    g.close()
+
+
+def test_failure_status_matches(gpu, oracle_lib):
+    num = workloads.numerics_default()
+    num.N_iter_Lp_max = 1
+    g, o = pair(oracle_lib, (2, 2, 2), 2, num=num)
+    F = np.tile((np.eye(3) + np.diag([5e-3, -2e-3, -2e-3])).reshape(-1, order='F'), (g.N, 1))
+    stg = g.constitutive_response(F, 1.0)[-1]
+    sto = o.constitutive_response(F, 1.0)[-1]
+    assert stg != 0 and sto != 0
+    g.close()
+
+
+def test_spectral_operators(gpu, oracle_lib, golden):
+    num = workloads.numerics_default()
+    num.divergence_correction = 'size'
+    f = golden['div_field']
+    g, o = pair(oracle_lib, f.shape[:3], 3, num=num, size=tuple(golden['div_size']))
+    P = f.transpose(2, 1, 0, 4, 3).reshape(-1, 9)
+    assert rel(g.divergence_rms(P), golden['div_rms']) < 1e-12      # reference python/damask/grid.py
+    aim = np.random.default_rng(2).normal(size=9)
+    assert rel(g.gamma_convolution(P, aim), o.gamma_convolution(P, aim)) < 1e-12
+    g.close()
+
+
+def run_both(g, o, n):
+    sg = run_load_cases(g, workloads.tension_x(60.0, 60), max_increments=n)
+    so = run_load_cases(o, workloads.tension_x(60.0, 60), max_increments=n)
+    return sg, so
+
+
+@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson'])
+def test_solver_parity(gpu, oracle_lib, case):
+    """grid_mechanical_spectral_basic_{forward,solution} + materialpoint_forward over several
+    increments of uniaxial tension: per-voxel fields within 1e-9, identical iteration counts."""
+    num = workloads.numerics_default()
+    if case == 'fcc16_anderson':
+        g, o, n = *pair(oracle_lib, (16, 16, 16), 20), 3
+    elif case == 'fcc8_richardson':
+        num.PETSc_options = '-snes_type nrichardson'
+        g, o, n = *pair(oracle_lib, (8, 8, 8), 6, num=num), 3
+    else:
+        g, o, n = *pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_24()), 2
+    sg, so = run_both(g, o, n)
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    for a, b in zip(sg, so):
+        assert rel(a.P_av, b.P_av) < TOL
+    for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    assert rel(g.aims()['C_volAvg'], o.aims()['C_volAvg']) < TOL
+    g.close()
+
+
+def test_mixed_precision_within_1e5(gpu, oracle_lib):
+    """FP32 FFT/Gamma/field update with the FP64 correction sweep: <P> within 1e-5 of FP64."""
+    rve = synthetic.voronoi_rve((16, 16, 16), workloads.SIZE_1MM, 12, 3)
+    ph, num = workloads.bcc_24(), workloads.numerics_default()
+    res = {}
+    for prec in ('fp64', 'mixed'):
+        s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, ph, num, precision=prec)
+        res[prec] = (run_load_cases(s, workloads.tension_x(100.0, 100), max_increments=3), s.get_field('P'))
+        s.close()
+    for a, b in zip(res['mixed'][0], res['fp64'][0]):
+        assert rel(a.P_av, b.P_av) < 1e-5
+    assert rel(res['mixed'][1], res['fp64'][1]) < 1e-5
+
+
+def test_field_access_roundtrip(gpu, oracle_lib):
+    g, _ = pair(oracle_lib, (4, 3, 2), 2)
+    F = np.tile(np.eye(3).reshape(-1, order='F'), (g.N, 1)) + 1e-3 * np.arange(g.N * 9).reshape(g.N, 9) / g.N
+    g.set_field('F_solver', F)
+    assert np.array_equal(g.get_field('F_solver'), F)
+    assert g.get_field('xi_sl').shape == (g.N, 12)
+    assert np.array_equal(g.get_field('F_i'), np.tile(np.eye(3).reshape(-1), (g.N, 1)))
+    g.close()

@@ -1,0 +1,189 @@
+"""Host-side logic: input formats, the increment driver, the C-ABI surface, multi-rank reductions."""
+import ctypes as C
+import os
+import re
+import socket
+from pathlib import Path
+
+import numpy as np
+import pytest
+import yaml
+
+from damask_b200 import _lib, config, workloads
+from damask_b200.config import Numerics, Phase, parse_load
+from damask_b200.grid import NotConverged, run_load_cases
+
+ROOT = Path(__file__).resolve().parent.parent
+
+LOAD = """
+solver:
+  mechanical: spectral_basic
+loadstep:
+  - boundary_conditions:
+      mechanical:
+        dot_F: [[1.0e-3, 0, 0], [0, x, 0], [0, 0, x]]
+        P: [[x, x, x], [x, 0, x], [x, x, 0]]
+    discretization: {t: 10, N: 40}
+    f_out: 4
+  - boundary_conditions:
+      mechanical:
+        F: [[1.1, 0, 0], [0, 1, 0], [0, 0, 1]]
+        R: [0, 0, 1, 90]
+    discretization: {t: 60, N: 60, r: 1.05}
+    estimate_rate: false
+    f_out: none
+"""
+
+
+def test_parse_load_cases():
+    lc = parse_load(yaml.safe_load(LOAD))
+    assert len(lc) == 2
+    a, b = lc
+    assert a.deformation_type == 'dot_F' and a.stress_type == 'P'
+    assert a.deformation_mask[1, 1] and a.deformation_mask[2, 2] and not a.deformation_mask[0, 0]
+    assert not a.stress_mask[1, 1] and a.stress_mask[0, 0]
+    assert a.t == 10 and a.N == 40 and a.f_out == 4 and a.estimate_rate
+    assert b.deformation_type == 'F' and b.stress_type is None and not b.estimate_rate
+    assert b.f_out == 2 ** 31 - 1 and b.r == 1.05
+    # R: 90 degrees about z, tRotation%fromAxisAngle with P = -1
+    assert np.allclose(b.q_rot, [np.cos(np.pi / 4), 0, 0, np.sin(np.pi / 4)])
+    bc = a.deformation_bc()
+    assert bc.type == 2 and bc.values[0] == 1e-3 and bc.mask[4] == 1
+
+
+def test_geometric_fraction_sums_to_one():
+    for r in (1.0, 1.05, 0.9):
+        assert abs(sum(config.geometric_fraction(r, i, 37) for i in range(1, 38)) - 1.0) < 1e-12
+
+
+def test_numerics_from_yaml_and_validation():
+    n = Numerics.from_dict({'solver': {'grid': {'N_cutback_max': 2, 'mechanical': {
+        'N_iter_min': 2, 'eps_rel_div(P)': 1e-4, 'PETSc_options': '-snes_type nrichardson'}}},
+        'phase': {'mechanical': {'N_iter_state_max': 10, 'plastic': {'N_iter_Lp_max': 20}}}})
+    assert n.N_iter_min == 2 and n.eps_rel_div == 1e-4 and n.N_cutback_max == 2
+    assert n.N_iter_state_max == 10 and n.N_iter_Lp_max == 20 and n.snes_type == 0
+    s = n.to_struct()
+    assert s.eps_rel_Li == n.eps_rel_Lp and s.snes_type == 0
+    assert Numerics().snes_type == 1          # reference default -snes_type ngmres -> accelerated
+    with pytest.raises(ValueError):
+        Numerics(N_iter_min=5, N_iter_max=2).to_struct()
+    with pytest.raises(ValueError):
+        Numerics(PETSc_options='-snes_type newtonls').to_struct()
+
+
+def test_phase_rejects_unsupported():
+    d = yaml.safe_load("""
+lattice: cF
+mechanical:
+  elastic: {type: Hooke, C_11: 1e11, C_12: 6e10, C_44: 3e10}
+  plastic: {type: dislotwin}
+""")
+    with pytest.raises(ValueError):
+        Phase.from_dict(d)
+
+
+class FakeSolver:
+    """Scripted solver: fails the solutions listed in `fail_at` (call index)."""
+
+    def __init__(self, fail_at):
+        self.fail_at = set(fail_at)
+        self.calls = []
+        self.n = 0
+
+    def forward(self, cutBack, guess, dt, dt_old, t_rem, lc):
+        self.calls.append(('forward', cutBack, guess, round(dt, 12), round(dt_old, 12)))
+
+    def materialpoint_forward(self):
+        self.calls.append(('mp_forward',))
+
+    def solution(self):
+        from damask_b200.config import SolutionStruct
+        s = SolutionStruct()
+        s.converged = int(self.n not in self.fail_at)
+        s.stagConverged = 1
+        s.iterationsNeeded = 3
+        s.residualEvals = 4
+        self.n += 1
+        return s
+
+    def update_coords(self):
+        pass
+
+
+def test_driver_cutback_semantics():
+    """DAMASK_grid.f90:288-460: a failed increment halves Delta_t (cutBack=.true., no
+    materialpoint_forward), the substeps of the level complete it, and the next
+    increment starts one cutback level lower."""
+    lc = workloads.tension_x(4.0, 4)
+    s = FakeSolver(fail_at=[1])
+    stats = run_load_cases(s, lc, max_increments=3)
+    forwards = [c for c in s.calls if c[0] == 'forward']
+    assert forwards[0] == ('forward', False, True, 1.0, 1.0)      # inc 1, guess from estimate_rate
+    assert forwards[1] == ('forward', False, True, 1.0, 1.0)      # inc 2 first try
+    assert forwards[2] == ('forward', True, True, 0.5, 1.0)       # cut back: dt/2, no mp_forward
+    assert forwards[3] == ('forward', False, True, 0.5, 0.5)      # second substep
+    assert forwards[4] == ('forward', False, True, 1.0, 0.5)      # inc 3 back at level 0
+    assert [st.t for st in stats] == [1.0, 1.5, 2.0, 3.0]
+    assert sum(1 for c in s.calls if c[0] == 'mp_forward') == 4
+
+
+def test_driver_gives_up_after_max_cutbacks():
+    s = FakeSolver(fail_at=range(1, 100))
+    with pytest.raises(NotConverged):
+        run_load_cases(s, workloads.tension_x(4.0, 4), N_cutback_max=3)
+    assert s.n == 5          # first increment + 4 tries of the second (levels 0..3)
+
+
+def test_library_exports_every_declared_symbol():
+    header = (ROOT / 'include' / 'damask_b200.h').read_text()
+    names = set(re.findall(r'\b(dmk_[A-Za-z0-9_]+)\s*\(', header))
+    assert len(names) >= 20
+    lib = C.CDLL(str(_lib.LIB_PATH))
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(_lib.EXPORTS) <= names
+
+
+def test_product_path_has_no_fallback(monkeypatch, tmp_path):
+    """Without the CUDA library the product raises instead of computing elsewhere."""
+    monkeypatch.setattr(_lib, '_lib', None)
+    with pytest.raises(RuntimeError, match='no CPU fallback'):
+        _lib.load(tmp_path / 'missing.so')
+
+
+def _free_port():
+    s = socket.socket()
+    s.bind(('127.0.0.1', 0))
+    p = s.getsockname()[1]
+    s.close()
+    return p
+
+
+def _rank_main(rank, world, port, q):
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    import datetime
+    import sys
+    import torch.distributed as dist
+    sys.path.insert(0, str(ROOT))
+    import bench
+    dist.init_process_group('gloo', rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
+    bench.barrier(world)
+    mx = bench.allreduce_max(10.0 + rank, world)
+    sm = bench.allreduce_sum(100.0 * (rank + 1), world)
+    dist.destroy_process_group()
+    q.put((rank, mx, sm))
+
+
+def test_replica_reductions_two_ranks():
+    """bench.py reports updates summed over replicas and the time of the slowest replica."""
+    import multiprocessing as mp
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_rank_main, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res = sorted(q.get(timeout=120) for _ in procs)
+    for p in procs:
+        p.join(timeout=60)
+    assert res == [(0, 11.0, 300.0), (1, 11.0, 300.0)]

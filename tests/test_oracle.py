@@ -1,0 +1,145 @@
+"""The oracle (CPU FP64 restatement) against the reference's golden vectors and the
+invariants its own self-tests check (spectral_utilities.f90:974-1108, math.f90:1240-1410)."""
+import numpy as np
+import pytest
+
+from damask_b200 import synthetic, workloads
+from damask_b200.config import Numerics
+from damask_b200.grid import run_load_cases
+
+from conftest import rel
+
+
+def small_oracle(oracle_lib, cells=(4, 4, 4), grains=3, seed=0, phase=None, num=None, size=workloads.SIZE_1MM,
+                 init=True):
+    rve = synthetic.voronoi_rve(cells, size, grains, seed)
+    return oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions,
+                                          phase or workloads.fcc_al(), num or workloads.numerics_default(),
+                                          threads=2, init=init)
+
+
+def test_seeds_and_rotations_match_reference(golden):
+    rng = np.random.default_rng(0)
+    s = synthetic.seeds_from_random([1.0e-3] * 3, 20, rng)
+    q = synthetic.rotations_from_random(20, rng)
+    assert np.array_equal(s, golden['seeds_0'])
+    assert np.allclose(q, golden['quats_0'], rtol=0, atol=1e-15)
+
+
+def test_fft_matches_numpy(oracle_lib):
+    x = np.random.default_rng(1).normal(size=(6, 5, 8)) + 1j * np.random.default_rng(2).normal(size=(6, 5, 8))
+    assert rel(oracle_lib.fft3(x, -1), np.fft.fftn(x)) < 1e-13
+    assert rel(oracle_lib.fft3(x, +1), np.fft.ifftn(x) * x.size) < 1e-13
+
+
+def test_divergence_rms_matches_reference_numpy(golden, oracle_lib):
+    """utilities_divergenceRMS with divergence_correction 'size' is the RMS of the
+    spectral divergence field computed by the reference's python/damask/grid.py."""
+    f = golden['div_field']                        # [x, y, z, 3, 3]
+    num = workloads.numerics_default()
+    num.divergence_correction = 'size'
+    o = small_oracle(oracle_lib, cells=f.shape[:3], size=tuple(golden['div_size']), num=num, init=False)
+    P = f.transpose(2, 1, 0, 4, 3).reshape(-1, 9)   # voxel-major, x fastest; column-major tensor
+    assert rel(o.divergence_rms(P), golden['div_rms']) < 1e-12
+
+
+def test_divergence_of_constant_field_vanishes(oracle_lib):
+    o = small_oracle(oracle_lib, cells=(5, 4, 6), init=False)
+    P = np.tile(np.random.default_rng(3).normal(size=9) * 1e8, (o.N, 1))
+    assert o.divergence_rms(P) < 5e-14 * 1e8
+
+
+def test_gamma_convolution_of_constant_field_is_aim(oracle_lib):
+    o = small_oracle(oracle_lib, cells=(4, 6, 5))
+    field = np.tile(np.random.default_rng(4).normal(size=9), (o.N, 1))
+    aim = np.random.default_rng(5).normal(size=9)
+    out = o.gamma_convolution(field, aim)
+    assert np.abs(out - aim).max() < 1e-13
+
+
+def test_gamma_is_projection_of_compatible_part(oracle_lib):
+    """Gamma applied to C_ref : grad(u) returns grad(u) (Gamma^0 C^0 is the projector on
+    compatible fields); the C2R of the unnormalised transform carries the 1/N of C_ref."""
+    o = small_oracle(oracle_lib, cells=(8, 8, 8))
+    C = o.aims()['C_minMaxAvg'].reshape(3, 3, 3, 3, order='F')
+    n = 8
+    x = (np.arange(n) + 0.5) / n * 1.0e-3
+    X, Y, Z = np.meshgrid(x, x, x, indexing='ij')
+    k = 2 * np.pi / 1.0e-3
+    # displacement u = a sin(k x) + b cos(2 k y) with gradient H = du/dX
+    H = np.zeros((n, n, n, 3, 3))
+    a, b = np.array([1e-4, 2e-4, -1e-4]), np.array([-3e-5, 1e-4, 5e-5])
+    H[..., :, 0] = a[None, None, None, :] * (k * np.cos(k * X))[..., None]
+    H[..., :, 1] = b[None, None, None, :] * (-2 * k * np.sin(2 * k * Y))[..., None]
+    tau = np.einsum('ijkl,xyzkl->xyzij', C, H)
+    field = tau.transpose(2, 1, 0, 4, 3).reshape(-1, 9)
+    out = o.gamma_convolution(field, np.zeros(9))
+    expect = H.transpose(2, 1, 0, 4, 3).reshape(-1, 9)
+    assert rel(out, expect) < 1e-12
+
+
+def test_hooke_small_strain(oracle_lib):
+    """At dt = 0 the response is elastic: P ~= C : eps for a small symmetric strain (cubic C)."""
+    ph = workloads.fcc_al()
+    o = small_oracle(oracle_lib, cells=(2, 2, 2), grains=1, phase=ph)
+    eps = np.array([[1e-5, 2e-6, 0], [2e-6, -3e-6, 1e-6], [0, 1e-6, 4e-6]])
+    F = np.tile((np.eye(3) + eps).reshape(-1, order='F'), (o.N, 1))
+    P, P_av, Cv, Cm, st = o.constitutive_response(F, 0.0)
+    assert st == 0
+    C = Cv.reshape(3, 3, 3, 3, order='F')
+    lin = np.einsum('ijkl,kl->ij', C, eps)
+    assert rel(P_av.reshape(3, 3, order='F'), lin) < 2e-5     # geometric nonlinearity ~ |eps|
+
+
+def _fd_tangent(o, F0, dt, h):
+    fd = np.zeros((3, 3, 3, 3))
+    for k in range(3):
+        for l in range(3):
+            Fp, Fm = F0.copy(), F0.copy()
+            Fp[k, l] += h
+            Fm[k, l] -= h
+            Pp = o.constitutive_response(np.tile(Fp.reshape(-1, order='F'), (o.N, 1)), dt)[0][0].reshape(3, 3, order='F')
+            Pm = o.constitutive_response(np.tile(Fm.reshape(-1, order='F'), (o.N, 1)), dt)[0][0].reshape(3, 3, order='F')
+            fd[:, :, k, l] = (Pp - Pm) / (2 * h)
+    return fd
+
+
+@pytest.mark.parametrize('dt,F_pert,tol', [
+    # elastic (dt = 0): the tangent is exact
+    (0.0, [[1e-4, 1e-5, 0], [0, -3e-5, 2e-5], [1e-5, 0, -3e-5]], 1e-6),
+    # plastic: phase_mechanical_dPdF holds the slip resistance fixed and the Lp Newton stops at
+    # eps_rel_Lp = 1e-6, so central differences agree to about 1e-3
+    (1.0, [[4e-3, 1e-4, 0], [0, -1.2e-3, 2e-4], [1e-4, 0, -1.3e-3]], 5e-3)])
+def test_tangent_matches_finite_differences(oracle_lib, dt, F_pert, tol):
+    o = small_oracle(oracle_lib, cells=(1, 1, 2), grains=1, phase=workloads.fcc_al())
+    F0 = np.eye(3) + np.array(F_pert)
+    P, *_, st = o.constitutive_response(np.tile(F0.reshape(-1, order='F'), (o.N, 1)), dt)
+    assert st == 0
+    D = o.dPdF(dt)[0].reshape(3, 3, 3, 3, order='F')
+    fd = _fd_tangent(o, F0, dt, 1e-7 if dt == 0.0 else 1e-8)
+    if dt > 0:
+        assert np.abs(P[0]).max() > 5e7                      # plastic flow at this strain
+    assert rel(D, fd) < tol
+
+
+@pytest.mark.parametrize('snes', ['', '-snes_type nrichardson'])
+def test_small_run_converges(oracle_lib, snes):
+    num = workloads.numerics_default()
+    num.PETSc_options = snes
+    o = small_oracle(oracle_lib, cells=(6, 6, 6), grains=4, num=num)
+    stats = run_load_cases(o, workloads.tension_x(60.0, 60), max_increments=4)
+    assert len(stats) == 4 and all(s.converged for s in stats)
+    Pxx = [s.P_av[0, 0] for s in stats]
+    assert all(b > a for a, b in zip(Pxx, Pxx[1:]))          # hardening under tension
+    assert abs(stats[-1].P_av[1, 1]) < 1e3 + 1e-3 * Pxx[-1]   # lateral stress BC held
+
+
+def test_state_loop_bound_is_honoured(oracle_lib):
+    """N_iter_Lp_max = 1 makes integrateStress fail (STATUS_..._LP_MAXIT) in the plastic range;
+    the substep cutback then fails below r_cutback_min and the solution reports no convergence."""
+    num = workloads.numerics_default()
+    num.N_iter_Lp_max = 1
+    o = small_oracle(oracle_lib, cells=(2, 2, 2), grains=2, num=num)
+    F = np.tile((np.eye(3) + np.diag([5e-3, -2e-3, -2e-3])).reshape(-1, order='F'), (o.N, 1))
+    *_, st = o.constitutive_response(F, 1.0)
+    assert st != 0
