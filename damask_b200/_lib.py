@@ -18,7 +18,7 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_constitutive_response', 'dmk_update_gamma', 'dmk_gamma_convolution', 'dmk_divergence_rms',
            'dmk_dPdF', 'dmk_get_iteration_counts', 'dmk_get_counters', 'dmk_get_timings', 'dmk_destroy',
            'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop', 'dmk_phase_schmid',
-           'dmk_phase_interaction']
+           'dmk_phase_interaction', 'dmk_field_mean_noalloc']
 
 _lib = None
 
@@ -67,6 +67,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_timer_stop': (C.c_int, [vp, dp]),
         'dmk_phase_schmid': (C.c_int, [C.POINTER(PhaseStruct), C.c_int, dp]),
         'dmk_phase_interaction': (C.c_int, [C.POINTER(PhaseStruct), dp]),
+        'dmk_field_mean_noalloc': (C.c_int, [C.c_void_p, C.c_int64, dp, C.c_void_p]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

@@ -50,6 +50,10 @@ int dalloc(T** p, size_t n) {
 
 }  // namespace
 
+namespace dmk {
+void set_last_error(const std::string& msg) { g_err = msg; }
+}  // namespace dmk
+
 struct dmk_ctx {
   int device = 0;
   int nsm = 148;

@@ -196,6 +196,22 @@ int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 int dmk_timer_start(dmk_ctx* ctx);
 int dmk_timer_stop(dmk_ctx* ctx, double* ms);
 
+/* Volume average <f> of a 9-component field that the caller already holds in device
+   memory (9 planes of n_voxels doubles: component c of voxel v at field[c*n_voxels + v]),
+   written to mean[9] on the host.  No counterpart in the reference: it exists for hosts
+   that may not allocate device memory at the time they need the average (a solver loop
+   confined to a memory arena its framework handed out, or a loop where an allocation
+   and its implicit device synchronisation are not allowed).  It allocates nothing: its
+   partial sums live in a fixed 1.13 MiB device array that every GPU loading the library
+   holds until the process exits.  n_voxels is limited to 16,777,216 (256^3); larger
+   sizes are rejected with DMK_ERR_ARG.  The first call on a device looks up that array's
+   device address (once per device, with the device current); make that first call
+   before any stream capture.  All calls share the array: calls that overlap on the GPU
+   (different streams or threads) race; each call overwrites what it uses, so no state
+   carries over.  stream: a cudaStream_t, or NULL for the default stream; the call waits
+   for the result. */
+int dmk_field_mean_noalloc(const double* field, int64_t n_voxels, double mean[9], void* stream);
+
 void dmk_destroy(dmk_ctx* ctx);
 const char* dmk_last_error(void);
 
