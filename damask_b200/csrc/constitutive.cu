@@ -1,0 +1,196 @@
+// Pass kernels of the constitutive update (see constitutive.cuh for the scheme).
+//
+//  constitutive_begin_kernel  every voxel: fused field update F <- F - r, phase restore
+//                             (mechanical_restore), substep set-up, then control up to
+//                             the first integrateStress.
+//  constitutive_pass_kernel   every voxel of the list: one integrateStress and the state
+//                             update / substep control up to the next one; voxels that
+//                             continue are appended to the next list.
+#include "kernels.cuh"
+#include "constitutive.cuh"
+
+namespace dmk {
+
+namespace {
+
+// voxel finished: iteration record and worst status
+__device__ __forceinline__ void finish_voxel(const Fields& f, int64_t v, const VoxelCtl& c) {
+  const int64_t N = f.N;
+  if (f.iter) {
+    f.iter[v] = c.nstate;
+    f.iter[N + v] = c.newton;
+    f.iter[2 * N + v] = c.nsub;
+    f.iter[3 * N + v] = c.status;
+  }
+  if (c.status != 0) atomicMax(f.status, 2);               // STATUS_FAIL_PHASE_MECHANICAL
+}
+
+// warp-aggregated append of the continuing voxels and of the iteration counters;
+// every thread of the block reaches this point
+__device__ __forceinline__ void append_and_count(const Fields& f, const PassWork& w, bool keep, int64_t v, int dstate,
+                                                 int dnewton) {
+  const unsigned full = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const unsigned m = __ballot_sync(full, keep);
+  if (m) {
+    const int leader = __ffs(m) - 1;
+    int base = 0;
+    if (lane == leader) base = atomicAdd(w.count_out, __popc(m));
+    base = __shfl_sync(full, base, leader);
+    if (keep) w.list_out[base + __popc(m & ((1u << lane) - 1u))] = int(v);
+  }
+  unsigned long long cs = dstate, cn = dnewton;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cs += __shfl_down_sync(full, cs, o);
+    cn += __shfl_down_sync(full, cn, o);
+  }
+  if (lane == 0 && f.counters && (cs | cn)) {
+    atomicAdd(&f.counters[1], cs);
+    atomicAdd(&f.counters[2], cn);
+  }
+}
+
+}  // namespace
+
+template <int NS>
+__global__ void __launch_bounds__(PASS_THREADS)
+constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
+                          const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
+                          int apply_update) {
+  extern __shared__ double slots[];
+  constexpr int NST = 2 * NS;
+  double* xs = slots + threadIdx.x;
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t N = f.N;
+  bool keep = false;
+  if (v < N) {
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      double x = f.Fsol[k * N + v];
+      if (apply_update) {
+        x = x - f.r[k * N + v];
+        f.Fsol[k * N + v] = x;
+      }
+      f.F[k * N + v] = x;
+      const double fp0 = f.Fp0[k * N + v];
+      f.Fp[k * N + v] = fp0;                               // mechanical_restore: Fp := Fp0
+      w.Fp0s[k * N + v] = fp0;                             // subFp0 = Fp0
+      w.F0s[k * N + v] = f.F0[k * N + v];                  // subF0 = F0
+      w.Lp0s[k * N + v] = f.Lp0[k * N + v];                // subLp0 = Lp0 (Lp itself is kept as warm start)
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) f.S[k * N + v] = f.S0[k * N + v];
+    for (int i = 0; i < NST; ++i) {
+      const double s = f.state0[i * N + v];
+      f.state[i * N + v] = s;
+      w.st0s[i * N + v] = s;
+    }
+    VoxelCtl c;
+    c.phase = PH_CTRL;
+    c.status = 1;                                          // STATUS_ITERATING: first control step sets subStep = 1
+    c.it = 0;
+    c.nsub = 0;
+    c.nstate = 0;
+    c.newton = 0;
+    c.stepFrac = 0.0;
+    c.step = 1.0 / nm.r_cutback;
+    advance<NS>(pc, nm, f, w, v, dt, c, xs);
+    store_ctl(w, N, v, c);
+    keep = c.phase == PH_STRESS;
+    if (!keep) finish_voxel(f, v, c);
+  }
+  append_and_count(f, w, keep, v, 0, 0);
+}
+
+template <int NS>
+__global__ void __launch_bounds__(PASS_THREADS)
+constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
+                         const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
+                         const int* __restrict__ list_in, int64_t n_in) {
+  extern __shared__ double slots[];
+  double* xs = slots + threadIdx.x;
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t N = f.N;
+  bool keep = false;
+  int64_t v = 0;
+  int dstate = 0, dnewton = 0;
+  if (idx < n_in) {
+    v = list_in[idx];
+    VoxelCtl c;
+    load_ctl(w, N, v, c);
+    // one state iteration: integrateStress (integrateStateFPI:626-629)
+    ++c.it;
+    ++c.nstate;
+    dstate = 1;
+    double F[9], Fp0[9], Lp[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) {
+      F[k] = w.Fs[k * N + v];
+      Fp0[k] = w.Fp0s[k * N + v];
+      Lp[k] = f.Lp[k * N + v];
+    }
+#pragma unroll
+    for (int s = 0; s < NS; ++s) xs[s * PASS_THREADS] = 1.0 / f.state[s * N + v];
+    double S[6], Fp[9], P[9], Fe[9];
+    const int st = integrate_stress<NS>(pc, nm, F, Fp0, xs, c.step * dt, Lp, S, Fp, P, Fe, dnewton);
+    c.newton += dnewton;
+    if (st != 0) {
+      c.status = st;
+      c.phase = PH_CTRL;
+    } else {
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        f.Lp[k * N + v] = Lp[k];
+        f.Fp[k * N + v] = Fp[k];
+        f.P[k * N + v] = P[k];
+        f.Fe[k * N + v] = Fe[k];
+      }
+#pragma unroll
+      for (int k = 0; k < 6; ++k) f.S[k * N + v] = S[k];
+      c.status = 0;
+      c.phase = PH_DOT1;
+    }
+    advance<NS>(pc, nm, f, w, v, dt, c, xs);
+    store_ctl(w, N, v, c);
+    keep = c.phase == PH_STRESS;
+    if (!keep) finish_voxel(f, v, c);
+  }
+  append_and_count(f, w, keep, v, dstate, dnewton);
+}
+
+template <int NS>
+cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
+                                      const PassWork& w, double dt, int apply_update, cudaStream_t s) {
+  const size_t smem = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const int nb = int((f.N + PASS_THREADS - 1) / PASS_THREADS);
+  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update);
+  return cudaGetLastError();
+}
+
+template <int NS>
+cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
+  const size_t smem = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(constitutive_pass_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  const int nb = int((n_in + PASS_THREADS - 1) / PASS_THREADS);
+  constitutive_pass_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  return cudaGetLastError();
+}
+
+#define DMK_INSTANTIATE(NS)                                                                                         \
+  template cudaError_t launch_constitutive_begin<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,          \
+                                                     const PassWork&, double, int, cudaStream_t);                   \
+  template cudaError_t launch_constitutive_pass<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,           \
+                                                    const PassWork&, double, const int*, int64_t, cudaStream_t);
+DMK_INSTANTIATE(12)
+DMK_INSTANTIATE(18)
+DMK_INSTANTIATE(24)
+#undef DMK_INSTANTIATE
+
+}  // namespace dmk

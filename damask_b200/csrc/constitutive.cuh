@@ -1,5 +1,5 @@
-// Per-voxel constitutive update of the DAMASK grid hot path, one thread per
-// material point, FP64.
+// Per-voxel constitutive update of the DAMASK grid hot path, FP64, one thread per
+// material point, organised as passes over the voxels that still iterate.
 //
 // Restates, for one constituent with pass/isostrain homogenization (F_phase =
 // F_cell, homogenization_mechanical.f90:94-123) and Hooke + phenopowerlaw slip:
@@ -18,66 +18,80 @@
 // collapses to  J[kl][pb] = delta + dt * sum_s dgamma_s P_s(k,l) (A^T Fe Q_s)(p,b)
 // with A = F Fp0^-1 and Q_s = C : P_nS_s precomputed per phase, so no 3x3x3x3
 // temporaries are formed.
+//
+// Execution model.  The nested loops of the reference (substeps > state
+// iterations > Newton iterations) are split at the state iteration: one pass
+// performs, for every voxel still iterating, exactly one integrateStress (the Newton
+// loop, in registers) followed by the state update and whatever substep control
+// leads to the next integrateStress.  Between passes the per-voxel iteration state
+// lives in HBM planes (PassWork), so the large per-system arrays of the state
+// iteration are never live during the Newton loop; all indexing into register
+// arrays is static, and the 9x9 Newton system is solved by Householder QR
+// (backward stable without a data-dependent row exchange).
 #pragma once
 #include "dmk_device.cuh"
 
 namespace dmk {
 
-// kinetics_sl without derivative; returns |dot_gamma| per system
-template <int NS>
-__device__ __forceinline__ void kinetics_abs(const PhaseConst<NS>& pc, const double s6[6], const double* xi, double* adg) {
-#pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
-    const double tmax = tp > tn ? tp : tn;
-    adg[s] = fabs(pc.dg0[s] * powr(tmax / xi[s], pc.n[s], pc.n_int[s]));
-  }
+__device__ __forceinline__ void load_ctl(const PassWork& w, int64_t N, int64_t v, VoxelCtl& c) {
+  c.phase = w.ctl[v];
+  c.status = w.ctl[N + v];
+  c.it = w.ctl[2 * N + v];
+  c.nsub = w.ctl[3 * N + v];
+  c.nstate = w.ctl[4 * N + v];
+  c.newton = w.ctl[5 * N + v];
+  c.stepFrac = w.sub[v];
+  c.step = w.sub[N + v];
+}
+__device__ __forceinline__ void store_ctl(const PassWork& w, int64_t N, int64_t v, const VoxelCtl& c) {
+  w.ctl[v] = c.phase;
+  w.ctl[N + v] = c.status;
+  w.ctl[2 * N + v] = c.it;
+  w.ctl[3 * N + v] = c.nsub;
+  w.ctl[4 * N + v] = c.nstate;
+  w.ctl[5 * N + v] = c.newton;
+  w.sub[v] = c.stepFrac;
+  w.sub[N + v] = c.step;
 }
 
-// phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0)
-template <int NS>
-__device__ __forceinline__ void dot_state(const PhaseConst<NS>& pc, const double s6[6], const double* st, double* dot) {
-  double adg[NS];
-  kinetics_abs<NS>(pc, s6, st, adg);
+// Solves J x = b for a row-major 9x9 J (overwritten with R) by Householder QR:
+// column k is reflected onto alpha e_k with alpha = -sign(x0) |x|, v = x - alpha e_k,
+// H y = y + v (v.y) / (alpha v0).  Returns true when a column of the remaining
+// matrix is exactly zero (the matrix is singular; dgesv info > 0).
+__device__ __forceinline__ bool qr_solve9(double* J, double* b) {
 #pragma unroll
-  for (int l = 0; l < NS; ++l) {
-    const double x = 1.0 - st[l] / pc.xiinf[l];
-    const double left = copysign(powr(fabs(x), pc.a[l], pc.a_int[l]), x);
-    double hg = 0.0;
+  for (int k = 0; k < 8; ++k) {
+    double s2 = 0.0;
 #pragma unroll
-    for (int k = 0; k < NS; ++k) hg = fma(pc.h[l][k], adg[k], hg);
-    dot[l] = pc.h0f[l] * left * hg;
-    dot[NS + l] = adg[l];
+    for (int i = k; i < 9; ++i) s2 = fma(J[i * 9 + k], J[i * 9 + k], s2);
+    if (s2 == 0.0) return true;
+    const double sig = sqrt(s2);
+    const double x0 = J[k * 9 + k];
+    const double alpha = x0 >= 0.0 ? -sig : sig;
+    const double v0 = x0 - alpha;
+    const double rs = 1.0 / (alpha * v0);
+#pragma unroll
+    for (int c = k + 1; c < 9; ++c) {
+      double d = v0 * J[k * 9 + c];
+#pragma unroll
+      for (int i = k + 1; i < 9; ++i) d = fma(J[i * 9 + k], J[i * 9 + c], d);
+      d *= rs;
+      J[k * 9 + c] = fma(d, v0, J[k * 9 + c]);
+#pragma unroll
+      for (int i = k + 1; i < 9; ++i) J[i * 9 + c] = fma(d, J[i * 9 + k], J[i * 9 + c]);
+    }
+    {
+      double d = v0 * b[k];
+#pragma unroll
+      for (int i = k + 1; i < 9; ++i) d = fma(J[i * 9 + k], b[i], d);
+      d *= rs;
+      b[k] = fma(d, v0, b[k]);
+#pragma unroll
+      for (int i = k + 1; i < 9; ++i) b[i] = fma(d, J[i * 9 + k], b[i]);
+    }
+    J[k * 9 + k] = alpha;
   }
-}
-
-// 9x9 LU with partial pivoting (first maximal |a|, as dgetrf) + solve; row-major J.
-// Returns true if a pivot is exactly zero (dgesv info > 0).
-__device__ __forceinline__ bool lu_solve9(double* J, double* b) {
-#pragma unroll
-  for (int j = 0; j < 9; ++j) {
-    int p = j;
-    double amax = fabs(J[j * 9 + j]);
-#pragma unroll
-    for (int i = j + 1; i < 9; ++i) {
-      const double v = fabs(J[i * 9 + j]);
-      if (v > amax) { amax = v; p = i; }
-    }
-    if (amax == 0.0) return true;
-    if (p != j) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) { const double t = J[j * 9 + k]; J[j * 9 + k] = J[p * 9 + k]; J[p * 9 + k] = t; }
-      const double t = b[j]; b[j] = b[p]; b[p] = t;
-    }
-    const double rp = 1.0 / J[j * 9 + j];
-#pragma unroll
-    for (int i = j + 1; i < 9; ++i) {
-      const double l = J[i * 9 + j] * rp;
-#pragma unroll
-      for (int k = j + 1; k < 9; ++k) J[i * 9 + k] = fma(-l, J[j * 9 + k], J[i * 9 + k]);
-      b[i] = fma(-l, b[j], b[i]);
-    }
-  }
+  if (J[80] == 0.0) return true;
 #pragma unroll
   for (int i = 8; i >= 0; --i) {
     double s = b[i];
@@ -88,28 +102,21 @@ __device__ __forceinline__ bool lu_solve9(double* J, double* b) {
   return false;
 }
 
-// Outcome of one integrateStress call kept in registers by the caller.
-struct StressOut {
-  double S[6];
-  double Lp[9];
-  double Fp[9];
-};
-
 // integrateStress, phase_mechanical.f90:379-584 (Fi = I, Li = 0).
-// Lp (in/out) is the warm start / result; on success P and Fe are written through.
+// xs: this thread's shared-memory slots (stride PASS_THREADS) holding 1/xi (first NS)
+// and the Newton weights dt*dgamma (next NS).  Lp (in/out) is the warm start and, on
+// success, the result; S, Fp, P and Fe are written only on success.
 template <int NS>
 __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, const double* F, const double* Fp0,
-                                const double* xi, double dt, double* Lp, double* S, double* Fp,
-                                double* Pout, double* Feout, int& newton) {
+                                double* xs, double dt, double* Lp, double* S, double* Fp, double* Pout, double* Feout,
+                                int& newton) {
+  double* const sw = xs + NS * PASS_THREADS;
   double invFp0[9];
   if (inv33(Fp0, invFp0)) return 5;                       // STATUS_FAIL_PHASE_MECHANICAL_STRESS
   double A[9];
   mm33(F, invFp0, A);
-  double inv_xi[NS];
-#pragma unroll
-  for (int s = 0; s < NS; ++s) inv_xi[s] = 1.0 / xi[s];
 
-  double Lg[9], Lg_old[9], dL[9], B[9], Fe[9], s6[6];
+  double Lg[9], Lg_old[9], dL[9], B[9], s6[6];
 #pragma unroll
   for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; Lg_old[k] = Lp[k]; dL[k] = 0.0; }
   double step = 1.0, res_old = 1.7976931348623157e308;
@@ -119,32 +126,32 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
     ++newton;
 #pragma unroll
     for (int k = 0; k < 9; ++k) B[k] = ((k % 4 == 0) ? 1.0 : 0.0) - dt * Lg[k];
+    double Fe[9];
     mm33(A, B, Fe);
     hooke_S<NS>(pc, Fe, s6);
-    // Lp_c and its derivative weights
+    // Lp_c = sum_s dot_gamma_s P_s and the weights of its derivative
     double Lc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    double w[NS];
-    int sense[NS];
+    unsigned neg = 0u;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
       const bool pos = tp > tn;
       const double tmax = pos ? tp : tn;
-      const double r = tmax * inv_xi[s];
+      const double r = tmax * xs[s * PASS_THREADS];
       double g, dg;
       if (pc.n_int[s] >= 1) {
         const double rn1 = powi(r, pc.n_int[s] - 1);
         const double sd = pos ? pc.dg0[s] : -pc.dg0[s];
         g = sd * (rn1 * r);
-        dg = (sd * pc.n[s]) * rn1 * inv_xi[s];
+        dg = (sd * pc.n[s]) * rn1 * xs[s * PASS_THREADS];
       } else {
         g = (pos ? pc.dg0[s] : -pc.dg0[s]) * pow(r, pc.n[s]);
         dg = g * pc.n[s] / tmax;
       }
       if (!(fabs(g) > TINY10)) dg = 0.0;
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
-      sense[s] = g > 0.0 ? 0 : 1;
-      w[s] = dt * dg;
+      if (!(g > 0.0)) neg |= 1u << s;
+      sw[s * PASS_THREADS] = dt * dg;
 #pragma unroll
       for (int k = 0; k < 9; ++k) Lc[k] = fma(g, pc.P[s][k], Lc[k]);
     }
@@ -168,6 +175,28 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
     }
     if (jaco % nm.f_update_jacobi_Lp == 0) {
       ++jaco;
+      // H^(kl) = sum_s w_s P_s(k,l) Q_s (symmetric, 11 22 33 23 13 12), row kl = 3k + l
+      double H[9][6];
+#pragma unroll
+      for (int i = 0; i < 9; ++i)
+#pragma unroll
+        for (int t = 0; t < 6; ++t) H[i][t] = 0.0;
+#pragma unroll
+      for (int s = 0; s < NS; ++s) {
+        const double ws = sw[s * PASS_THREADS];
+        const bool ng = (neg >> s) & 1u;
+        double q[6];
+#pragma unroll
+        for (int t = 0; t < 6; ++t) q[t] = ng ? pc.q6[1][s][t] : pc.q6[0][s][t];
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            const double c = ws * pc.P[s][k + 3 * l];
+#pragma unroll
+            for (int t = 0; t < 6; ++t) H[3 * k + l][t] = fma(c, q[t], H[3 * k + l][t]);
+          }
+      }
       double M[9];
       mtm33(A, Fe, M);                                    // M = A^T Fe
       double J[81], rhs[9];
@@ -176,16 +205,8 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
 #pragma unroll
         for (int l = 0; l < 3; ++l) {
           const int row = 3 * k + l;
-          double H[6] = {0, 0, 0, 0, 0, 0};
-#pragma unroll
-          for (int s = 0; s < NS; ++s) {
-            const double c = w[s] * pc.P[s][k + 3 * l];
-            const double* q = pc.q6[sense[s]][s];
-#pragma unroll
-            for (int t = 0; t < 6; ++t) H[t] = fma(c, q[t], H[t]);
-          }
-          // H as symmetric 3x3: (11,22,33,23,13,12)
-          const double Hm[9] = {H[0], H[5], H[4], H[5], H[1], H[3], H[4], H[3], H[2]};
+          const double* h = H[row];
+          const double Hm[9] = {h[0], h[5], h[4], h[5], h[1], h[3], h[4], h[3], h[2]};
 #pragma unroll
           for (int p = 0; p < 3; ++p)
 #pragma unroll
@@ -195,7 +216,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
             }
           rhs[row] = R[k + 3 * l];                        // math_33to9 (row-major flattening)
         }
-      if (lu_solve9(J, rhs)) return 8;                   // STATUS_FAIL_PHASE_MECHANICAL_STRESS_LP_DGESV
+      if (qr_solve9(J, rhs)) return 8;                   // STATUS_FAIL_PHASE_MECHANICAL_STRESS_LP_DGESV
 #pragma unroll
       for (int k = 0; k < 3; ++k)
 #pragma unroll
@@ -222,130 +243,136 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
   return 0;
 }
 
+// phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0) at the stored
+// stress and state of voxel v, written to this thread's slots: xi rates first, then
+// |dot_gamma|.  Returns true if any rate is NaN.
+template <int NS>
+__device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double s6[6], const double* __restrict__ state,
+                                int64_t N, int64_t v, double* xs) {
+  double adg[NS];
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
+    const double tmax = tp > tn ? tp : tn;
+    adg[s] = fabs(pc.dg0[s] * powr(tmax / state[s * N + v], pc.n[s], pc.n_int[s]));
+  }
+  bool bad = false;
+#pragma unroll
+  for (int l = 0; l < NS; ++l) {
+    const double x = 1.0 - state[l * N + v] / pc.xiinf[l];
+    const double left = copysign(powr(fabs(x), pc.a[l], pc.a_int[l]), x);
+    double hg = 0.0;
+#pragma unroll
+    for (int k = 0; k < NS; ++k) hg = fma(pc.h[l][k], adg[k], hg);
+    const double d = pc.h0f[l] * left * hg;
+    bad |= isnan(d) || isnan(adg[l]);
+    xs[l * PASS_THREADS] = d;
+    xs[(NS + l) * PASS_THREADS] = adg[l];
+  }
+  return bad;
+}
+
 // damper, phase_mechanical.f90:653-674
 __device__ __forceinline__ double damper(double d01, double d12, double d22) {
   if (fmin(d01, d12) < 0.0 && d22 > 0.0) return 0.75 + 0.25 * tanh(2.0 + 4.0 * d12 / d22);
   return 1.0;
 }
 
-// integrateStateFPI, phase_mechanical.f90:591-676.
-// S (in/out) is the current stress (S0 after restore), st (in/out) the current state.
+// Advances voxel v through the control flow of phase_mechanical_constitutive and
+// integrateStateFPI until its next integrateStress (phase PH_STRESS) or its end
+// (PH_DONE).  Entered in PH_CTRL (substep control after an integration attempt) or
+// PH_DOT1 (state update after a successful integrateStress).
 template <int NS>
-__device__ int integrate_state_fpi(const PhaseConst<NS>& pc, const Numerics& nm, const double* F, const double* Fp0,
-                                   const double* st0, double dt, double* st, double* S, double* Lp, double* Fp,
-                                   double* Pout, double* Feout, int& nstate, int& newton) {
-  constexpr int NST = 2 * NS;
-  double dot[NST], last1[NST], last2[NST];
-  dot_state<NS>(pc, S, st, dot);
-#pragma unroll
-  for (int i = 0; i < NST; ++i)
-    if (isnan(dot[i])) return 3;                           // STATUS_FAIL_PHASE_MECHANICAL_STATE
-#pragma unroll
-  for (int i = 0; i < NST; ++i) { st[i] = fma(dot[i], dt, st0[i]); last1[i] = 0.0; }
-  int status = 3;
-  for (int it = 1; it <= nm.N_iter_state_max; ++it) {
-    ++nstate;
-#pragma unroll
-    for (int i = 0; i < NST; ++i) { last2[i] = it > 1 ? last1[i] : 0.0; last1[i] = dot[i]; }
-    status = integrate_stress<NS>(pc, nm, F, Fp0, st, dt, Lp, S, Fp, Pout, Feout, newton);
-    if (status != 0) break;
-    dot_state<NS>(pc, S, st, dot);
-    bool bad = false;
-    double d01 = 0.0, d12 = 0.0, d22 = 0.0;
-#pragma unroll
-    for (int i = 0; i < NST; ++i) {
-      bad |= isnan(dot[i]);
-      const double a = dot[i] - last1[i], b = last1[i] - last2[i];
-      d12 = fma(a, b, d12);
-      d22 = fma(b, b, d22);
-      d01 = fma(dot[i], last1[i], d01);
-    }
-    if (bad) break;
-    const double zeta = damper(d01, d12, d22);
-    bool conv = true;
-#pragma unroll
-    for (int i = 0; i < NST; ++i) {
-      const double d = dot[i] * zeta + last1[i] * (1.0 - zeta);
-      dot[i] = d;
-      const double r = st[i] - st0[i] - d * dt;
-      st[i] = st[i] - r;
-      const double atol = i < NS ? pc.atol_xi : pc.atol_gamma;
-      conv = conv && (fabs(r) <= fmax(atol, nm.eps_rel_state * fabs(st[i])));
-    }
-    if (conv) { status = 0; break; }
-  }
-  return status;
-}
-
-// phase_mechanical_constitutive, phase_mechanical.f90:1008-1090, after
-// mechanical_restore (Fp := Fp0, S := S0, state := state0; Lp kept as warm start).
-template <int NS>
-__device__ int constitutive_point(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, int64_t v,
-                                  const double* Fnew, double dt, int& nstate, int& newton, int& nsub) {
+__device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, const PassWork& w, int64_t v,
+                        double dt, VoxelCtl& c, double* xs) {
   constexpr int NST = 2 * NS;
   const int64_t N = f.N;
-  double F0[9], Fp0s[9], Lp0s[9], Lp[9], Fp[9], S[6], st[NST], st0s[NST], Fs[9];
+  // every control step shrinks the substep or advances stepFrac; the bound only
+  // guards against numerics (r_cutback >= 1) under which the reference loops forever
+  for (int guard = 0; c.phase != PH_STRESS && c.phase != PH_DONE; ++guard) {
+    if (guard > 4096) { c.status = 3; c.phase = PH_DONE; break; }
+    if (c.phase == PH_CTRL) {
+      // substep control, phase_mechanical.f90:1040-1080
+      bool todo;
+      if (c.status == 0) {
+        c.stepFrac = c.stepFrac + c.step;
+        c.step = fmin(1.0 - c.stepFrac, nm.r_increase * c.step);
+        todo = c.step > 0.0;
+        if (todo) {
 #pragma unroll
-  for (int k = 0; k < 9; ++k) {
-    F0[k] = f.F0[k * N + v];
-    Fp0s[k] = f.Fp0[k * N + v];
-    Lp0s[k] = f.Lp0[k * N + v];
-    Lp[k] = f.Lp[k * N + v];
-    Fp[k] = Fp0s[k];
-  }
+          for (int k = 0; k < 9; ++k) {
+            w.F0s[k * N + v] = w.Fs[k * N + v];
+            w.Lp0s[k * N + v] = f.Lp[k * N + v];
+            w.Fp0s[k * N + v] = f.Fp[k * N + v];
+          }
+          for (int i = 0; i < NST; ++i) w.st0s[i * N + v] = f.state[i * N + v];
+        }
+      } else {
+        c.step = nm.r_cutback * c.step;
 #pragma unroll
-  for (int k = 0; k < 6; ++k) S[k] = f.S0[k * N + v];
+        for (int k = 0; k < 9; ++k) f.Fp[k * N + v] = w.Fp0s[k * N + v];
 #pragma unroll
-  for (int i = 0; i < NST; ++i) { st0s[i] = f.state0[i * N + v]; st[i] = st0s[i]; }
-  double Pl[9], Fel[9];
-  bool wrote = false;
-  double stepFrac = 0.0, step = 1.0 / nm.r_cutback;
-  int status = 1;                                         // STATUS_ITERATING
-  bool todo = true;
-  while (todo) {
-    if (status == 0) {
-      stepFrac = stepFrac + step;
-      step = fmin(1.0 - stepFrac, nm.r_increase * step);
-      todo = step > 0.0;
-      if (todo) {
+        for (int k = 0; k < 6; ++k) f.S[k * N + v] = f.S0[k * N + v];
+        if (c.step < 1.0)
 #pragma unroll
-        for (int k = 0; k < 9; ++k) { F0[k] = Fs[k]; Lp0s[k] = Lp[k]; Fp0s[k] = Fp[k]; }
-#pragma unroll
-        for (int i = 0; i < NST; ++i) st0s[i] = st[i];
+          for (int k = 0; k < 9; ++k) f.Lp[k * N + v] = w.Lp0s[k * N + v];
+        for (int i = 0; i < NST; ++i) f.state[i * N + v] = w.st0s[i * N + v];
+        todo = c.step > nm.r_cutback_min;
       }
+      if (!todo) { c.phase = PH_DONE; break; }
+      ++c.nsub;
+#pragma unroll
+      for (int k = 0; k < 9; ++k)
+        w.Fs[k * N + v] = fma(c.step, f.F[k * N + v] - f.F0[k * N + v], w.F0s[k * N + v]);
+      c.phase = PH_DOT0;
     } else {
-      step = nm.r_cutback * step;
+      // dotState at the current stress and state: start (DOT0) or update (DOT1) of a state iteration
+      double s6[6];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Fp[k] = Fp0s[k];
-#pragma unroll
-      for (int k = 0; k < 6; ++k) S[k] = f.S0[k * N + v];
-      if (step < 1.0)
-#pragma unroll
-        for (int k = 0; k < 9; ++k) Lp[k] = Lp0s[k];
-#pragma unroll
-      for (int i = 0; i < NST; ++i) st[i] = st0s[i];
-      todo = step > nm.r_cutback_min;
-    }
-    if (todo) {
-      ++nsub;
-#pragma unroll
-      for (int k = 0; k < 9; ++k) Fs[k] = fma(step, Fnew[k] - f.F0[k * N + v], F0[k]);
-      status = integrate_state_fpi<NS>(pc, nm, Fs, Fp0s, st0s, step * dt, st, S, Lp, Fp, Pl, Fel, nstate, newton);
-      if (status == 0) wrote = true;
+      for (int k = 0; k < 6; ++k) s6[k] = f.S[k * N + v];
+      const bool bad = dot_state_slots<NS>(pc, s6, f.state, N, v, xs);
+      const double dts = c.step * dt;
+      if (c.phase == PH_DOT0) {
+        // integrateStateFPI:616-620
+        if (bad) { c.status = 3; c.phase = PH_CTRL; continue; }   // STATUS_FAIL_PHASE_MECHANICAL_STATE
+        for (int i = 0; i < NST; ++i) {
+          const double d = xs[i * PASS_THREADS];
+          f.state[i * N + v] = fma(d, dts, w.st0s[i * N + v]);
+          w.dot[i * N + v] = d;
+        }
+        c.it = 0;
+        c.phase = PH_STRESS;
+      } else {
+        // integrateStateFPI:631-646 (the stress integration of this iteration succeeded: status 0)
+        if (bad) { c.phase = PH_CTRL; continue; }
+        double d01 = 0.0, d12 = 0.0, d22 = 0.0;
+        for (int i = 0; i < NST; ++i) {
+          const double d = xs[i * PASS_THREADS];
+          const double l1 = w.dot[i * N + v];                          // dotState_last(:,1)
+          const double l2 = c.it > 1 ? w.last1[i * N + v] : 0.0;      // dotState_last(:,2)
+          const double a = d - l1, b = l1 - l2;
+          d12 = fma(a, b, d12);
+          d22 = fma(b, b, d22);
+          d01 = fma(d, l1, d01);
+        }
+        const double zeta = damper(d01, d12, d22);
+        bool conv = true;
+        for (int i = 0; i < NST; ++i) {
+          const double l1 = w.dot[i * N + v];
+          const double d = xs[i * PASS_THREADS] * zeta + l1 * (1.0 - zeta);
+          const double st = f.state[i * N + v];
+          const double r = st - w.st0s[i * N + v] - d * dts;
+          const double stn = st - r;
+          f.state[i * N + v] = stn;
+          w.last1[i * N + v] = l1;
+          w.dot[i * N + v] = d;
+          const double atol = i < NS ? pc.atol_xi : pc.atol_gamma;
+          conv = conv && (fabs(r) <= fmax(atol, nm.eps_rel_state * fabs(stn)));
+        }
+        c.phase = (conv || c.it >= nm.N_iter_state_max) ? PH_CTRL : PH_STRESS;
+      }
     }
   }
-  // write back the phase containers (current values)
-#pragma unroll
-  for (int k = 0; k < 9; ++k) { f.Lp[k * N + v] = Lp[k]; f.Fp[k * N + v] = Fp[k]; }
-#pragma unroll
-  for (int k = 0; k < 6; ++k) f.S[k * N + v] = S[k];
-#pragma unroll
-  for (int i = 0; i < NST; ++i) f.state[i * N + v] = st[i];
-  if (wrote) {
-#pragma unroll
-    for (int k = 0; k < 9; ++k) { f.P[k * N + v] = Pl[k]; f.Fe[k * N + v] = Fel[k]; }
-  }
-  return status;
 }
 
 }  // namespace dmk

@@ -112,6 +112,13 @@ struct dmk_ctx {
   int aa_m = 0;
   int aa_blocks = 0;
   double *aa_dX = nullptr, *aa_dR = nullptr, *aa_Rprev = nullptr, *aa_partials = nullptr, *aa_out = nullptr;
+  // constitutive pass scheme: per-voxel iteration state, voxel lists, pass counts
+  double* pw = nullptr;          // Fs F0s Fp0s Lp0s (9 each), st0s dot last1 (2 NS each), stepFrac, step
+  int* pctl = nullptr;           // 6 planes of per-voxel control integers
+  int* plist[2] = {nullptr, nullptr};
+  int* pcount = nullptr;         // [0], [1]: entries appended to plist[0], plist[1]
+  int* hcount = nullptr;         // pinned host copy of pcount and status
+  int64_t passes = 0;            // constitutive passes launched (all evaluations)
 };
 
 namespace {
@@ -126,13 +133,55 @@ Fields make_fields(dmk_ctx* c, const double* r) {
   return f;
 }
 
-cudaError_t run_constitutive(dmk_ctx* c, const Fields& f, double dt, int apply) {
-  switch (c->NS) {
-    case 12: return launch_constitutive<12>(*c->pc12, c->nm, f, dt, apply, c->stream);
-    case 18: return launch_constitutive<18>(*c->pc18, c->nm, f, dt, apply, c->stream);
-    case 24: return launch_constitutive<24>(*c->pc24, c->nm, f, dt, apply, c->stream);
+PassWork pass_work(dmk_ctx* c, int out) {
+  const int64_t N = c->N;
+  const int NST = 2 * c->NS;
+  PassWork w;
+  w.Fs = c->pw;
+  w.F0s = w.Fs + 9 * N;
+  w.Fp0s = w.F0s + 9 * N;
+  w.Lp0s = w.Fp0s + 9 * N;
+  w.st0s = w.Lp0s + 9 * N;
+  w.dot = w.st0s + NST * N;
+  w.last1 = w.dot + NST * N;
+  w.sub = w.last1 + NST * N;
+  w.ctl = c->pctl;
+  w.list_out = c->plist[out];
+  w.count_out = c->pcount + out;
+  return w;
+}
+size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 6 * NS + 2); }
+
+template <int NS>
+int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, double dt, int apply) {
+  // pass 0: restore and control up to the first integrateStress of every voxel
+  CK(cudaMemsetAsync(c->pcount, 0, 2 * sizeof(int), c->stream));
+  CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, 0), dt, apply, c->stream));
+  ++c->passes;
+  int cur = 0;
+  for (int pass = 1;; ++pass) {
+    CK(cudaMemcpyAsync(c->hcount, c->pcount + cur, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int64_t n = c->hcount[0];
+    if (n == 0) break;
+    // bounded by substeps x state iterations; a runaway count means corrupted control state
+    if (pass > 100000) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
+    const int nxt = 1 - cur;
+    CK(cudaMemsetAsync(c->pcount + nxt, 0, sizeof(int), c->stream));
+    CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, nxt), dt, c->plist[cur], n, c->stream));
+    ++c->passes;
+    cur = nxt;
   }
-  return cudaErrorInvalidValue;
+  return 0;
+}
+
+int run_constitutive(dmk_ctx* c, const Fields& f, double dt, int apply) {
+  switch (c->NS) {
+    case 12: return constitutive_passes<12>(c, *c->pc12, f, dt, apply);
+    case 18: return constitutive_passes<18>(c, *c->pc18, f, dt, apply);
+    case 24: return constitutive_passes<24>(c, *c->pc24, f, dt, apply);
+  }
+  return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
 }
 cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o) {
   switch (c->NS) {
@@ -344,7 +393,7 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
   CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
   Fields f = make_fields(c, r);
   CK(cudaEventRecord(c->ev[0], c->stream));
-  CKL(run_constitutive(c, f, dt, apply));
+  if (int rc = run_constitutive(c, f, dt, apply)) return rc;
   CK(cudaEventRecord(c->ev[1], c->stream));
   int st = 0;
   CK(cudaMemcpyAsync(&st, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
@@ -353,7 +402,7 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
   CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
   c->last_ms[0] += ms;
   if (st == 0) std::swap(c->P, c->Pnew);
-  else CKL(launch_sum9(c->P, c->N, c->partials, c->stream));
+  CKL(launch_sum9(c->P, c->N, c->partials, c->stream));   // <P> of the committed (or kept) stress field
   *status_out = st;
   return 0;
 }
@@ -521,6 +570,7 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   c->N = int64_t(cells[0]) * cells[1] * cells[2];
   c->wgt = 1.0 / double(c->N);
   const int64_t N = c->N;
+  if (N > 2147483647LL) { delete c; return fail(DMK_ERR_ARG, "at most 2^31 - 1 cells per context"); }
   for (int64_t v = 0; v < N; ++v)
     if (materialAt[v] < 0 || materialAt[v] >= n_materials) { delete c; return fail(DMK_ERR_ARG, "material index out of range"); }
 
@@ -559,8 +609,15 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->partials, 9 * (size_t)nblocks_const(c))) || (rc = dalloc(&c->sums, 16)) ||
       (rc = dalloc(&c->div_partials, (size_t)gamma_div_blocks(cells[0], cells[1], cells[2]))) ||
       (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
-      (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)))
+      (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)) ||
+      (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 6 * size_t(N))) ||
+      (rc = dalloc(&c->plist[0], size_t(N))) || (rc = dalloc(&c->plist[1], size_t(N))) ||
+      (rc = dalloc(&c->pcount, 2)))
     return bail(rc);
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), 4 * sizeof(int)) != cudaSuccess) {
+    c->hcount = nullptr;
+    return bail(fail(DMK_ERR_CUDA, "cudaMallocHost failed"));
+  }
   if (precision == DMK_PRECISION_MIXED)
     if ((rc = dalloc(&c->specf, 2 * 9 * plane)) || (rc = dalloc(&c->Pf, 9 * N))) return bail(rc);
   c->tan_blocks = dPdF_blocks(N);
@@ -1017,8 +1074,10 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->partials, (void*)c->sums, (void*)c->div_partials, (void*)c->status, (void*)c->iter,
                   (void*)c->counters, (void*)c->sc, (void*)c->scratch, (void*)c->tan_out, (void*)c->tan_idx,
                   (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work,
-                  (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out})
+                  (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
+                  (void*)c->pw, (void*)c->pctl, (void*)c->plist[0], (void*)c->plist[1], (void*)c->pcount})
     if (p) cudaFree(p);
+  if (c->hcount) cudaFreeHost(c->hcount);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto e : c->tev)

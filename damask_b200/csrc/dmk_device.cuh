@@ -60,6 +60,30 @@ struct Fields {
   unsigned long long* counters;   // [0] evaluations [1] state iterations [2] Newton iterations
 };
 
+constexpr int PASS_THREADS = 128;   // threads per block of the pass kernels
+
+// Per-voxel iteration state of the pass scheme (planes of N entries each).
+struct PassWork {
+  double* Fs;      // 9: F of the current substep
+  double* F0s;     // 9: F at the start of the current substep (subF0)
+  double* Fp0s;    // 9: subFp0
+  double* Lp0s;    // 9: subLp0
+  double* st0s;    // 2 NS: subState0
+  double* dot;     // 2 NS: (damped) dotState of the last state iteration
+  double* last1;   // 2 NS: dotState of the iteration before (dotState_last(:,1))
+  double* sub;     // 2: stepFrac (subFrac), step (subStep)
+  int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
+  int* list_out;   // voxels that continue into the next pass
+  int* count_out;  // number of entries appended to list_out
+};
+
+enum : int { PH_CTRL = 0, PH_DOT0 = 1, PH_STRESS = 2, PH_DOT1 = 3, PH_DONE = 4 };
+
+struct VoxelCtl {
+  int phase, status, it, nsub, nstate, newton;
+  double stepFrac, step;
+};
+
 // ------------------------------------------------------------- 3x3 helpers
 // Column-major: a[i + 3*j] = A(i,j)
 __device__ __forceinline__ void mm33(const double* A, const double* B, double* C) {

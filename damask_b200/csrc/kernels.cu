@@ -1,8 +1,6 @@
 // CUDA kernels of the damask_b200 hot path (sm_100a).
 //
-//  constitutive_kernel  one thread per voxel: fused Richardson field update
-//                       F <- F - r, phase restore, substep cutback, FPI state
-//                       integration, Lp Newton, P; per-block partial sums of P.
+//  (the constitutive pass kernels are in constitutive.cu)
 //  gamma_div_kernel     one thread per Fourier point: divergence-RMS partial sums
 //                       and the Gamma-operator application (closed form) with the
 //                       DC term set to the aim, in one pass over the spectrum.
@@ -10,76 +8,11 @@
 //                       min/max Frobenius-norm selection.
 //  small kernels        aim/BC update, convergence test, layout transposes.
 #include "kernels.cuh"
-#include "constitutive.cuh"
 
 #include <algorithm>
 #include <cfloat>
 
 namespace dmk {
-
-// ------------------------------------------------------------------ constitutive
-template <int NS>
-__global__ void __launch_bounds__(CONST_THREADS)
-constitutive_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
-                    const __grid_constant__ Fields f, double dt, int apply_update) {
-  __shared__ double red[9 * (CONST_THREADS / 32)];
-  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
-  const int64_t N = f.N;
-  double Psum[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-  int status = 0, nstate = 0, newton = 0, nsub = 0;
-  if (v < N) {
-    double Fn[9];
-#pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      double x = f.Fsol[k * N + v];
-      if (apply_update) {
-        x = x - f.r[k * N + v];
-        f.Fsol[k * N + v] = x;
-      }
-      Fn[k] = x;
-      f.F[k * N + v] = x;
-    }
-    status = constitutive_point<NS>(pc, nm, f, v, Fn, dt, nstate, newton, nsub);
-    if (status == 0) {
-#pragma unroll
-      for (int k = 0; k < 9; ++k) Psum[k] = f.P[k * N + v];
-    } else {
-      atomicMax(f.status, 2);                     // STATUS_FAIL_PHASE_MECHANICAL
-    }
-    if (f.iter) {
-      f.iter[v] = nstate;
-      f.iter[N + v] = newton;
-      f.iter[2 * N + v] = nsub;
-      f.iter[3 * N + v] = status;
-    }
-  }
-  // iteration counters (warp aggregated)
-  unsigned long long cs = nstate, cn = newton;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    cs += __shfl_down_sync(0xffffffffu, cs, o);
-    cn += __shfl_down_sync(0xffffffffu, cn, o);
-  }
-  if ((threadIdx.x & 31) == 0 && f.counters) {
-    atomicAdd(&f.counters[1], cs);
-    atomicAdd(&f.counters[2], cn);
-  }
-  block_reduce_sum<9>(Psum, red);
-  if (threadIdx.x == 0)
-#pragma unroll
-    for (int k = 0; k < 9; ++k) f.partials[int64_t(blockIdx.x) * 9 + k] = Psum[k];
-}
-
-template <int NS>
-cudaError_t launch_constitutive(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, double dt,
-                                int apply_update, cudaStream_t s) {
-  const int nb = int((f.N + CONST_THREADS - 1) / CONST_THREADS);
-  constitutive_kernel<NS><<<nb, CONST_THREADS, 0, s>>>(pc, nm, f, dt, apply_update);
-  return cudaGetLastError();
-}
-template cudaError_t launch_constitutive<12>(const PhaseConst<12>&, const Numerics&, const Fields&, double, int, cudaStream_t);
-template cudaError_t launch_constitutive<18>(const PhaseConst<18>&, const Numerics&, const Fields&, double, int, cudaStream_t);
-template cudaError_t launch_constitutive<24>(const PhaseConst<24>&, const Numerics&, const Fields&, double, int, cudaStream_t);
 
 // partial sums of a 9-plane field (used when the stale P field is kept after a failure)
 __global__ void __launch_bounds__(CONST_THREADS) sum9_kernel(const double* __restrict__ X, int64_t N, double* partials) {

@@ -4,7 +4,7 @@
 
 namespace dmk {
 
-constexpr int CONST_THREADS = 128;   // constitutive block size (register-heavy FP64 threads)
+constexpr int CONST_THREADS = 128;   // block size of the per-voxel partial sums of P
 constexpr int SPEC_THREADS = 256;    // spectral pointwise kernels
 
 // Solver scalars living in device memory (grid_mech_spectral_basic.f90:30-45 module state
@@ -35,9 +35,13 @@ struct Numerics2 {
   double eps_abs_div, eps_rel_div, eps_abs_P, eps_rel_P;
 };
 
+// constitutive passes (constitutive.cu)
 template <int NS>
-cudaError_t launch_constitutive(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, double dt,
-                                int apply_update, cudaStream_t s);
+cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
+                                      const PassWork& w, double dt, int apply_update, cudaStream_t s);
+template <int NS>
+cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
 cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s);
 cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s);
 cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int nparts, double wgt, const int* status,
