@@ -108,8 +108,11 @@ __global__ void __launch_bounds__(PASS_THREADS)
 constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                          const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                          const int* __restrict__ list_in, int64_t n_in) {
-  extern __shared__ double slots[];
-  double* xs = slots + threadIdx.x;
+  extern __shared__ double2 smem2[];
+  SysConst* sc = reinterpret_cast<SysConst*>(smem2);
+  double* xs = reinterpret_cast<double*>(sc + NS) + threadIdx.x;
+  stage_sys_const<NS>(pc, sc);
+  __syncthreads();
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
   bool keep = false;
@@ -123,17 +126,14 @@ constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid
     ++c.it;
     ++c.nstate;
     dstate = 1;
-    double F[9], Fp0[9], Lp[9];
+    double Lp[9];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) {
-      F[k] = w.Fs[k * N + v];
-      Fp0[k] = w.Fp0s[k * N + v];
-      Lp[k] = f.Lp[k * N + v];
-    }
+    for (int k = 0; k < 9; ++k) Lp[k] = f.Lp[k * N + v];
 #pragma unroll
     for (int s = 0; s < NS; ++s) xs[s * PASS_THREADS] = 1.0 / f.state[s * N + v];
     double S[6], Fp[9], P[9], Fe[9];
-    const int st = integrate_stress<NS>(pc, nm, F, Fp0, xs, c.step * dt, Lp, S, Fp, P, Fe, dnewton);
+    const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, w.Fp0s + v, N, xs, c.step * dt, Lp, S, Fp, P, Fe,
+                                        dnewton);
     c.newton += dnewton;
     if (st != 0) {
       c.status = st;
@@ -174,7 +174,7 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
-  const size_t smem = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  const size_t smem = size_t(NS) * sizeof(SysConst) + size_t(2 * NS + 27) * PASS_THREADS * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_pass_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;

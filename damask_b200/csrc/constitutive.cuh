@@ -26,8 +26,9 @@
 // leads to the next integrateStress.  Between passes the per-voxel iteration state
 // lives in HBM planes (PassWork), so the large per-system arrays of the state
 // iteration are never live during the Newton loop; all indexing into register
-// arrays is static, and the 9x9 Newton system is solved by Householder QR
-// (backward stable without a data-dependent row exchange).
+// arrays is static, and the 9x9 Newton system, a rank-6 update of the identity, is
+// solved through its 6x6 Woodbury form by Householder QR (no data-dependent row
+// exchange, so the matrix stays in registers).
 #pragma once
 #include "dmk_device.cuh"
 
@@ -54,71 +55,84 @@ __device__ __forceinline__ void store_ctl(const PassWork& w, int64_t N, int64_t 
   w.sub[N + v] = c.step;
 }
 
-// Solves J x = b for a row-major 9x9 J (overwritten with R) by Householder QR:
+// Solves A x = b for a row-major n x n A (overwritten with R) by Householder QR:
 // column k is reflected onto alpha e_k with alpha = -sign(x0) |x|, v = x - alpha e_k,
 // H y = y + v (v.y) / (alpha v0).  Returns true when a column of the remaining
-// matrix is exactly zero (the matrix is singular; dgesv info > 0).
-__device__ __forceinline__ bool qr_solve9(double* J, double* b) {
+// matrix is exactly zero (the matrix is singular; dgesv info > 0).  All indices are
+// compile-time constants, so A stays in registers.
+template <int n>
+__device__ __forceinline__ bool qr_solve(double* A, double* b) {
 #pragma unroll
-  for (int k = 0; k < 8; ++k) {
+  for (int k = 0; k < n - 1; ++k) {
     double s2 = 0.0;
 #pragma unroll
-    for (int i = k; i < 9; ++i) s2 = fma(J[i * 9 + k], J[i * 9 + k], s2);
+    for (int i = k; i < n; ++i) s2 = fma(A[i * n + k], A[i * n + k], s2);
     if (s2 == 0.0) return true;
     const double sig = sqrt(s2);
-    const double x0 = J[k * 9 + k];
+    const double x0 = A[k * n + k];
     const double alpha = x0 >= 0.0 ? -sig : sig;
     const double v0 = x0 - alpha;
     const double rs = 1.0 / (alpha * v0);
 #pragma unroll
-    for (int c = k + 1; c < 9; ++c) {
-      double d = v0 * J[k * 9 + c];
+    for (int c = k + 1; c < n; ++c) {
+      double d = v0 * A[k * n + c];
 #pragma unroll
-      for (int i = k + 1; i < 9; ++i) d = fma(J[i * 9 + k], J[i * 9 + c], d);
+      for (int i = k + 1; i < n; ++i) d = fma(A[i * n + k], A[i * n + c], d);
       d *= rs;
-      J[k * 9 + c] = fma(d, v0, J[k * 9 + c]);
+      A[k * n + c] = fma(d, v0, A[k * n + c]);
 #pragma unroll
-      for (int i = k + 1; i < 9; ++i) J[i * 9 + c] = fma(d, J[i * 9 + k], J[i * 9 + c]);
+      for (int i = k + 1; i < n; ++i) A[i * n + c] = fma(d, A[i * n + k], A[i * n + c]);
     }
     {
       double d = v0 * b[k];
 #pragma unroll
-      for (int i = k + 1; i < 9; ++i) d = fma(J[i * 9 + k], b[i], d);
+      for (int i = k + 1; i < n; ++i) d = fma(A[i * n + k], b[i], d);
       d *= rs;
       b[k] = fma(d, v0, b[k]);
 #pragma unroll
-      for (int i = k + 1; i < 9; ++i) b[i] = fma(d, J[i * 9 + k], b[i]);
+      for (int i = k + 1; i < n; ++i) b[i] = fma(d, A[i * n + k], b[i]);
     }
-    J[k * 9 + k] = alpha;
+    A[k * n + k] = alpha;
   }
-  if (J[80] == 0.0) return true;
+  if (A[n * n - 1] == 0.0) return true;
 #pragma unroll
-  for (int i = 8; i >= 0; --i) {
+  for (int i = n - 1; i >= 0; --i) {
     double s = b[i];
 #pragma unroll
-    for (int k = i + 1; k < 9; ++k) s = fma(-J[i * 9 + k], b[k], s);
-    b[i] = s / J[i * 9 + i];
+    for (int k = i + 1; k < n; ++k) s = fma(-A[i * n + k], b[k], s);
+    b[i] = s / A[i * n + i];
   }
   return false;
 }
 
 // integrateStress, phase_mechanical.f90:379-584 (Fi = I, Li = 0).
-// xs: this thread's shared-memory slots (stride PASS_THREADS) holding 1/xi (first NS)
-// and the Newton weights dt*dgamma (next NS).  Lp (in/out) is the warm start and, on
-// success, the result; S, Fp, P and Fe are written only on success.
+// F and Fp0 point at voxel v's planes (stride N); they are read at the start and again
+// for the final Fp / P so that no copy stays in registers through the Newton loop.
+// xs: this thread's shared-memory slots (stride PASS_THREADS): 1/xi (NS entries), the
+// Newton weights dt*dgamma (NS), then A, the last accepted Lp guess and the Newton
+// step (9 each).  Lp (in/out) is the warm start and, on success, the result; S, Fp,
+// P and Fe are written only on success.
 template <int NS>
-__device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, const double* F, const double* Fp0,
-                                double* xs, double dt, double* Lp, double* S, double* Fp, double* Pout, double* Feout,
-                                int& newton) {
+__device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __restrict__ sc, const Numerics& nm,
+                                const double* Fg, const double* Fp0g, int64_t N, double* xs, double dt, double* Lp,
+                                double* S, double* Fp, double* Pout, double* Feout, int& newton) {
   double* const sw = xs + NS * PASS_THREADS;
-  double invFp0[9];
-  if (inv33(Fp0, invFp0)) return 5;                       // STATUS_FAIL_PHASE_MECHANICAL_STRESS
-  double A[9];
-  mm33(F, invFp0, A);
-
-  double Lg[9], Lg_old[9], dL[9], B[9], s6[6];
+  double* const sA = xs + 2 * NS * PASS_THREADS;
+  double* const sLo = sA + 9 * PASS_THREADS;
+  double* const sdL = sLo + 9 * PASS_THREADS;
+  {
+    double F[9], Fp0[9], invFp0[9], A[9];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; Lg_old[k] = Lp[k]; dL[k] = 0.0; }
+    for (int k = 0; k < 9; ++k) { F[k] = Fg[k * N]; Fp0[k] = Fp0g[k * N]; }
+    if (inv33(Fp0, invFp0)) return 5;                     // STATUS_FAIL_PHASE_MECHANICAL_STRESS
+    mm33(F, invFp0, A);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) sA[k * PASS_THREADS] = A[k];
+  }
+
+  double Lg[9], B[9], s6[6];
+#pragma unroll
+  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; sLo[k * PASS_THREADS] = Lp[k]; sdL[k * PASS_THREADS] = 0.0; }
   double step = 1.0, res_old = 1.7976931348623157e308;
   int jaco = 0;
   for (int it = 1;; ++it) {
@@ -127,33 +141,50 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
 #pragma unroll
     for (int k = 0; k < 9; ++k) B[k] = ((k % 4 == 0) ? 1.0 : 0.0) - dt * Lg[k];
     double Fe[9];
-    mm33(A, B, Fe);
+    {
+      double A[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) A[k] = sA[k * PASS_THREADS];
+      mm33(A, B, Fe);
+    }
     hooke_S<NS>(pc, Fe, s6);
     // Lp_c = sum_s dot_gamma_s P_s and the weights of its derivative
     double Lc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     unsigned neg = 0u;
-#pragma unroll
+#pragma unroll 2
     for (int s = 0; s < NS; ++s) {
-      const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
+      const SysConst& c = sc[s];
+      double2 p[6];
+#pragma unroll
+      for (int t = 0; t < 6; ++t) p[t] = c.p6[t];
+      const double tp = s6[0] * p[0].x + s6[1] * p[1].x + s6[2] * p[2].x + s6[3] * p[3].x + s6[4] * p[4].x + s6[5] * p[5].x;
+      const double tn = s6[0] * p[0].y + s6[1] * p[1].y + s6[2] * p[2].y + s6[3] * p[3].y + s6[4] * p[4].y + s6[5] * p[5].y;
       const bool pos = tp > tn;
       const double tmax = pos ? tp : tn;
-      const double r = tmax * xs[s * PASS_THREADS];
+      const double ixs = xs[s * PASS_THREADS];
+      const double r = tmax * ixs;
+      const double2 kin = c.kin;
+      const int ni = c.n_int;
       double g, dg;
-      if (pc.n_int[s] >= 1) {
-        const double rn1 = powi(r, pc.n_int[s] - 1);
-        const double sd = pos ? pc.dg0[s] : -pc.dg0[s];
+      if (ni >= 1) {
+        const double rn1 = powi_fixed<6>(r, ni - 1);
+        const double sd = pos ? kin.x : -kin.x;
         g = sd * (rn1 * r);
-        dg = (sd * pc.n[s]) * rn1 * xs[s * PASS_THREADS];
+        dg = (sd * kin.y) * rn1 * ixs;
       } else {
-        g = (pos ? pc.dg0[s] : -pc.dg0[s]) * pow(r, pc.n[s]);
-        dg = g * pc.n[s] / tmax;
+        g = (pos ? kin.x : -kin.x) * pow(r, kin.y);
+        dg = g * kin.y / tmax;
       }
       if (!(fabs(g) > TINY10)) dg = 0.0;
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
       if (!(g > 0.0)) neg |= 1u << s;
       sw[s * PASS_THREADS] = dt * dg;
+      double2 P[5];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Lc[k] = fma(g, pc.P[s][k], Lc[k]);
+      for (int k = 0; k < 5; ++k) P[k] = c.P[k];
+      const double Ps[9] = {P[0].x, P[0].y, P[1].x, P[1].y, P[2].x, P[2].y, P[3].x, P[3].y, P[4].x};
+#pragma unroll
+      for (int k = 0; k < 9; ++k) Lc[k] = fma(g, Ps[k], Lc[k]);
     }
     double R[9];
 #pragma unroll
@@ -165,69 +196,102 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const Numerics& nm, co
     if (nR < res_old) {
       res_old = nR;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Lg_old[k] = Lg[k];
+      for (int k = 0; k < 9; ++k) sLo[k * PASS_THREADS] = Lg[k];
       step = 1.0;
     } else {
       step = nm.r_linesearch_Lp * step;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Lg[k] = fma(dL[k], step, Lg_old[k]);
+      for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * PASS_THREADS], step, sLo[k * PASS_THREADS]);
       continue;
     }
     if (jaco % nm.f_update_jacobi_Lp == 0) {
       ++jaco;
-      // H^(kl) = sum_s w_s P_s(k,l) Q_s (symmetric, 11 22 33 23 13 12), row kl = 3k + l
-      double H[9][6];
+      // Newton step J dLp = -R with J = I + K, K[kl][pb] = (M H^(kl))(p,b), M = A^T Fe,
+      // H^(kl) = sum_s w_s P_s(k,l) Q_s.  Every row of K is M times a symmetric matrix,
+      // so K = Hm L^T has rank 6 (Hm: 9x6 rows h^(kl); L: 9x6, L^T z = symfold(M^T Z)) and
+      // by the Woodbury identity  J^-1 z = z - Hm (I6 + L^T Hm)^-1 L^T z.  With P_s = d_s (x) n_s,
+      //   C6 = I6 + sum_s w_s symfold((M^T d_s) (x) n_s) (x) q_s,   y = C6^-1 symfold(M^T R),
+      //   dLp = sum_s w_s (q_s . y) P_s - R,
+      // the same solution as the 9x9 system without forming it.
+      double M[9];
+      {
+        double A[9];
 #pragma unroll
-      for (int i = 0; i < 9; ++i)
+        for (int k = 0; k < 9; ++k) A[k] = sA[k * PASS_THREADS];
+        mtm33(A, Fe, M);                                  // M = A^T Fe, M[p + 3q] = M(p,q)
+      }
+      double C6[36];
 #pragma unroll
-        for (int t = 0; t < 6; ++t) H[i][t] = 0.0;
-#pragma unroll
+      for (int i = 0; i < 36; ++i) C6[i] = (i % 7 == 0) ? 1.0 : 0.0;
+#pragma unroll 2
       for (int s = 0; s < NS; ++s) {
+        const SysConst& c = sc[s];
         const double ws = sw[s * PASS_THREADS];
         const bool ng = (neg >> s) & 1u;
         double q[6];
 #pragma unroll
-        for (int t = 0; t < 6; ++t) q[t] = ng ? pc.q6[1][s][t] : pc.q6[0][s][t];
-#pragma unroll
-        for (int k = 0; k < 3; ++k)
-#pragma unroll
-          for (int l = 0; l < 3; ++l) {
-            const double c = ws * pc.P[s][k + 3 * l];
-#pragma unroll
-            for (int t = 0; t < 6; ++t) H[3 * k + l][t] = fma(c, q[t], H[3 * k + l][t]);
-          }
-      }
-      double M[9];
-      mtm33(A, Fe, M);                                    // M = A^T Fe
-      double J[81], rhs[9];
-#pragma unroll
-      for (int k = 0; k < 3; ++k)
-#pragma unroll
-        for (int l = 0; l < 3; ++l) {
-          const int row = 3 * k + l;
-          const double* h = H[row];
-          const double Hm[9] = {h[0], h[5], h[4], h[5], h[1], h[3], h[4], h[3], h[2]};
-#pragma unroll
-          for (int p = 0; p < 3; ++p)
-#pragma unroll
-            for (int b = 0; b < 3; ++b) {
-              const double v = M[p] * Hm[3 * b] + M[p + 3] * Hm[1 + 3 * b] + M[p + 6] * Hm[2 + 3 * b];
-              J[row * 9 + 3 * p + b] = (row == 3 * p + b ? 1.0 : 0.0) + v;
-            }
-          rhs[row] = R[k + 3 * l];                        // math_33to9 (row-major flattening)
+        for (int t = 0; t < 6; ++t) {
+          const double2 qq = c.q6[t];
+          q[t] = ng ? qq.y : qq.x;
         }
-      if (qr_solve9(J, rhs)) return 8;                   // STATUS_FAIL_PHASE_MECHANICAL_STRESS_LP_DGESV
+        const double2 dn0 = c.dn[0], dn1 = c.dn[1], dn2 = c.dn[2];
+        const double d0 = dn0.x, d1 = dn0.y, d2 = dn1.x, n0 = dn1.y, n1 = dn2.x, n2 = dn2.y;
+        // u = M^T d
+        const double u0 = M[0] * d0 + M[1] * d1 + M[2] * d2;
+        const double u1 = M[3] * d0 + M[4] * d1 + M[5] * d2;
+        const double u2 = M[6] * d0 + M[7] * d1 + M[8] * d2;
+        const double a6[6] = {ws * (u0 * n0), ws * (u1 * n1), ws * (u2 * n2), ws * (u1 * n2 + u2 * n1),
+                              ws * (u0 * n2 + u2 * n0), ws * (u0 * n1 + u1 * n0)};
 #pragma unroll
-      for (int k = 0; k < 3; ++k)
+        for (int i = 0; i < 6; ++i)
 #pragma unroll
-        for (int l = 0; l < 3; ++l) dL[k + 3 * l] = -rhs[3 * k + l];
+          for (int j = 0; j < 6; ++j) C6[6 * i + j] = fma(a6[i], q[j], C6[6 * i + j]);
+      }
+      // y6 = symfold(M^T R)
+      double y6[6];
+      {
+        double G[9];
+        mtm33(M, R, G);                                   // G(a,b) = sum_p M(p,a) R(p,b)
+        y6[0] = G[0]; y6[1] = G[4]; y6[2] = G[8];
+        y6[3] = G[7] + G[5]; y6[4] = G[6] + G[2]; y6[5] = G[3] + G[1];
+      }
+      if (qr_solve<6>(C6, y6)) return 8;                 // singular: STATUS_FAIL_PHASE_MECHANICAL_STRESS_LP_DGESV
+      double X[9];
+#pragma unroll
+      for (int k = 0; k < 9; ++k) X[k] = -R[k];
+#pragma unroll 2
+      for (int s = 0; s < NS; ++s) {
+        const SysConst& c = sc[s];
+        const bool ng = (neg >> s) & 1u;
+        double cq = 0.0;
+#pragma unroll
+        for (int t = 0; t < 6; ++t) {
+          const double2 qq = c.q6[t];
+          cq = fma(ng ? qq.y : qq.x, y6[t], cq);
+        }
+        cq *= sw[s * PASS_THREADS];
+        double2 P[5];
+#pragma unroll
+        for (int k = 0; k < 5; ++k) P[k] = c.P[k];
+        const double Ps[9] = {P[0].x, P[0].y, P[1].x, P[1].y, P[2].x, P[2].y, P[3].x, P[3].y, P[4].x};
+#pragma unroll
+        for (int k = 0; k < 9; ++k) X[k] = fma(cq, Ps[k], X[k]);
+      }
+#pragma unroll
+      for (int k = 0; k < 9; ++k) sdL[k * PASS_THREADS] = X[k];
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Lg[k] = fma(dL[k], step, Lg[k]);
+    for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * PASS_THREADS], step, Lg[k]);
   }
   // Fp = (Fp0^-1 B)^-1 / det^(1/3); P = F Fp^-1 S Fp^-T; Fe = F Fp^-1  (:571-581)
-  double invFpn[9], Fpn[9];
-  mm33(invFp0, B, invFpn);
+  double F[9], invFpn[9], Fpn[9];
+  {
+    double Fp0[9], invFp0[9];
+#pragma unroll
+    for (int k = 0; k < 9; ++k) { F[k] = Fg[k * N]; Fp0[k] = Fp0g[k * N]; }
+    inv33(Fp0, invFp0);                                   // invertible: checked on entry
+    mm33(invFp0, B, invFpn);
+  }
   if (inv33(invFpn, Fpn)) return 5;
   const double cb = 1.0 / cbrt(det33(Fpn));
   double FiF[9];

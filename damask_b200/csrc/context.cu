@@ -212,6 +212,7 @@ void fill_phase_const(const HostPhase& hp, PhaseConst<NS>& pc) {
       pc.PnS[0][s][k] = hp.Ppos[s][k];
       pc.PnS[1][s][k] = hp.Pneg[s][k];
     }
+    for (int k = 0; k < 6; ++k) pc.dn[s][k] = hp.dn[s][k];
     for (int sense = 0; sense < 2; ++sense) {
       const double* Pn = sense == 0 ? hp.Ppos[s].data() : hp.Pneg[s].data();
       // tau = S : P_nS with S symmetric -> weights on (11,22,33,23,13,12)

@@ -23,6 +23,7 @@ struct PhaseConst {
   double p6[2][NS][6];     // tau = S : P_nS  ->  symmetric weights (pos/neg sense)
   double q6[2][NS][6];     // Q = C : P_nS, symmetric (11,22,33,23,13,12)
   double PnS[2][NS][9];    // P_nS (pos/neg sense), column-major
+  double dn[NS][6];        // slip direction d and plane normal n (unit): P = d (x) n
   double dg0[NS], n[NS], a[NS], h0f[NS], xiinf[NS];
   double h[NS][NS];        // slip-slip hardening matrix, row = reacting system
   int n_int[NS];           // stress exponent as integer if integral, else -1
@@ -146,7 +147,54 @@ __device__ __forceinline__ double powi(double x, int n) {
   }
   return r;
 }
-__device__ __forceinline__ double powr(double x, double e, int ei) { return ei >= 0 ? powi(x, ei) : pow(x, e); }
+// x^n for 0 <= n < 2^BITS: the products of powi in the same order, as a fixed
+// sequence of predicated steps (no data-dependent branch)
+template <int BITS>
+__device__ __forceinline__ double powi_fixed(double x, int n) {
+  double r = 1.0;
+#pragma unroll
+  for (int b = 0; b < BITS; ++b) {
+    if ((n >> b) & 1) r *= x;
+    x *= x;
+  }
+  return r;
+}
+// integral exponents are at most 64 (set up on the host), otherwise pow
+__device__ __forceinline__ double powr(double x, double e, int ei) { return ei >= 0 ? powi_fixed<7>(x, ei) : pow(x, e); }
+
+// Per slip system constants of the Newton loop, staged in shared memory once per
+// block; pairs hold the positive and negative sense so that one 16-byte load serves both.
+struct SysConst {
+  double2 p6[6];     // (p6[0][s][t], p6[1][s][t]): tau = S : P_nS
+  double2 q6[6];     // (q6[0][s][t], q6[1][s][t]): Q = C : P_nS
+  double2 P[5];      // P_s in column-major order, P[4].y unused
+  double2 dn[3];     // (d0, d1), (d2, n0), (n1, n2): P = d (x) n
+  double2 kin;       // (dot_gamma_0, n)
+  int n_int;         // stress exponent if integral (1..64), else -1
+  int pad[3];
+};
+
+template <int NS>
+__device__ __forceinline__ void stage_sys_const(const PhaseConst<NS>& pc, SysConst* sc) {
+  for (int i = threadIdx.x; i < NS; i += blockDim.x) {
+    SysConst c;
+#pragma unroll
+    for (int t = 0; t < 6; ++t) {
+      c.p6[t] = make_double2(pc.p6[0][i][t], pc.p6[1][i][t]);
+      c.q6[t] = make_double2(pc.q6[0][i][t], pc.q6[1][i][t]);
+    }
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c.P[k] = make_double2(pc.P[i][2 * k], pc.P[i][2 * k + 1]);
+    c.P[4] = make_double2(pc.P[i][8], 0.0);
+    c.dn[0] = make_double2(pc.dn[i][0], pc.dn[i][1]);
+    c.dn[1] = make_double2(pc.dn[i][2], pc.dn[i][3]);
+    c.dn[2] = make_double2(pc.dn[i][4], pc.dn[i][5]);
+    c.kin = make_double2(pc.dg0[i], pc.n[i]);
+    c.n_int = pc.n_int[i];
+    c.pad[0] = c.pad[1] = c.pad[2] = 0;
+    sc[i] = c;
+  }
+}
 
 // Hooke in Mandel notation with Fi = I: S = C66 : sym6(E), E = (Fe^T Fe - I)/2
 // (phase_hooke_SandItsTangents, phase_mechanical_elastic.f90:172-205)

@@ -42,6 +42,25 @@ void rotate_vector(const double* v, const double* q, double* o) {
   for (int i = 0; i < 3; ++i) o[i] = A * v[i] + B * qv[i] + C * c[i];
 }
 
+// unit slip direction and plane normal of every system (the factors of the Schmid matrix)
+std::vector<std::array<double, 6>> slip_dn(const dmk_phase& p) {
+  const int* famMax = p.lattice == 0 ? CF_NSLIP_FAMILY : CI_NSLIP_FAMILY;
+  std::vector<std::array<double, 6>> out;
+  int base = 0;
+  for (int f = 0; f < p.n_families; ++f) {
+    for (int s = 0; s < p.N_sl[f]; ++s) {
+      const signed char* row = p.lattice == 0 ? CF_SLIP_SYSTEMS[base + s] : CI_SLIP_SYSTEMS[base + s];
+      double d[3] = {double(row[0]), double(row[1]), double(row[2])};
+      double n[3] = {double(row[3]), double(row[4]), double(row[5])};
+      normalize(d);
+      normalize(n);
+      out.push_back({d[0], d[1], d[2], n[0], n[1], n[2]});
+    }
+    base += famMax[f];
+  }
+  return out;
+}
+
 // Schmid matrices for one sense; non-Schmid terms for cI family 1
 std::vector<std::array<double, 9>> schmid(const dmk_phase& p, int sense, bool with_nonschmid) {
   const int* famMax = p.lattice == 0 ? CF_NSLIP_FAMILY : CI_NSLIP_FAMILY;
@@ -122,6 +141,7 @@ int build_host_phase(const dmk_phase& p, HostPhase& hp, std::string& err) {
         for (int y = 0; y < 2; ++y) hp.C[ii[x] + 3 * jj[x] + 9 * kk[y] + 27 * ll[y]] = v;
     }
   hp.P = schmid(p, +1, false);
+  hp.dn = slip_dn(p);
   hp.Ppos = schmid(p, +1, true);
   hp.Pneg = schmid(p, -1, true);
   // interaction matrix

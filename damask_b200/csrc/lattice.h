@@ -14,6 +14,7 @@ struct HostPhase {
   double C66[6][6];
   double C[81];                                  // column-major 3x3x3x3
   std::vector<std::array<double, 9>> P, Ppos, Pneg;   // column-major 3x3 per system
+  std::vector<std::array<double, 6>> dn;              // unit slip direction d and plane normal n: P = d (x) n
   std::vector<double> dg0, n, a, h0f, xiinf, xi0;
   std::vector<double> h;                         // Ns x Ns, row = reacting system
   double atol_xi = 1.0, atol_gamma = 1.0e-6;
