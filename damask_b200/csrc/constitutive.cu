@@ -3,9 +3,11 @@
 //  constitutive_begin_kernel  every voxel: fused field update F <- F - r, phase restore
 //                             (mechanical_restore), substep set-up, then control up to
 //                             the first integrateStress.
-//  constitutive_pass_kernel   every voxel of the list: one integrateStress and the state
-//                             update / substep control up to the next one; voxels that
-//                             continue are appended to the next list.
+//  constitutive_stress_kernel every voxel of the list: one integrateStress (the Newton
+//                             loop; compute bound, register resident)
+//  constitutive_control_kernel every voxel of the list: state update and substep control
+//                             up to the next integrateStress (memory bound, high
+//                             occupancy); voxels that continue are appended to the next list.
 #include "kernels.cuh"
 #include "constitutive.cuh"
 
@@ -54,7 +56,7 @@ __device__ __forceinline__ void append_and_count(const Fields& f, const PassWork
 }  // namespace
 
 template <int NS>
-__global__ void __launch_bounds__(PASS_THREADS)
+__global__ void __launch_bounds__(PASS_THREADS, 4)
 constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                           int apply_update) {
@@ -103,11 +105,12 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
   append_and_count(f, w, keep, v, 0, 0);
 }
 
+// one state iteration of every listed voxel: integrateStress (integrateStateFPI:626-629)
 template <int NS>
 __global__ void __launch_bounds__(PASS_THREADS)
-constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
-                         const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
-                         const int* __restrict__ list_in, int64_t n_in) {
+constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
+                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
+                           const int* __restrict__ list_in, int64_t n_in) {
   extern __shared__ double2 smem2[];
   SysConst* sc = reinterpret_cast<SysConst*>(smem2);
   double* xs = reinterpret_cast<double*>(sc + NS) + threadIdx.x;
@@ -115,30 +118,20 @@ constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid
   __syncthreads();
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
-  bool keep = false;
-  int64_t v = 0;
-  int dstate = 0, dnewton = 0;
-  if (idx < n_in) {
-    v = list_in[idx];
-    VoxelCtl c;
-    load_ctl(w, N, v, c);
-    // one state iteration: integrateStress (integrateStateFPI:626-629)
-    ++c.it;
-    ++c.nstate;
-    dstate = 1;
+  int dnewton = 0;
+  const bool active = idx < n_in;
+  if (active) {
+    const int64_t v = list_in[idx];
+    const double step = w.sub[N + v];
     double Lp[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) Lp[k] = f.Lp[k * N + v];
 #pragma unroll
     for (int s = 0; s < NS; ++s) xs[s * PASS_THREADS] = 1.0 / f.state[s * N + v];
     double S[6], Fp[9], P[9], Fe[9];
-    const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, w.Fp0s + v, N, xs, c.step * dt, Lp, S, Fp, P, Fe,
+    const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, w.Fp0s + v, N, xs, step * dt, Lp, S, Fp, P, Fe,
                                         dnewton);
-    c.newton += dnewton;
-    if (st != 0) {
-      c.status = st;
-      c.phase = PH_CTRL;
-    } else {
+    if (st == 0) {
 #pragma unroll
       for (int k = 0; k < 9; ++k) {
         f.Lp[k * N + v] = Lp[k];
@@ -148,15 +141,49 @@ constitutive_pass_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid
       }
 #pragma unroll
       for (int k = 0; k < 6; ++k) f.S[k * N + v] = S[k];
-      c.status = 0;
-      c.phase = PH_DOT1;
     }
+    w.ctl[v] = st == 0 ? PH_DOT1 : PH_CTRL;
+    w.ctl[N + v] = st;
+    w.ctl[2 * N + v] += 1;                                 // state iteration of this substep
+    w.ctl[4 * N + v] += 1;                                 // state iterations, total
+    w.ctl[5 * N + v] += dnewton;                           // Newton iterations, total
+  }
+  // iteration counters (warp aggregated)
+  unsigned long long cs = active ? 1 : 0, cn = dnewton;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    cs += __shfl_down_sync(0xffffffffu, cs, o);
+    cn += __shfl_down_sync(0xffffffffu, cn, o);
+  }
+  if ((threadIdx.x & 31) == 0 && f.counters && cs) {
+    atomicAdd(&f.counters[1], cs);
+    atomicAdd(&f.counters[2], cn);
+  }
+}
+
+// state update and substep control of every listed voxel up to its next
+// integrateStress; the voxels that continue are appended to the next list
+template <int NS>
+__global__ void __launch_bounds__(PASS_THREADS, 4)
+constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
+                            const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
+                            const int* __restrict__ list_in, int64_t n_in) {
+  extern __shared__ double slots[];
+  double* xs = slots + threadIdx.x;
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t N = f.N;
+  bool keep = false;
+  int64_t v = 0;
+  if (idx < n_in) {
+    v = list_in[idx];
+    VoxelCtl c;
+    load_ctl(w, N, v, c);
     advance<NS>(pc, nm, f, w, v, dt, c, xs);
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
     if (!keep) finish_voxel(f, v, c);
   }
-  append_and_count(f, w, keep, v, dstate, dnewton);
+  append_and_count(f, w, keep, v, 0, 0);
 }
 
 template <int NS>
@@ -174,12 +201,16 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
-  const size_t smem = size_t(NS) * sizeof(SysConst) + size_t(2 * NS + 27) * PASS_THREADS * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(constitutive_pass_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(smem));
+  const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(2 * NS + 27) * PASS_THREADS * sizeof(double);
+  const size_t smem_c = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem_s));
+  if (e == cudaSuccess)
+    e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_c));
   if (e != cudaSuccess) return e;
   const int nb = int((n_in + PASS_THREADS - 1) / PASS_THREADS);
-  constitutive_pass_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  constitutive_stress_kernel<NS><<<nb, PASS_THREADS, smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  constitutive_control_kernel<NS><<<nb, PASS_THREADS, smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in);
   return cudaGetLastError();
 }
 

@@ -369,6 +369,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
             w.Lp0s[k * N + v] = f.Lp[k * N + v];
             w.Fp0s[k * N + v] = f.Fp[k * N + v];
           }
+#pragma unroll 12
           for (int i = 0; i < NST; ++i) w.st0s[i * N + v] = f.state[i * N + v];
         }
       } else {
@@ -380,6 +381,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
         if (c.step < 1.0)
 #pragma unroll
           for (int k = 0; k < 9; ++k) f.Lp[k * N + v] = w.Lp0s[k * N + v];
+#pragma unroll 12
         for (int i = 0; i < NST; ++i) f.state[i * N + v] = w.st0s[i * N + v];
         todo = c.step > nm.r_cutback_min;
       }
@@ -399,6 +401,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
       if (c.phase == PH_DOT0) {
         // integrateStateFPI:616-620
         if (bad) { c.status = 3; c.phase = PH_CTRL; continue; }   // STATUS_FAIL_PHASE_MECHANICAL_STATE
+#pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
           f.state[i * N + v] = fma(d, dts, w.st0s[i * N + v]);
@@ -410,6 +413,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
         // integrateStateFPI:631-646 (the stress integration of this iteration succeeded: status 0)
         if (bad) { c.phase = PH_CTRL; continue; }
         double d01 = 0.0, d12 = 0.0, d22 = 0.0;
+#pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
           const double l1 = w.dot[i * N + v];                          // dotState_last(:,1)
@@ -421,6 +425,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
         }
         const double zeta = damper(d01, d12, d22);
         bool conv = true;
+#pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double l1 = w.dot[i * N + v];
           const double d = xs[i * PASS_THREADS] * zeta + l1 * (1.0 - zeta);

@@ -169,6 +169,7 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
     const int nxt = 1 - cur;
     CK(cudaMemsetAsync(c->pcount + nxt, 0, sizeof(int), c->stream));
     CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, nxt), dt, c->plist[cur], n, c->stream));
+    ++c->launches;                                         // a pass is a stress and a control kernel
     ++c->passes;
     cur = nxt;
   }
