@@ -62,7 +62,10 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
                           int apply_update) {
   extern __shared__ double slots[];
   constexpr int NST = 2 * NS;
-  double* xs = slots + threadIdx.x;
+  double* hs = slots;
+  double* xs = slots + NS * NS + threadIdx.x;
+  stage_hardening<NS>(pc, hs);
+  __syncthreads();
   const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
   bool keep = false;
@@ -97,7 +100,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
     c.newton = 0;
     c.stepFrac = 0.0;
     c.step = 1.0 / nm.r_cutback;
-    advance<NS>(pc, nm, f, w, v, dt, c, xs);
+    advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
     if (!keep) finish_voxel(f, v, c);
@@ -169,7 +172,10 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
                             const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                             const int* __restrict__ list_in, int64_t n_in) {
   extern __shared__ double slots[];
-  double* xs = slots + threadIdx.x;
+  double* hs = slots;
+  double* xs = slots + NS * NS + threadIdx.x;
+  stage_hardening<NS>(pc, hs);
+  __syncthreads();
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
   bool keep = false;
@@ -178,7 +184,7 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
     v = list_in[idx];
     VoxelCtl c;
     load_ctl(w, N, v, c);
-    advance<NS>(pc, nm, f, w, v, dt, c, xs);
+    advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
     if (!keep) finish_voxel(f, v, c);
@@ -189,7 +195,7 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
 template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                       const PassWork& w, double dt, int apply_update, cudaStream_t s) {
-  const size_t smem = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
@@ -202,7 +208,7 @@ template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
   const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(2 * NS + 27) * PASS_THREADS * sizeof(double);
-  const size_t smem_c = size_t(2 * NS) * PASS_THREADS * sizeof(double);
+  const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem_s));
   if (e == cudaSuccess)

@@ -307,12 +307,19 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
   return 0;
 }
 
+// Hardening matrix staged in shared memory once per block (row = reacting system),
+// read with uniform addresses (broadcast) in the control kernels.
+template <int NS>
+__device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double* hs) {
+  for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.h[i / NS][i % NS];
+}
+
 // phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0) at the stored
 // stress and state of voxel v, written to this thread's slots: xi rates first, then
-// |dot_gamma|.  Returns true if any rate is NaN.
+// |dot_gamma|.  hs: the hardening matrix in shared memory.  Returns true if any rate is NaN.
 template <int NS>
-__device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double s6[6], const double* __restrict__ state,
-                                int64_t N, int64_t v, double* xs) {
+__device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double* __restrict__ hs, const double s6[6],
+                                const double* __restrict__ state, int64_t N, int64_t v, double* xs) {
   double adg[NS];
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
@@ -321,17 +328,26 @@ __device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double s6[6], co
     adg[s] = fabs(pc.dg0[s] * powr(tmax / state[s * N + v], pc.n[s], pc.n_int[s]));
   }
   bool bad = false;
-#pragma unroll
+#pragma unroll 2
   for (int l = 0; l < NS; ++l) {
     const double x = 1.0 - state[l * N + v] / pc.xiinf[l];
     const double left = copysign(powr(fabs(x), pc.a[l], pc.a_int[l]), x);
+    const double2* hrow = reinterpret_cast<const double2*>(hs + l * NS);
     double hg = 0.0;
 #pragma unroll
-    for (int k = 0; k < NS; ++k) hg = fma(pc.h[l][k], adg[k], hg);
+    for (int k = 0; k < NS / 2; ++k) {
+      const double2 hh = hrow[k];
+      hg = fma(hh.x, adg[2 * k], hg);
+      hg = fma(hh.y, adg[2 * k + 1], hg);
+    }
     const double d = pc.h0f[l] * left * hg;
-    bad |= isnan(d) || isnan(adg[l]);
+    bad |= isnan(d);
     xs[l * PASS_THREADS] = d;
-    xs[(NS + l) * PASS_THREADS] = adg[l];
+  }
+#pragma unroll
+  for (int s = 0; s < NS; ++s) {
+    bad |= isnan(adg[s]);
+    xs[(NS + s) * PASS_THREADS] = adg[s];
   }
   return bad;
 }
@@ -342,13 +358,20 @@ __device__ __forceinline__ double damper(double d01, double d12, double d22) {
   return 1.0;
 }
 
+// dotState generations of the state iteration alternate between two 2NS-plane arrays:
+// iteration it (0 = the start) stores its damped rate in array it % 2, which then holds
+// dotState_last(:,1) for iteration it + 1 and dotState_last(:,2) for iteration it + 2.
+__device__ __forceinline__ double* dot_gen(const PassWork& w, int it, int NST, int64_t N) {
+  return w.D + int64_t(it & 1) * NST * N;
+}
+
 // Advances voxel v through the control flow of phase_mechanical_constitutive and
 // integrateStateFPI until its next integrateStress (phase PH_STRESS) or its end
 // (PH_DONE).  Entered in PH_CTRL (substep control after an integration attempt) or
 // PH_DOT1 (state update after a successful integrateStress).
 template <int NS>
-__device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, const PassWork& w, int64_t v,
-                        double dt, VoxelCtl& c, double* xs) {
+__device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs, const Numerics& nm, const Fields& f,
+                        const PassWork& w, int64_t v, double dt, VoxelCtl& c, double* xs) {
   constexpr int NST = 2 * NS;
   const int64_t N = f.N;
   // every control step shrinks the substep or advances stepFrac; the bound only
@@ -396,28 +419,33 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
       double s6[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) s6[k] = f.S[k * N + v];
-      const bool bad = dot_state_slots<NS>(pc, s6, f.state, N, v, xs);
+      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state, N, v, xs);
       const double dts = c.step * dt;
       if (c.phase == PH_DOT0) {
         // integrateStateFPI:616-620
         if (bad) { c.status = 3; c.phase = PH_CTRL; continue; }   // STATUS_FAIL_PHASE_MECHANICAL_STATE
+        double* D0 = dot_gen(w, 0, NST, N) + v;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
           f.state[i * N + v] = fma(d, dts, w.st0s[i * N + v]);
-          w.dot[i * N + v] = d;
+          D0[i * N] = d;
         }
         c.it = 0;
         c.phase = PH_STRESS;
       } else {
         // integrateStateFPI:631-646 (the stress integration of this iteration succeeded: status 0)
         if (bad) { c.phase = PH_CTRL; continue; }
+        // generations: dotState of the last iteration (it - 1) and the one before (it - 2,
+        // whose storage receives the damped rate of this iteration)
+        const double* L1 = dot_gen(w, c.it + 1, NST, N) + v;
+        double* L2 = dot_gen(w, c.it, NST, N) + v;
         double d01 = 0.0, d12 = 0.0, d22 = 0.0;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
-          const double l1 = w.dot[i * N + v];                          // dotState_last(:,1)
-          const double l2 = c.it > 1 ? w.last1[i * N + v] : 0.0;      // dotState_last(:,2)
+          const double l1 = L1[i * N];                                 // dotState_last(:,1)
+          const double l2 = c.it > 1 ? L2[i * N] : 0.0;               // dotState_last(:,2)
           const double a = d - l1, b = l1 - l2;
           d12 = fma(a, b, d12);
           d22 = fma(b, b, d22);
@@ -427,14 +455,13 @@ __device__ void advance(const PhaseConst<NS>& pc, const Numerics& nm, const Fiel
         bool conv = true;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
-          const double l1 = w.dot[i * N + v];
+          const double l1 = L1[i * N];
           const double d = xs[i * PASS_THREADS] * zeta + l1 * (1.0 - zeta);
           const double st = f.state[i * N + v];
           const double r = st - w.st0s[i * N + v] - d * dts;
           const double stn = st - r;
           f.state[i * N + v] = stn;
-          w.last1[i * N + v] = l1;
-          w.dot[i * N + v] = d;
+          L2[i * N] = d;
           const double atol = i < NS ? pc.atol_xi : pc.atol_gamma;
           conv = conv && (fabs(r) <= fmax(atol, nm.eps_rel_state * fabs(stn)));
         }

@@ -142,9 +142,8 @@ PassWork pass_work(dmk_ctx* c, int out) {
   w.Fp0s = w.F0s + 9 * N;
   w.Lp0s = w.Fp0s + 9 * N;
   w.st0s = w.Lp0s + 9 * N;
-  w.dot = w.st0s + NST * N;
-  w.last1 = w.dot + NST * N;
-  w.sub = w.last1 + NST * N;
+  w.D = w.st0s + NST * N;
+  w.sub = w.D + 2 * NST * N;
   w.ctl = c->pctl;
   w.list_out = c->plist[out];
   w.count_out = c->pcount + out;

@@ -70,8 +70,7 @@ struct PassWork {
   double* Fp0s;    // 9: subFp0
   double* Lp0s;    // 9: subLp0
   double* st0s;    // 2 NS: subState0
-  double* dot;     // 2 NS: (damped) dotState of the last state iteration
-  double* last1;   // 2 NS: dotState of the iteration before (dotState_last(:,1))
+  double* D;       // 2 x 2 NS: (damped) dotState of the last two state iterations
   double* sub;     // 2: stepFrac (subFrac), step (subStep)
   int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
   int* list_out;   // voxels that continue into the next pass
@@ -160,7 +159,8 @@ __device__ __forceinline__ double powi_fixed(double x, int n) {
   return r;
 }
 // integral exponents are at most 64 (set up on the host), otherwise pow
-__device__ __forceinline__ double powr(double x, double e, int ei) { return ei >= 0 ? powi_fixed<7>(x, ei) : pow(x, e); }
+// (exponents are per slip system, so the powering loop is uniform across a warp)
+__device__ __forceinline__ double powr(double x, double e, int ei) { return ei >= 0 ? powi(x, ei) : pow(x, e); }
 
 // Per slip system constants of the Newton loop, staged in shared memory once per
 // block; pairs hold the positive and negative sense so that one 16-byte load serves both.
