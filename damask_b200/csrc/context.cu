@@ -896,6 +896,7 @@ int dmk_get_field(dmk_ctx* c, int field, double* host) {
     case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NS);
     case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NS);
     case DMK_FIELD_S:
+      if (int rc = ensure_scratch(c, 9)) return rc;
       CKL(launch_sym6_to9(c->S, c->scratch, N, c->stream));
       CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));

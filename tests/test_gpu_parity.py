@@ -130,3 +130,11 @@ def test_field_access_roundtrip(gpu, oracle_lib):
     assert g.get_field('xi_sl').shape == (g.N, 12)
     assert np.array_equal(g.get_field('F_i'), np.tile(np.eye(3).reshape(-1), (g.N, 1)))
     g.close()
+
+
+def test_stress_field_as_first_read(gpu, oracle_lib):
+    """dmk_get_field(S) as the first field read of a context: its staging buffer is
+    allocated on demand, as for every other field."""
+    g, o = pair(oracle_lib, (4, 3, 2), 2)
+    assert np.array_equal(g.get_field('S'), o.get_field('S'))
+    g.close()
