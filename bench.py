@@ -36,10 +36,19 @@ FP64_NOMINAL_TFLOPS = 37.0   # B200 FP64 (CUDA cores), datasheet figure
 
 
 def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> float:
-    """Static arithmetic count of the constitutive kernel (see DESIGN.md, FP64 FLOPs):
-    per Newton iteration 1458 + 173 Ns, per state iteration 2 Ns^2 + 57 Ns + 400,
-    per update 2 Ns^2 + 28 Ns (initial dotState)."""
-    return newton * (1458 + 173 * ns) + state * (2 * ns * ns + 57 * ns + 400) + updates * (2 * ns * ns + 28 * ns)
+    """Static FP64 FLOP count of the constitutive passes (FMA = 2):
+    per residual evaluation (Newton iteration) 264 + 56 Ns; per Newton step (Woodbury
+    6x6 system: assembly, QR, back-substitution; one per non-final Newton iteration)
+    567 + 135 Ns; per state iteration (stress start/finish, hardening, damped update)
+    455 + 86 Ns; per substep start (kinetics and hardening) 89 Ns."""
+    steps = max(newton - state, 0.0)
+    return newton * (264 + 56 * ns) + steps * (567 + 135 * ns) + state * (455 + 86 * ns) + updates * (89 * ns)
+
+
+# DRAM bytes that the constitutive kernels move per material-point update, from the ncu
+# capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (64^3 cut of this
+# workload; the traffic grows with the number of voxels)
+TRAFFIC_BYTES_PER_UPDATE = 13653
 
 
 def bc_bytes() -> int:
@@ -334,11 +343,14 @@ def main():
         'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
         'mixed_over_fp64': value / fp_value,
         'mixed_vs_fp64_P_av_rel_err_max': max(rel) if rel else None,
-        'roofline': {'bound': 'hbm', 'kernel': 'constitutive_kernel<24>', 'achieved': achieved_gbs,
-                     'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved_gbs / peaks['hbm_gbs'],
-                     'peak_source': peaks['source'], 'traffic': None, 'bytes_per_update': bpu,
-                     'fp64_tflops': fp64_tflops, 'fp64_frac_of_nominal': fp64_tflops / FP64_NOMINAL_TFLOPS,
-                     'avg_launch_ms': avg_launch_ms},
+        'roofline': {'bound': 'hbm', 'kernel': 'constitutive update (begin + stress/control pass kernels), one '
+                                               'evaluation of all voxels',
+                     'achieved': achieved_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
+                     'frac': achieved_gbs / peaks['hbm_gbs'], 'peak_source': peaks['source'],
+                     'traffic': TRAFFIC_BYTES_PER_UPDATE * mx['N'], 'traffic_source': 'ncu at 64^3, scaled by voxels',
+                     'bytes_per_update': bpu, 'avg_launch_ms': avg_launch_ms,
+                     'fp64': {'achieved': fp64_tflops, 'peak': FP64_NOMINAL_TFLOPS, 'unit': 'TFLOP/s',
+                              'frac': fp64_tflops / FP64_NOMINAL_TFLOPS, 'peak_source': 'datasheet (not measured)'}},
         'cpu_baseline': cpu,
         'e2e': {'value': e2e_value, 'unit': 'updates/s', 'h2d_bytes_per_step': bc_bytes(),
                 'd2h_bytes_per_step': mx['d2h_bytes']},
