@@ -1,0 +1,78 @@
+"""Generate ``golden_17grains_bcc.npz`` from the reference's regression resources.
+
+Run here (where the reference tree is mounted), not on the test machines:
+
+    python tests/golden/make_golden_17grains.py /root/reference
+
+Source: ``tests/integration/resources/plastic_detect_changes/`` of the reference, the
+inputs and stored result of ``tests/integration/test_plastic_detect_changes.py`` for
+the ``phenopowerlawbcc`` model: a 10x16x12 grid of 17 grains (``17grains.vti``), the
+bcc phenopowerlaw phase with non-Schmid terms (``material.yaml``), tension along x with
+mixed boundary conditions over 150 increments (``tensionX.yaml``), ``N_iter_min: 4``
+(``numerics.yaml``), and the reference's result file
+``17grains_tensionX_phenopowerlawbcc.hdf5`` (read with ``dadf5.py``).  The reference test
+compares every dataset at rtol 2.5 %, atol = max(1e-5 max|x|, 1e-6).
+
+Fixture contents: ``material`` (0-based material index per cell, x fastest), ``cells``,
+``size``, ``quaternions`` (one per material), the phase, load and numerics dictionaries
+as JSON strings, and ``xi_sl_<inc>`` / ``gamma_sl_<inc>`` for the stored increments
+0, 75 and 150 (shape (cells, N_sl)).  Also ``vti_known``: the base64 known answers of
+the reference's VTI decoder tests (``tests/unit_cpp/test_VTI.cpp``) with their decoded
+bytes, for the reader in ``damask_b200/vti.py``.
+"""
+import json
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+import yaml
+
+HERE = Path(__file__).resolve().parent
+sys.path.insert(0, str(HERE))
+sys.path.insert(0, str(HERE.parents[1]))
+
+from dadf5 import DADF5                      # noqa: E402
+from damask_b200 import vti                  # noqa: E402
+
+
+def vti_known_answers(root: Path) -> dict:
+    """The base64 strings and expected byte sequences of test_VTI.cpp."""
+    src = (root / 'tests' / 'unit_cpp' / 'test_VTI.cpp').read_text()
+    consts = {}
+    for name in ('B64_UC32', 'B64_UC64', 'B64_COMP32', 'B64_COMP64'):
+        m = re.search(name + r'\s*=\s*((?:"[^"]*"\s*)+);', src)
+        consts[name] = ''.join(re.findall(r'"([^"]*)"', m.group(1)))
+    exp = {}
+    for name in ('EXPECTED_UNCOMPRESSED', 'EXPECTED_COMPRESSED'):
+        m = re.search(name + r'\s*=\s*\{([^}]*)\}', src)
+        exp[name] = [int(x) for x in m.group(1).split(',')]
+    return {'uc32': (consts['B64_UC32'], 4, False, exp['EXPECTED_UNCOMPRESSED']),
+            'uc64': (consts['B64_UC64'], 8, False, exp['EXPECTED_UNCOMPRESSED']),
+            'comp32': (consts['B64_COMP32'], 4, True, exp['EXPECTED_COMPRESSED']),
+            'comp64': (consts['B64_COMP64'], 8, True, exp['EXPECTED_COMPRESSED'])}
+
+
+def main(root: str) -> None:
+    root = Path(root)
+    res = root / 'tests' / 'integration' / 'resources' / 'plastic_detect_changes'
+    geom = vti.load(res / '17grains.vti')
+    mat = yaml.safe_load((res / 'material.yaml').read_text())
+    quats = np.array([m['constituents'][0]['O'] for m in mat['material']], dtype=np.float64)
+    phase = mat['phase']['phenopowerlawbcc']
+    load = yaml.safe_load((res / 'tensionX.yaml').read_text())
+    numerics = yaml.safe_load((res / 'numerics.yaml').read_text())
+    out = {'material': geom.material, 'cells': np.array(geom.cells), 'size': np.array(geom.size),
+           'quaternions': quats, 'phase_json': json.dumps(phase), 'load_json': json.dumps(load),
+           'numerics_json': json.dumps(numerics),
+           'vti_known_json': json.dumps(vti_known_answers(root))}
+    f = DADF5(res / '17grains_tensionX_phenopowerlawbcc.hdf5')
+    for inc in (0, 75, 150):
+        for name in ('xi_sl', 'gamma_sl'):
+            out[f'{name}_{inc}'] = f.read(f'increment_{inc}/phase/phenopowerlawbcc/mechanical/{name}')
+    np.savez_compressed(HERE / 'golden_17grains_bcc.npz', **out)
+    print('wrote', HERE / 'golden_17grains_bcc.npz', sorted(out))
+
+
+if __name__ == '__main__':
+    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
