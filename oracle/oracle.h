@@ -11,14 +11,15 @@
  * Fortran semantics: M3 a[i][j] is M(i+1,j+1); fields are stored per voxel as
  * column-major 3x3 blocks (F11 F21 F31 F12 ...), voxels x-fastest.
  *
- * Pinning: the restatement is checked against the reference's own golden HDF5
- * regression file (tests/integration/resources/plastic_detect_changes,
- * phenopowerlaw bcc) at the reference test's tolerance, and against the
+ * Pinning: the restatement reproduces the reference's stored regression result
+ * (tests/integration/resources/plastic_detect_changes, phenopowerlaw bcc with
+ * non-Schmid terms, 150 increments; xi_sl and gamma_sl of increments 75 and 150)
+ * at the reference test's tolerance (tests/test_golden_17grains.py), and the
  * spectral self-test invariants of spectral_utilities.f90:974-1108.  The
  * reference's solver uses PETSc SNES NGMRES, which is third-party and absent;
- * the fixed-point iteration here is the Richardson form of the same residual
- * (SNES nrichardson with basic line search), so iteration counts are
- * pinned only against this restatement.
+ * the fixed point here is Anderson acceleration (Walker-Ni type II) or the
+ * Richardson form of the same residual, so iteration counts are pinned only
+ * against this restatement.
  */
 #pragma once
 #include <cstdint>
