@@ -878,6 +878,7 @@ int dmk_mech_update_coords(dmk_ctx* c) { return c ? 0 : fail(DMK_ERR_ARG, "null 
 int dmk_field_size(dmk_ctx* c, int field) {
   if (!c) return fail(DMK_ERR_ARG, "null argument");
   if (field == DMK_FIELD_XI_SL || field == DMK_FIELD_GAMMA_SL) return c->NS;
+  if (field == DMK_FIELD_O) return 4;
   if (field >= 0 && field <= DMK_FIELD_F_SOLVER) return 9;
   return fail(DMK_ERR_ARG, "unknown field");
 }
@@ -901,6 +902,17 @@ int dmk_get_field(dmk_ctx* c, int field, double* host) {
       CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * 9 * N, cudaMemcpyDeviceToHost, c->stream));
       CK(cudaStreamSynchronize(c->stream));
       return 0;
+    case DMK_FIELD_O: {
+      if (int rc = ensure_scratch(c, 4)) return rc;
+      CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
+      CKL(launch_orientations(c->Fe, N, c->scratch, c->status, c->stream));
+      int bad = 0;
+      CK(cudaMemcpyAsync(host, c->scratch, sizeof(double) * 4 * N, cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaMemcpyAsync(&bad, c->status, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+      CK(cudaStreamSynchronize(c->stream));
+      if (bad) return fail(DMK_ERR_STATE, "orientation: the rotational part of Fe is not a rotation (|det - 1| > 1e-5)");
+      return 0;
+    }
     case DMK_FIELD_FI:
     case DMK_FIELD_LI:
       for (int64_t v = 0; v < N; ++v)

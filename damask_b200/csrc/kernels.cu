@@ -418,6 +418,76 @@ cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cuda
 
 namespace dmk {
 
+// crystallite_orientations (phase.f90:659-673) per voxel: the rotational part of Fe in
+// closed form (math_rotationalPart, math.f90:1004-1044), transposed, as a unit
+// quaternion (om2qu, rotations.f90:486-514, P = -1); fromMatrix's determinant check
+// (rotations.f90:221-222) raises *bad.  Output voxel-major, 4 per voxel.
+__global__ void orientation_kernel(const double* __restrict__ Fe, int64_t N, double* __restrict__ out,
+                                   int* __restrict__ bad) {
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  double F[9];
+  for (int k = 0; k < 9; ++k) F[k] = Fe[k * N + v];
+  double C[9], FF[9];
+  mtm33(F, F, C);
+  mm33(F, F, FF);
+  const double IC1 = C[0] + C[4] + C[8];
+  const double IC2 = C[0] * C[4] + C[0] * C[8] + C[4] * C[8] - (C[3] * C[3] + C[6] * C[6] + C[7] * C[7]);
+  const double IC3 = -(C[0] * C[7] * C[7] + C[4] * C[6] * C[6] + C[8] * C[3] * C[3]) + C[0] * C[4] * C[8] +
+                     2.0 * C[3] * C[6] * C[7];
+  const double IF1 = F[0] + F[4] + F[8];
+  const double IF2 = 0.5 * (IF1 * IF1 - (FF[0] + FF[4] + FF[8]));
+  const double x = pow(fmax(IC1 * IC1 - 3.0 * IC2, 0.0), 1.5);
+  double lam[3];
+  if (fabs(x) > TINY10) {
+    const double Phi = acos(fmin(fmax((IC1 * IC1 * IC1 - 4.5 * IC1 * IC2 + 13.5 * IC3) / x, -1.0), 1.0));
+    const double TAU = 6.283185307179586476925286766559;
+    for (int k = 0; k < 3; ++k) {
+      const double l = IC1 + (2.0 * sqrt(fmax(IC1 * IC1 - 3.0 * IC2, 0.0))) * cos((Phi - TAU * double(k + 1)) / 3.0);
+      lam[k] = sqrt(fmax(l, 0.0) / 3.0);
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) lam[k] = sqrt(IC1 / 3.0);
+  }
+  const double IU1 = lam[0] + lam[1] + lam[2];
+  const double IU2 = lam[0] * lam[1] + lam[1] * lam[2] + lam[2] * lam[0];
+  double FC[9], R[9];
+  mm33(F, C, FC);
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i)
+      R[i + 3 * j] = (i == j ? IU1 * IF2 : 0.0) + (IU1 * IU1 - IU2) * F[i + 3 * j] - IU1 * IF1 * F[j + 3 * i] +
+                     IU1 * FF[j + 3 * i] - FC[i + 3 * j];
+  const double sc = pow(det33(R), -1.0 / 3.0);
+  double om[9];   // om = R^T, column-major
+  for (int j = 0; j < 3; ++j)
+    for (int i = 0; i < 3; ++i) om[i + 3 * j] = sc * R[j + 3 * i];
+  if (!(fabs(det33(om) - 1.0) <= 1.0e-5)) atomicMax(bad, 1);
+  // om(i,j) = om[(i-1) + 3 (j-1)]
+  const double t = om[0] + om[4] + om[8];
+  double q[4];
+  if (t > 0.0) {
+    const double s = 0.5 / sqrt(t + 1.0);
+    q[0] = 0.25 / s; q[1] = (om[5] - om[7]) * s; q[2] = (om[6] - om[2]) * s; q[3] = (om[1] - om[3]) * s;
+  } else if (om[0] > om[4] && om[0] > om[8]) {
+    const double s = 2.0 * sqrt(1.0 + om[0] - om[4] - om[8]);
+    q[0] = (om[5] - om[7]) / s; q[1] = 0.25 * s; q[2] = (om[3] + om[1]) / s; q[3] = (om[6] + om[2]) / s;
+  } else if (om[4] > om[8]) {
+    const double s = 2.0 * sqrt(1.0 + om[4] - om[0] - om[8]);
+    q[0] = (om[6] - om[2]) / s; q[1] = (om[3] + om[1]) / s; q[2] = 0.25 * s; q[3] = (om[7] + om[5]) / s;
+  } else {
+    const double s = 2.0 * sqrt(1.0 + om[8] - om[0] - om[4]);
+    q[0] = (om[1] - om[3]) / s; q[1] = (om[6] + om[2]) / s; q[2] = (om[7] + om[5]) / s; q[3] = 0.25 * s;
+  }
+  if (signbit(q[0])) for (int k = 0; k < 4; ++k) q[k] = -q[k];
+  for (int k = 1; k < 4; ++k) if (!(fabs(q[k]) <= TINY10)) q[k] = -q[k];
+  const double n = sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+  for (int k = 0; k < 4; ++k) out[4 * v + k] = q[k] / n;
+}
+cudaError_t launch_orientations(const double* Fe, int64_t N, double* out, int* bad, cudaStream_t s) {
+  orientation_kernel<<<int((N + 255) / 256), 256, 0, s>>>(Fe, N, out, bad);
+  return cudaGetLastError();
+}
+
 // mechanical_init per voxel (phase_mechanical.f90:249-266) with V_e = I:
 // F = F0 = Fsol = F_lastinc = I, Fp = Fp0 = O%asMatrix() (qu2om, rotations.f90:399-423),
 // Fe = Fp^T, plastic state xi = xi_0, gamma = 0 (phenopowerlaw.f90:259-285).

@@ -60,6 +60,7 @@ cudaError_t launch_init_state(const int* material, const double* quats, const do
                               double* F0, double* Fsol, double* Flast, double* Fp, double* Fp0, double* Fe, double* state,
                               double* state0, cudaStream_t s);
 cudaError_t launch_copy(const double* a, double* b, int64_t n, int nsm, cudaStream_t s);
+cudaError_t launch_orientations(const double* Fe, int64_t N, double* out /* 4 per voxel */, int* bad, cudaStream_t s);
 cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s);
 cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
 

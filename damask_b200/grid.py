@@ -22,7 +22,7 @@ from . import _lib
 from .config import LoadCase, Numerics, Phase, SolutionStruct, geometric_fraction
 
 FIELDS = {'F': 0, 'P': 1, 'F_e': 2, 'F_p': 3, 'L_p': 4, 'S': 5, 'xi_sl': 6, 'gamma_sl': 7,
-          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11}
+          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12}
 
 PRECISIONS = {'fp64': 0, 'mixed': 1}
 

@@ -120,7 +120,11 @@ enum {
   DMK_FIELD_F_LASTINC = 8,
   DMK_FIELD_FI = 9,
   DMK_FIELD_LI = 10,
-  DMK_FIELD_F_SOLVER = 11 /* solution field F of the spectral solver */
+  DMK_FIELD_F_SOLVER = 11, /* solution field F of the spectral solver */
+  DMK_FIELD_O = 12         /* orientation (4,N): unit quaternion w,x,y,z of the rotational part of Fe,
+                              as crystallite_orientations (phase.f90:659-673); get only.  A voxel whose
+                              rotation has |det - 1| > 1e-5 makes the call fail with DMK_ERR_STATE
+                              (IO_error 402 of rotations.f90:221-222). */
 };
 
 /* Create a context and run grid_mechanical_spectral_basic_init

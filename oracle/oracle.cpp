@@ -1382,7 +1382,77 @@ static std::vector<M3>* field_ptr(orc_ctx* c, int field) {
   }
 }
 
+namespace {
+// math_rotationalPart, math.f90:1004-1044 (closed form through the invariants of C = F^T F)
+M3 rotational_part(const M3& F) {
+  const M3 C = mm(tr(F), F);
+  const double IC1 = C.a[0][0] + C.a[1][1] + C.a[2][2];
+  const double IC2 = C.a[0][0] * C.a[1][1] + C.a[0][0] * C.a[2][2] + C.a[1][1] * C.a[2][2]
+                   - (C.a[0][1] * C.a[0][1] + C.a[0][2] * C.a[0][2] + C.a[1][2] * C.a[1][2]);
+  const double IC3 = -(C.a[0][0] * C.a[1][2] * C.a[1][2] + C.a[1][1] * C.a[0][2] * C.a[0][2]
+                       + C.a[2][2] * C.a[0][1] * C.a[0][1])
+                     + C.a[0][0] * C.a[1][1] * C.a[2][2] + 2.0 * C.a[0][1] * C.a[0][2] * C.a[1][2];   // math_detSym33
+  const M3 FF = mm(F, F);
+  const double IF1 = F.a[0][0] + F.a[1][1] + F.a[2][2];
+  const double IF2 = 0.5 * (IF1 * IF1 - (FF.a[0][0] + FF.a[1][1] + FF.a[2][2]));
+  const double x = std::pow(std::max(IC1 * IC1 - 3.0 * IC2, 0.0), 1.5);
+  double lam[3];
+  if (std::fabs(x) > 10.0 * TINY) {                                   // dNeq0
+    const double Phi = std::acos(std::min(std::max((IC1 * IC1 * IC1 - 4.5 * IC1 * IC2 + 13.5 * IC3) / x, -1.0), 1.0));
+    for (int k = 0; k < 3; ++k) {
+      const double l = IC1 + (2.0 * std::sqrt(std::max(IC1 * IC1 - 3.0 * IC2, 0.0))) * std::cos((Phi - TAU * double(k + 1)) / 3.0);
+      lam[k] = std::sqrt(std::max(l, 0.0) / 3.0);
+    }
+  } else {
+    for (int k = 0; k < 3; ++k) lam[k] = std::sqrt(IC1 / 3.0);
+  }
+  const double IU1 = lam[0] + lam[1] + lam[2];
+  const double IU2 = lam[0] * lam[1] + lam[1] * lam[2] + lam[2] * lam[0];
+  const M3 FT = tr(F), FFT = tr(FF), FC = mm(F, C);
+  M3 R;
+  for (int i = 0; i < 3; ++i)
+    for (int j = 0; j < 3; ++j)
+      R.a[i][j] = (i == j ? IU1 * IF2 : 0.0) + (IU1 * IU1 - IU2) * F.a[i][j] - IU1 * IF1 * FT.a[i][j]
+                + IU1 * FFT.a[i][j] - FC.a[i][j];
+  return scl(std::pow(det33(R), -1.0 / 3.0), R);
+}
+
+// om2qu, rotations.f90:486-514 (P = -1, rotations.f90:57)
+void om2qu(const M3& om, double* qu) {
+  const double t = om.a[0][0] + om.a[1][1] + om.a[2][2];
+  if (t > 0.0) {
+    const double s = 0.5 / std::sqrt(t + 1.0);
+    qu[0] = 0.25 / s; qu[1] = (om.a[2][1] - om.a[1][2]) * s; qu[2] = (om.a[0][2] - om.a[2][0]) * s; qu[3] = (om.a[1][0] - om.a[0][1]) * s;
+  } else if (om.a[0][0] > om.a[1][1] && om.a[0][0] > om.a[2][2]) {
+    const double s = 2.0 * std::sqrt(1.0 + om.a[0][0] - om.a[1][1] - om.a[2][2]);
+    qu[0] = (om.a[2][1] - om.a[1][2]) / s; qu[1] = 0.25 * s; qu[2] = (om.a[0][1] + om.a[1][0]) / s; qu[3] = (om.a[0][2] + om.a[2][0]) / s;
+  } else if (om.a[1][1] > om.a[2][2]) {
+    const double s = 2.0 * std::sqrt(1.0 + om.a[1][1] - om.a[0][0] - om.a[2][2]);
+    qu[0] = (om.a[0][2] - om.a[2][0]) / s; qu[1] = (om.a[0][1] + om.a[1][0]) / s; qu[2] = 0.25 * s; qu[3] = (om.a[1][2] + om.a[2][1]) / s;
+  } else {
+    const double s = 2.0 * std::sqrt(1.0 + om.a[2][2] - om.a[0][0] - om.a[1][1]);
+    qu[0] = (om.a[1][0] - om.a[0][1]) / s; qu[1] = (om.a[0][2] + om.a[2][0]) / s; qu[2] = (om.a[1][2] + om.a[2][1]) / s; qu[3] = 0.25 * s;
+  }
+  if (std::signbit(qu[0])) for (int k = 0; k < 4; ++k) qu[k] = -qu[k];
+  for (int k = 1; k < 4; ++k) if (!(std::fabs(qu[k]) <= 10.0 * TINY)) qu[k] = -qu[k];
+  const double n = std::sqrt(qu[0] * qu[0] + qu[1] * qu[1] + qu[2] * qu[2] + qu[3] * qu[3]);
+  for (int k = 0; k < 4; ++k) qu[k] /= n;
+}
+}  // namespace
+
+// crystallite_orientations, phase.f90:659-673: O = fromMatrix(transpose(rotationalPart(Fe)));
+// fromMatrix (rotations.f90:215-226) rejects |det - 1| > 1e-5 (IO_error 402)
+static int orientations(const orc_ctx* c, double* out) {
+  for (long v = 0; v < c->N; ++v) {
+    const M3 om = tr(rotational_part(c->Fe[v]));
+    if (!(std::fabs(det33(om) - 1.0) <= 1.0e-5)) return -2;
+    om2qu(om, out + 4 * v);
+  }
+  return 0;
+}
+
 int orc_get_field(orc_ctx* c, int field, double* out) {
+  if (field == 12) return orientations(c, out);
   if (field == 6 || field == 7) {
     const int Ns = c->pc.Ns;
     for (long v = 0; v < c->N; ++v) for (int s = 0; s < Ns; ++s) out[v * Ns + s] = c->state[v * c->sizeState + (field == 6 ? 0 : Ns) + s];

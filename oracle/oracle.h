@@ -95,7 +95,8 @@ void orc_gamma_convolution(orc_ctx*, double* field, const double aim[9]);
 double orc_divergence_rms(orc_ctx*, const double* P);
 void orc_dPdF(orc_ctx*, double dt, double* dPdF /* 81 per voxel */);
 
-/* field access: 0 F, 1 P, 2 Fe, 3 Fp, 4 Lp, 5 S, 6 xi_sl, 7 gamma_sl, 8 F_lastinc, 9 Fi, 10 Li */
+/* field access: 0 F, 1 P, 2 Fe, 3 Fp, 4 Lp, 5 S, 6 xi_sl, 7 gamma_sl, 8 F_lastinc, 9 Fi, 10 Li,
+   11 F of the solver, 12 O (orientation quaternion w,x,y,z per voxel; get only) */
 int  orc_get_field(orc_ctx*, int field, double* out);
 int  orc_set_field(orc_ctx*, int field, const double* in);
 void orc_get_aims(orc_ctx*, double F_aim[9], double P_aim[9], double C_volAvg[81], double C_minMaxAvg[81]);

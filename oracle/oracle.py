@@ -19,7 +19,7 @@ from damask_b200.config import BCStruct, LoadCase, Numerics, NumericsStruct, Pha
 HERE = Path(__file__).resolve().parent
 LIB = HERE / 'build' / 'liboracle.so'
 FIELDS = {'F': 0, 'P': 1, 'F_e': 2, 'F_p': 3, 'L_p': 4, 'S': 5, 'xi_sl': 6, 'gamma_sl': 7,
-          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11}
+          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12}
 _lib = None
 dp = C.POINTER(C.c_double)
 
@@ -114,7 +114,7 @@ class OracleSpectralBasic:
         pass
 
     def get_field(self, name: str) -> np.ndarray:
-        k = self.n_slip if name in ('xi_sl', 'gamma_sl') else 9
+        k = self.n_slip if name in ('xi_sl', 'gamma_sl') else 4 if name == 'O' else 9
         out = np.empty((self.N, k))
         if self.lib.orc_get_field(self.ctx, FIELDS[name], _p(out)) != 0:
             raise KeyError(name)

@@ -102,7 +102,7 @@ def test_solver_parity(gpu, oracle_lib, case):
     assert [s.iterations for s in sg] == [s.iterations for s in so]
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < TOL
-    for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl'):
+    for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'O'):
         assert rel(g.get_field(name), o.get_field(name)) < TOL, name
     assert rel(g.aims()['C_volAvg'], o.aims()['C_volAvg']) < TOL
     g.close()

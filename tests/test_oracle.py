@@ -143,3 +143,22 @@ def test_state_loop_bound_is_honoured(oracle_lib):
     F = np.tile((np.eye(3) + np.diag([5e-3, -2e-3, -2e-3])).reshape(-1, order='F'), (o.N, 1))
     *_, st = o.constitutive_response(F, 1.0)
     assert st != 0
+
+
+def test_orientation_output(oracle_lib):
+    """crystallite_orientations: O is the rotational part of Fe.  At init Fe is the
+    inverse lattice orientation, so O returns the input quaternions; a right stretch
+    Fe U (U symmetric positive definite) leaves it unchanged."""
+    rve = synthetic.voronoi_rve((3, 3, 2), workloads.SIZE_1MM, 4, 5)
+    o = oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, workloads.fcc_al(),
+                                       workloads.numerics_default(), threads=2)
+    q = rve.quaternions[rve.material]
+    q = q * np.sign(q[:, :1])
+    assert np.abs(o.get_field('O') - q).max() < 1e-13
+    Fe = o.get_field('F_e').reshape(-1, 3, 3, order='C')           # per voxel: column-major 3x3
+    U = np.array([[1.02, 0.003, -0.001], [0.003, 0.99, 0.002], [-0.001, 0.002, 1.005]])
+    Fe_m = np.transpose(Fe, (0, 2, 1))                              # as matrices
+    Fs = np.transpose(Fe_m @ U, (0, 2, 1)).reshape(-1, 9)
+    o.set_field('F_e', Fs)
+    assert np.abs(o.get_field('O') - q).max() < 1e-12
+    o.close()
