@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .config import BCStruct, NumericsStruct, PhaseStruct, SolutionStruct
+from .config import BCStruct, NumericsStruct, PhaseStruct, RestartStruct, SolutionStruct
 
 LIB_PATH = Path(__file__).resolve().parent / 'libdamask_b200.so'
 
@@ -18,7 +18,7 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_constitutive_response', 'dmk_update_gamma', 'dmk_gamma_convolution', 'dmk_divergence_rms',
            'dmk_dPdF', 'dmk_get_iteration_counts', 'dmk_get_counters', 'dmk_get_timings', 'dmk_destroy',
            'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop', 'dmk_phase_schmid',
-           'dmk_phase_interaction', 'dmk_field_mean_noalloc']
+           'dmk_phase_interaction', 'dmk_field_mean_noalloc', 'dmk_restart_write', 'dmk_restart_read']
 
 _lib = None
 
@@ -54,6 +54,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_set_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_field_size': (C.c_int, [vp, C.c_int]),
         'dmk_get_aims': (C.c_int, [vp, dp, dp, dp, dp, dp, dp, dp]),
+        'dmk_restart_write': (C.c_int, [vp, C.POINTER(RestartStruct)]),
+        'dmk_restart_read': (C.c_int, [vp, C.POINTER(RestartStruct)]),
         'dmk_constitutive_response': (C.c_int, [vp, dp, C.c_double, dp, dp, dp, dp, ip]),
         'dmk_update_gamma': (C.c_int, [vp, dp]),
         'dmk_gamma_convolution': (C.c_int, [vp, dp, dp]),

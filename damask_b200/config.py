@@ -49,6 +49,16 @@ class BCStruct(C.Structure):
     _fields_ = [('values', C.c_double * 9), ('mask', C.c_int * 9), ('type', C.c_int)]
 
 
+class RestartStruct(C.Structure):
+    """dmk_restart (include/damask_b200.h)."""
+    _fields_ = [('F', C.POINTER(C.c_double)), ('F_lastinc', C.POINTER(C.c_double)),
+                ('F_phase', C.POINTER(C.c_double)), ('F_p', C.POINTER(C.c_double)),
+                ('L_p', C.POINTER(C.c_double)), ('omega_plastic', C.POINTER(C.c_double)),
+                ('P_aim', C.c_double * 9), ('F_aim', C.c_double * 9), ('F_aim_lastinc', C.c_double * 9),
+                ('F_aimDot', C.c_double * 9), ('C_volAvg', C.c_double * 81), ('C_volAvgLastInc', C.c_double * 81),
+                ('C_minMaxAvg', C.c_double * 81)]
+
+
 class SolutionStruct(C.Structure):
     _fields_ = [('iterationsNeeded', C.c_int), ('converged', C.c_int), ('stagConverged', C.c_int),
                 ('residualEvals', C.c_int), ('err_div', C.c_double), ('err_BC', C.c_double),

@@ -100,6 +100,7 @@ struct dmk_ctx {
   // host copy of the solver module state (grid_mech_spectral_basic.f90:30-45)
   double F_aim[9], F_aim_lastinc[9], F_aimDot[9], P_aim[9], P_av[9];
   double C_volAvg[81], C_volAvgLastInc[81], C_minMaxAvg[81], C_minMaxAvgLastInc[81], Scomp[81];
+  double C_gamma[81];            // reference stiffness of the Gamma operator in use (C_minMaxAvgRestart)
   int stress_mask[9];
   double q_rot[4];
   double dt = 0.0;
@@ -430,7 +431,10 @@ int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
 }
 
 void update_gamma_host(dmk_ctx* c, const double* C) {
-  for (int k = 0; k < 81; ++k) c->gc.Cref[k] = C[k] / c->wgt;
+  for (int k = 0; k < 81; ++k) {
+    c->C_gamma[k] = C[k];
+    c->gc.Cref[k] = C[k] / c->wgt;
+  }
 }
 
 // D2Z of the committed P, fused divergence + Gamma, Z2D into r (FP64 or FP32 spectral path)
@@ -870,6 +874,56 @@ int dmk_materialpoint_forward(dmk_ctx* c) {
   CK(cudaMemcpyAsync(c->S0, c->S, b6, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->state0, c->state, bs, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_restart_write(dmk_ctx* c, dmk_restart* r) {
+  if (!c || !r || !r->F || !r->F_lastinc || !r->F_phase || !r->F_p || !r->L_p || !r->omega_plastic)
+    return fail(DMK_ERR_ARG, "null argument");
+  int rc;
+  if ((rc = d2h_planes(c, c->Fsol, r->F, 9)) || (rc = d2h_planes(c, c->Flast, r->F_lastinc, 9)) ||
+      (rc = d2h_planes(c, c->F, r->F_phase, 9)) || (rc = d2h_planes(c, c->Fp, r->F_p, 9)) ||
+      (rc = d2h_planes(c, c->Lp, r->L_p, 9)) || (rc = d2h_planes(c, c->state, r->omega_plastic, 2 * c->NS)))
+    return rc;
+  std::memcpy(r->P_aim, c->P_aim, sizeof r->P_aim);
+  std::memcpy(r->F_aim, c->F_aim, sizeof r->F_aim);
+  std::memcpy(r->F_aim_lastinc, c->F_aim_lastinc, sizeof r->F_aim_lastinc);
+  std::memcpy(r->F_aimDot, c->F_aimDot, sizeof r->F_aimDot);
+  std::memcpy(r->C_volAvg, c->C_volAvg, sizeof r->C_volAvg);
+  std::memcpy(r->C_volAvgLastInc, c->C_volAvgLastInc, sizeof r->C_volAvgLastInc);
+  std::memcpy(r->C_minMaxAvg, c->C_gamma, sizeof r->C_minMaxAvg);
+  return 0;
+}
+
+int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
+  if (!c || !r || !r->F || !r->F_lastinc || !r->F_phase || !r->F_p || !r->L_p || !r->omega_plastic)
+    return fail(DMK_ERR_ARG, "null argument");
+  const size_t b9 = sizeof(double) * 9 * c->N, bs = sizeof(double) * 2 * c->NS * c->N;
+  int rc;
+  // mechanical_restartRead: the converged phase state; the current values follow at the sweep
+  if ((rc = h2d_planes(c, r->F_phase, c->F0, 9)) || (rc = h2d_planes(c, r->F_p, c->Fp0, 9)) ||
+      (rc = h2d_planes(c, r->L_p, c->Lp0, 9)) || (rc = h2d_planes(c, r->omega_plastic, c->state0, 2 * c->NS)) ||
+      (rc = h2d_planes(c, r->F, c->Fsol, 9)) || (rc = h2d_planes(c, r->F_lastinc, c->Flast, 9)))
+    return rc;
+  CK(cudaMemcpyAsync(c->F, c->F0, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->Fp, c->Fp0, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->Lp, c->Lp0, b9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(c->state, c->state0, bs, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemsetAsync(c->S0, 0, sizeof(double) * 6 * c->N, c->stream));
+  CK(cudaMemsetAsync(c->S, 0, sizeof(double) * 6 * c->N, c->stream));
+  // solver module state (grid_mech_spectral_basic.f90:203-208)
+  std::memcpy(c->P_aim, r->P_aim, sizeof c->P_aim);
+  std::memcpy(c->F_aim, r->F_aim, sizeof c->F_aim);
+  std::memcpy(c->F_aim_lastinc, r->F_aim_lastinc, sizeof c->F_aim_lastinc);
+  std::memcpy(c->F_aimDot, r->F_aimDot, sizeof c->F_aimDot);
+  if ((rc = upload_scalars(c, true))) return rc;
+  // constitutive response at the loaded F, dt = 0 (:216-221), then the stored stiffnesses (:224-235)
+  int st = 0;
+  if ((rc = response(c, 0.0, &st))) return rc;
+  std::memcpy(c->C_volAvg, r->C_volAvg, sizeof c->C_volAvg);
+  std::memcpy(c->C_volAvgLastInc, r->C_volAvgLastInc, sizeof c->C_volAvgLastInc);
+  std::memcpy(c->C_minMaxAvg, r->C_minMaxAvg, sizeof c->C_minMaxAvg);
+  update_gamma_host(c, c->C_minMaxAvg);
   return 0;
 }
 

@@ -19,7 +19,7 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from .config import LoadCase, Numerics, Phase, SolutionStruct, geometric_fraction
+from .config import LoadCase, Numerics, Phase, RestartStruct, SolutionStruct, geometric_fraction
 
 FIELDS = {'F': 0, 'P': 1, 'F_e': 2, 'F_p': 3, 'L_p': 4, 'S': 5, 'xi_sl': 6, 'gamma_sl': 7,
           'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12}
@@ -98,6 +98,37 @@ class SpectralBasic:
         v = np.ascontiguousarray(values, dtype=np.float64)
         _lib.check(self.lib.dmk_set_field(self.ctx, FIELDS[name], _dp(v)))
 
+    # -- restart (grid_mech_spectral_basic.f90:198-235,378-416; phase_mechanical.f90:1248-1280) --
+    RESTART_FIELDS = ('F', 'F_lastinc', 'F_phase', 'F_p', 'L_p')
+    RESTART_AIMS = ('P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot', 'C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg')
+
+    def restart_write(self) -> dict:
+        """The data the reference writes to its restart file, as numpy arrays (per voxel,
+        voxel-major)."""
+        d = {k: np.empty((self.N, 9)) for k in self.RESTART_FIELDS}
+        d['omega_plastic'] = np.empty((self.N, 2 * self.phase.n_slip))
+        r = RestartStruct()
+        for k in self.RESTART_FIELDS + ('omega_plastic',):
+            setattr(r, k, _dp(d[k]))
+        _lib.check(self.lib.dmk_restart_write(self.ctx, C.byref(r)))
+        for k in self.RESTART_AIMS:
+            d[k] = np.array(getattr(r, k)[:])
+        return d
+
+    def restart_read(self, d: dict) -> None:
+        """Resume from restart data on this (freshly initialised) context."""
+        keep = {k: np.ascontiguousarray(d[k], dtype=np.float64) for k in self.RESTART_FIELDS + ('omega_plastic',)}
+        if keep['omega_plastic'].shape != (self.N, 2 * self.phase.n_slip) or \
+                any(keep[k].shape != (self.N, 9) for k in self.RESTART_FIELDS):
+            raise ValueError('restart data do not match the grid and phase of this context')
+        r = RestartStruct()
+        for k, v in keep.items():
+            setattr(r, k, _dp(v))
+        for k in self.RESTART_AIMS:
+            getattr(r, k)[:] = [float(x) for x in np.ravel(d[k])]
+        _lib.check(self.lib.dmk_restart_read(self.ctx, C.byref(r)))
+
+
     def aims(self) -> dict:
         bufs = {k: np.zeros(n) for k, n in (('F_aim', 9), ('F_aim_lastinc', 9), ('F_aimDot', 9), ('P_aim', 9),
                                             ('C_volAvg', 81), ('C_volAvgLastInc', 81), ('C_minMaxAvg', 81))}
@@ -175,6 +206,16 @@ class SpectralBasic:
             pass
 
 
+def save_restart(path, data: dict, increment: int) -> None:
+    """Restart data and the increment they belong to, in one .npz container."""
+    np.savez(path, increment=increment, **data)
+
+
+def load_restart(path) -> tuple[dict, int]:
+    z = np.load(path)
+    return {k: z[k] for k in z.files if k != 'increment'}, int(z['increment'])
+
+
 class NotConverged(RuntimeError):
     """IO_error 950: no convergence after the maximum number of cutbacks."""
 
@@ -202,7 +243,8 @@ class IncrementDriver:
     """
     sub_step_factor = 2
 
-    def __init__(self, solver, loadcases: list[LoadCase], N_cutback_max: int = 3, sync=None):
+    def __init__(self, solver, loadcases: list[LoadCase], N_cutback_max: int = 3, sync=None, restart_inc: int = 0):
+        self.restart_inc = restart_inc       # increments up to this one were computed before a restart
         self.solver = solver
         self.loadcases = loadcases
         self.N_cutback_max = N_cutback_max
@@ -235,6 +277,14 @@ class IncrementDriver:
         ssf = self.sub_step_factor
         Delta_t_prev = self.Delta_t
         self.Delta_t = lc.t * geometric_fraction(lc.r, inc, lc.N) * float(ssf) ** (-float(self.cut_back_level))
+        if self.total <= self.restart_inc:
+            # DAMASK_grid.f90:301-303: before the restart increment only the time advances
+            self.t = self.t + self.Delta_t
+            self._guess = True
+            if self._inc >= lc.N:
+                self._l += 1
+                self._inc = 0
+            return out
         step_fraction = 0
         while step_fraction < ssf ** self.cut_back_level:
             t_remaining = lc.t + self._t_0 - self.t
@@ -271,9 +321,10 @@ class IncrementDriver:
 
 
 def run_load_cases(solver, loadcases: list[LoadCase], N_cutback_max: int = 3, max_increments: int | None = None,
-                   on_increment=None, sync=None) -> list[IncrementStats]:
-    """Run the whole load-case list (or its first ``max_increments`` increments)."""
-    drv = IncrementDriver(solver, loadcases, N_cutback_max, sync)
+                   on_increment=None, sync=None, restart_inc: int = 0) -> list[IncrementStats]:
+    """Run the whole load-case list (or its first ``max_increments`` increments); after a
+    restart, ``restart_inc`` increments are skipped (only the time advances)."""
+    drv = IncrementDriver(solver, loadcases, N_cutback_max, sync, restart_inc)
     stats: list[IncrementStats] = []
     while not drv.done and (max_increments is None or drv.total < max_increments):
         for rec in drv.step():

@@ -157,6 +157,36 @@ int dmk_get_field(dmk_ctx* ctx, int field, double* host_out);
 int dmk_set_field(dmk_ctx* ctx, int field, const double* host_in);
 int dmk_field_size(dmk_ctx* ctx, int field);   /* doubles per voxel, or <0 */
 
+/* Restart data: what grid_mechanical_spectral_basic_restartWrite
+   (grid_mech_spectral_basic.f90:378-416) and mechanical_restartWrite
+   (phase_mechanical.f90:1248-1261) store.  Per-voxel arrays are host buffers owned by
+   the caller, voxel-major: 9 per voxel (3x3 column-major) or 2 Ns per voxel (xi then
+   gamma).  F_i and L_i are I and 0 on this path and are not carried. */
+typedef struct {
+  double* F;             /* solver F (9 N) */
+  double* F_lastinc;     /* solver F of the last converged increment (9 N) */
+  double* F_phase;       /* phase F ('F' of the phase group, 9 N) */
+  double* F_p;           /* (9 N) */
+  double* L_p;           /* (9 N) */
+  double* omega_plastic; /* plastic state (2 Ns N) */
+  double P_aim[9], F_aim[9], F_aim_lastinc[9], F_aimDot[9];
+  double C_volAvg[81], C_volAvgLastInc[81];
+  double C_minMaxAvg[81];   /* the Gamma reference stiffness in use (C_minMaxAvgRestart) */
+} dmk_restart;
+
+/* Fill r (caller-allocated arrays) from the context, after a converged increment and
+   dmk_materialpoint_forward, as the reference writes its restart file. */
+int dmk_restart_write(dmk_ctx* ctx, dmk_restart* r);
+
+/* Resume from r on a freshly initialised context with the same grid and phase, as
+   grid_mechanical_spectral_basic_init and mechanical_restartRead do for a restart
+   increment (grid_mech_spectral_basic.f90:198-235, phase_mechanical.f90:1267-1280):
+   the converged phase state (F0, Fp0, Lp0, state0) and the solver fields and aims are
+   loaded, one constitutive sweep at dt = 0 runs at the loaded F (S0 = 0, as the
+   reference keeps it), then C_volAvg, C_volAvgLastInc and C_minMaxAvg are taken from r
+   and the Gamma operator is set up with C_minMaxAvg. */
+int dmk_restart_read(dmk_ctx* ctx, const dmk_restart* r);
+
 /* Restart contract (grid_mech_spectral_basic.f90:378-416): F_aim, F_aim_lastinc,
    F_aimDot, P_aim (9 each), C_volAvg, C_volAvgLastInc, C_minMaxAvg (81 each). */
 int dmk_get_aims(dmk_ctx* ctx, double F_aim[9], double F_aim_lastinc[9], double F_aimDot[9],

@@ -127,6 +127,19 @@ def test_driver_cutback_semantics():
     assert sum(1 for c in s.calls if c[0] == 'mp_forward') == 4
 
 
+def test_driver_restart_skips_computed_increments():
+    """DAMASK_grid.f90:301-303: increments up to the restart increment only advance the
+    time; the first computed increment then starts with guess = .true. and the previous
+    increment's Delta_t."""
+    lc = workloads.tension_x(4.0, 4)
+    s = FakeSolver(fail_at=[])
+    stats = run_load_cases(s, lc, restart_inc=2)
+    forwards = [c for c in s.calls if c[0] == 'forward']
+    assert len(forwards) == 2 and s.n == 2
+    assert forwards[0] == ('forward', False, True, 1.0, 1.0)
+    assert [st.inc for st in stats] == [3, 4] and [st.t for st in stats] == [3.0, 4.0]
+
+
 def test_driver_gives_up_after_max_cutbacks():
     s = FakeSolver(fail_at=range(1, 100))
     with pytest.raises(NotConverged):
@@ -187,3 +200,17 @@ def test_replica_reductions_two_ranks():
     for p in procs:
         p.join(timeout=60)
     assert res == [(0, 11.0, 300.0), (1, 11.0, 300.0)]
+
+
+def test_plugin_object_interface():
+    """SpectralBasic (GPU) and the oracle offer the plugin procedures the driver calls and
+    the accessors the tests use."""
+    from damask_b200.grid import SpectralBasic
+    from oracle.oracle import OracleSpectralBasic
+    common = ('forward', 'solution', 'materialpoint_forward', 'update_coords', 'get_field', 'set_field',
+              'aims', 'counters', 'constitutive_response', 'gamma_convolution', 'divergence_rms', 'dPdF', 'close')
+    for cls in (SpectralBasic, OracleSpectralBasic):
+        missing = [m for m in common if not callable(getattr(cls, m, None))]
+        assert not missing, (cls.__name__, missing)
+    for m in ('restart_write', 'restart_read', 'timer_start', 'timer_stop', 'launches', 'iteration_counts'):
+        assert callable(getattr(SpectralBasic, m, None)), m
