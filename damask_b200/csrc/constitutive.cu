@@ -70,6 +70,8 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
   const int64_t N = f.N;
   bool keep = false;
   if (v < N) {
+    // F <- F - r (the Richardson/Anderson update of the previous evaluation), phase F
+    double Fn[9];
 #pragma unroll
     for (int k = 0; k < 9; ++k) {
       double x = f.Fsol[k * N + v];
@@ -78,29 +80,58 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         f.Fsol[k * N + v] = x;
       }
       f.F[k * N + v] = x;
-      const double fp0 = f.Fp0[k * N + v];
-      f.Fp[k * N + v] = fp0;                               // mechanical_restore: Fp := Fp0
-      w.Fp0s[k * N + v] = fp0;                             // subFp0 = Fp0
-      w.F0s[k * N + v] = f.F0[k * N + v];                  // subF0 = F0
-      w.Lp0s[k * N + v] = f.Lp0[k * N + v];                // subLp0 = Lp0 (Lp itself is kept as warm start)
+      Fn[k] = x;
     }
-#pragma unroll
-    for (int k = 0; k < 6; ++k) f.S[k * N + v] = f.S0[k * N + v];
-    for (int i = 0; i < NST; ++i) {
-      const double s = f.state0[i * N + v];
-      f.state[i * N + v] = s;
-      w.st0s[i * N + v] = s;
-    }
+    // mechanical_restore and the first substep control step (status ITERATING: subStep =
+    // r_cutback / r_cutback = 1, nothing to restore beyond the increment-start values,
+    // which stay where they are while stepFrac = 0; Lp is kept as warm start)
     VoxelCtl c;
-    c.phase = PH_CTRL;
-    c.status = 1;                                          // STATUS_ITERATING: first control step sets subStep = 1
+    c.status = 1;
     c.it = 0;
     c.nsub = 0;
     c.nstate = 0;
     c.newton = 0;
     c.stepFrac = 0.0;
-    c.step = 1.0 / nm.r_cutback;
-    advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
+    c.step = nm.r_cutback * (1.0 / nm.r_cutback);
+    if (!(c.step > nm.r_cutback_min)) {
+      c.phase = PH_DONE;
+    } else {
+      c.nsub = 1;
+#pragma unroll
+      for (int k = 0; k < 9; ++k) {
+        const double f0 = f.F0[k * N + v];
+        w.Fs[k * N + v] = fma(c.step, Fn[k] - f0, f0);
+      }
+      // start of the state iteration (integrateStateFPI:614-620) at S0 and state0
+      double s6[6];
+#pragma unroll
+      for (int k = 0; k < 6; ++k) s6[k] = f.S0[k * N + v];
+      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state0, N, v, xs);
+      if (bad) {
+        // STATUS_FAIL_PHASE_MECHANICAL_STATE: restore as the cutback branch does and continue
+        // with the general control flow
+#pragma unroll
+        for (int k = 0; k < 9; ++k) f.Fp[k * N + v] = f.Fp0[k * N + v];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) f.S[k * N + v] = s6[k];
+#pragma unroll 12
+        for (int i = 0; i < NST; ++i) f.state[i * N + v] = f.state0[i * N + v];
+        c.status = 3;
+        c.phase = PH_CTRL;
+        advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
+      } else {
+        const double dts = c.step * dt;
+        double* D0 = w.D + v;                               // dotState generation 0
+#pragma unroll 12
+        for (int i = 0; i < NST; ++i) {
+          const double d = xs[i * PASS_THREADS];
+          f.state[i * N + v] = fma(d, dts, f.state0[i * N + v]);
+          D0[i * N] = d;
+        }
+        // S is written by the first successful integrateStress (a failure restores S0)
+        c.phase = PH_STRESS;
+      }
+    }
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
     if (!keep) finish_voxel(f, v, c);
@@ -132,7 +163,8 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
 #pragma unroll
     for (int s = 0; s < NS; ++s) xs[s * PASS_THREADS] = 1.0 / f.state[s * N + v];
     double S[6], Fp[9], P[9], Fe[9];
-    const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, w.Fp0s + v, N, xs, step * dt, Lp, S, Fp, P, Fe,
+    const double* Fp0s = (w.sub[v] == 0.0 ? f.Fp0 : w.Fp0s) + v;   // subFp0 (see sub_start)
+    const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, Fp0s, N, xs, step * dt, Lp, S, Fp, P, Fe,
                                         dnewton);
     if (st == 0) {
 #pragma unroll

@@ -358,6 +358,18 @@ __device__ __forceinline__ double damper(double d01, double d12, double d22) {
   return 1.0;
 }
 
+// Substep-start values (subF0, subFp0, subLp0, subState0 of phase_mechanical_constitutive).
+// Until the first substep of an evaluation has advanced (stepFrac == 0) they equal the
+// increment-start values F0, Fp0, Lp0, state0 and are read from there; the first advance
+// writes them to the pass records, which are read from then on.
+struct SubStart {
+  const double *F0, *Fp0, *Lp0, *st0;
+};
+__device__ __forceinline__ SubStart sub_start(const Fields& f, const PassWork& w, double stepFrac) {
+  const bool first = stepFrac == 0.0;
+  return {first ? f.F0 : w.F0s, first ? f.Fp0 : w.Fp0s, first ? f.Lp0 : w.Lp0s, first ? f.state0 : w.st0s};
+}
+
 // dotState generations of the state iteration alternate between two 2NS-plane arrays:
 // iteration it (0 = the start) stores its damped rate in array it % 2, which then holds
 // dotState_last(:,1) for iteration it + 1 and dotState_last(:,2) for iteration it + 2.
@@ -397,22 +409,24 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         }
       } else {
         c.step = nm.r_cutback * c.step;
+        const SubStart ss = sub_start(f, w, c.stepFrac);
 #pragma unroll
-        for (int k = 0; k < 9; ++k) f.Fp[k * N + v] = w.Fp0s[k * N + v];
+        for (int k = 0; k < 9; ++k) f.Fp[k * N + v] = ss.Fp0[k * N + v];
 #pragma unroll
         for (int k = 0; k < 6; ++k) f.S[k * N + v] = f.S0[k * N + v];
         if (c.step < 1.0)
 #pragma unroll
-          for (int k = 0; k < 9; ++k) f.Lp[k * N + v] = w.Lp0s[k * N + v];
+          for (int k = 0; k < 9; ++k) f.Lp[k * N + v] = ss.Lp0[k * N + v];
 #pragma unroll 12
-        for (int i = 0; i < NST; ++i) f.state[i * N + v] = w.st0s[i * N + v];
+        for (int i = 0; i < NST; ++i) f.state[i * N + v] = ss.st0[i * N + v];
         todo = c.step > nm.r_cutback_min;
       }
       if (!todo) { c.phase = PH_DONE; break; }
       ++c.nsub;
+      const double* F0s = sub_start(f, w, c.stepFrac).F0;
 #pragma unroll
       for (int k = 0; k < 9; ++k)
-        w.Fs[k * N + v] = fma(c.step, f.F[k * N + v] - f.F0[k * N + v], w.F0s[k * N + v]);
+        w.Fs[k * N + v] = fma(c.step, f.F[k * N + v] - f.F0[k * N + v], F0s[k * N + v]);
       c.phase = PH_DOT0;
     } else {
       // dotState at the current stress and state: start (DOT0) or update (DOT1) of a state iteration
@@ -425,10 +439,11 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         // integrateStateFPI:616-620
         if (bad) { c.status = 3; c.phase = PH_CTRL; continue; }   // STATUS_FAIL_PHASE_MECHANICAL_STATE
         double* D0 = dot_gen(w, 0, NST, N) + v;
+        const double* st0 = sub_start(f, w, c.stepFrac).st0;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
-          f.state[i * N + v] = fma(d, dts, w.st0s[i * N + v]);
+          f.state[i * N + v] = fma(d, dts, st0[i * N + v]);
           D0[i * N] = d;
         }
         c.it = 0;
@@ -452,13 +467,14 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
           d01 = fma(d, l1, d01);
         }
         const double zeta = damper(d01, d12, d22);
+        const double* st0 = sub_start(f, w, c.stepFrac).st0;
         bool conv = true;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double l1 = L1[i * N];
           const double d = xs[i * PASS_THREADS] * zeta + l1 * (1.0 - zeta);
           const double st = f.state[i * N + v];
-          const double r = st - w.st0s[i * N + v] - d * dts;
+          const double r = st - st0[i * N + v] - d * dts;
           const double stn = st - r;
           f.state[i * N + v] = stn;
           L2[i * N] = d;
