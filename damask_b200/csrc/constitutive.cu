@@ -59,17 +59,17 @@ template <int NS>
 __global__ void __launch_bounds__(PASS_THREADS, 4)
 constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
-                          int apply_update) {
+                          int apply_update, int64_t v_begin, int64_t v_end) {
   extern __shared__ double slots[];
   constexpr int NST = 2 * NS;
   double* hs = slots;
   double* xs = slots + NS * NS + threadIdx.x;
   stage_hardening<NS>(pc, hs);
   __syncthreads();
-  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t v = v_begin + int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
   bool keep = false;
-  if (v < N) {
+  if (v < v_end) {
     // F <- F - r (the Richardson/Anderson update of the previous evaluation), phase F
     double Fn[9];
 #pragma unroll
@@ -226,13 +226,15 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
 
 template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                      const PassWork& w, double dt, int apply_update, cudaStream_t s) {
+                                      const PassWork& w, double dt, int apply_update, int64_t v_begin, int64_t v_end,
+                                      cudaStream_t s) {
   const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
-  const int nb = int((f.N + PASS_THREADS - 1) / PASS_THREADS);
-  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update);
+  if (v_end <= v_begin) return cudaSuccess;
+  const int nb = int((v_end - v_begin + PASS_THREADS - 1) / PASS_THREADS);
+  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update, v_begin, v_end);
   return cudaGetLastError();
 }
 
@@ -254,7 +256,7 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
 
 #define DMK_INSTANTIATE(NS)                                                                                         \
   template cudaError_t launch_constitutive_begin<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,          \
-                                                     const PassWork&, double, int, cudaStream_t);                   \
+                                                     const PassWork&, double, int, int64_t, int64_t, cudaStream_t); \
   template cudaError_t launch_constitutive_pass<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,           \
                                                     const PassWork&, double, const int*, int64_t, cudaStream_t);
 DMK_INSTANTIATE(12)

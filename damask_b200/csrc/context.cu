@@ -116,9 +116,14 @@ struct dmk_ctx {
   // constitutive pass scheme: per-voxel iteration state, voxel lists, pass counts
   double* pw = nullptr;          // Fs F0s Fp0s Lp0s (9 each), st0s dot last1 (2 NS each), stepFrac, step
   int* pctl = nullptr;           // 6 planes of per-voxel control integers
-  int* plist[2] = {nullptr, nullptr};
-  int* pcount = nullptr;         // [0], [1]: entries appended to plist[0], plist[1]
-  int* hcount = nullptr;         // pinned host copy of pcount and status
+  // The voxels are split into PASS_CHUNKS chunks whose pass loops run on their own streams,
+  // so that the latency-bound control kernel of one chunk overlaps the compute-bound stress
+  // kernel of another.  Per chunk: two voxel lists alternating between passes, their counts.
+  cudaStream_t cstream[PASS_CHUNKS] = {};   // [0] is `stream`
+  cudaEvent_t fork = nullptr, join[PASS_CHUNKS] = {};
+  int* plist[PASS_CHUNKS][2] = {};
+  int* pcount = nullptr;         // [2 h + k]: entries appended to plist[h][k]
+  int* hcount = nullptr;         // pinned host copies of the current counts of the chunks
   int64_t passes = 0;            // constitutive passes launched (all evaluations)
 };
 
@@ -134,7 +139,7 @@ Fields make_fields(dmk_ctx* c, const double* r) {
   return f;
 }
 
-PassWork pass_work(dmk_ctx* c, int out) {
+PassWork pass_work(dmk_ctx* c, int half, int out) {
   const int64_t N = c->N;
   const int NST = 2 * c->NS;
   PassWork w;
@@ -146,32 +151,60 @@ PassWork pass_work(dmk_ctx* c, int out) {
   w.D = w.st0s + NST * N;
   w.sub = w.D + 2 * NST * N;
   w.ctl = c->pctl;
-  w.list_out = c->plist[out];
-  w.count_out = c->pcount + out;
+  w.list_out = c->plist[half][out];
+  w.count_out = c->pcount + 2 * half + out;
   return w;
 }
 size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 6 * NS + 2); }
 
 template <int NS>
 int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, double dt, int apply) {
-  // pass 0: restore and control up to the first integrateStress of every voxel
-  CK(cudaMemsetAsync(c->pcount, 0, 2 * sizeof(int), c->stream));
-  CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, 0), dt, apply, c->stream));
-  ++c->passes;
-  int cur = 0;
-  for (int pass = 1;; ++pass) {
-    CK(cudaMemcpyAsync(c->hcount, c->pcount + cur, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    const int64_t n = c->hcount[0];
-    if (n == 0) break;
-    // bounded by substeps x state iterations; a runaway count means corrupted control state
-    if (pass > 100000) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
-    const int nxt = 1 - cur;
-    CK(cudaMemsetAsync(c->pcount + nxt, 0, sizeof(int), c->stream));
-    CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, nxt), dt, c->plist[cur], n, c->stream));
-    ++c->launches;                                         // a pass is a stress and a control kernel
+  constexpr int K = PASS_CHUNKS;
+  int64_t lo[K], hi[K];
+  for (int h = 0; h < K; ++h) {
+    lo[h] = c->N * h / K;
+    hi[h] = c->N * (h + 1) / K;
+  }
+  // the other streams start after everything queued on the first
+  CK(cudaEventRecord(c->fork, c->stream));
+  for (int h = 1; h < K; ++h) CK(cudaStreamWaitEvent(c->cstream[h], c->fork, 0));
+  int cur[K];
+  bool active[K];
+  for (int h = 0; h < K; ++h) {
+    // pass 0: restore and control up to the first integrateStress of every voxel of the chunk
+    cur[h] = 0;
+    CK(cudaMemsetAsync(c->pcount + 2 * h, 0, 2 * sizeof(int), c->cstream[h]));
+    CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, h, 0), dt, apply, lo[h], hi[h], c->cstream[h]));
+    CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
     ++c->passes;
-    cur = nxt;
+    active[h] = hi[h] > lo[h];
+  }
+  // each chunk advances as soon as its previous pass has ended, so the chunks pipeline
+  for (int pass = 1;;) {
+    bool any = false;
+    for (int h = 0; h < K; ++h) {
+      if (!active[h]) continue;
+      CK(cudaStreamSynchronize(c->cstream[h]));
+      const int64_t n = c->hcount[h];
+      if (n == 0) { active[h] = false; continue; }
+      any = true;
+      // bounded by substeps x state iterations; a runaway count means corrupted control state
+      if (++pass > 400000) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
+      const int nxt = 1 - cur[h];
+      CK(cudaMemsetAsync(c->pcount + 2 * h + nxt, 0, sizeof(int), c->cstream[h]));
+      CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, h, nxt), dt, c->plist[h][cur[h]], n,
+                                       c->cstream[h]));
+      ++c->launches;                                       // a pass is a stress and a control kernel
+      ++c->passes;
+      CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h + nxt, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
+      cur[h] = nxt;
+    }
+    if (!any) break;
+  }
+  // join: later work on the first stream sees all chunks
+  for (int h = 1; h < K; ++h) {
+    CK(cudaEventRecord(c->join[h], c->cstream[h]));
+    CK(cudaStreamWaitEvent(c->stream, c->join[h], 0));
   }
   return 0;
 }
@@ -582,7 +615,16 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   auto bail = [&](int code) { dmk_destroy(c); return code; };
   if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(DMK_ERR_CUDA, "cudaSetDevice failed"); }
   cudaDeviceGetAttribute(&c->nsm, cudaDevAttrMultiProcessorCount, device);
-  if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess) { delete c; return fail(DMK_ERR_CUDA, "stream"); }
+  bool ok = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) == cudaSuccess &&
+            cudaEventCreateWithFlags(&c->fork, cudaEventDisableTiming) == cudaSuccess;
+  c->cstream[0] = c->stream;
+  for (int h = 1; ok && h < PASS_CHUNKS; ++h)
+    ok = cudaStreamCreateWithFlags(&c->cstream[h], cudaStreamNonBlocking) == cudaSuccess &&
+         cudaEventCreateWithFlags(&c->join[h], cudaEventDisableTiming) == cudaSuccess;
+  if (!ok) {
+    dmk_destroy(c);
+    return fail(DMK_ERR_CUDA, "stream");
+  }
   for (auto& e : c->ev) cudaEventCreate(&e);
 
   c->nm.r_cutback_min = num->r_cutback_min; c->nm.r_cutback = num->r_cutback; c->nm.r_increase = num->r_increase;
@@ -616,10 +658,13 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
       (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)) ||
       (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 6 * size_t(N))) ||
-      (rc = dalloc(&c->plist[0], size_t(N))) || (rc = dalloc(&c->plist[1], size_t(N))) ||
-      (rc = dalloc(&c->pcount, 2)))
+      (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)))
     return bail(rc);
-  if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), 4 * sizeof(int)) != cudaSuccess) {
+  for (int h = 0; h < PASS_CHUNKS; ++h) {
+    const size_t len = size_t(N * (h + 1) / PASS_CHUNKS - N * h / PASS_CHUNKS);
+    if ((rc = dalloc(&c->plist[h][0], len)) || (rc = dalloc(&c->plist[h][1], len))) return bail(rc);
+  }
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), PASS_CHUNKS * sizeof(int)) != cudaSuccess) {
     c->hcount = nullptr;
     return bail(fail(DMK_ERR_CUDA, "cudaMallocHost failed"));
   }
@@ -1134,6 +1179,8 @@ void dmk_destroy(dmk_ctx* c) {
   if (!c) return;
   cudaSetDevice(c->device);
   if (c->stream) cudaStreamSynchronize(c->stream);
+  for (int h = 1; h < PASS_CHUNKS; ++h)
+    if (c->cstream[h]) cudaStreamSynchronize(c->cstream[h]);
   for (cufftHandle p : {c->plan_fwd, c->plan_bwd, c->plan_fwd_f, c->plan_bwd_f})
     if (p) cufftDestroy(p);
   for (void* p : {(void*)c->Fsol, (void*)c->r, (void*)c->F, (void*)c->F0, (void*)c->Fp, (void*)c->Fp0, (void*)c->Lp,
@@ -1143,14 +1190,22 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->counters, (void*)c->sc, (void*)c->scratch, (void*)c->tan_out, (void*)c->tan_idx,
                   (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work,
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
-                  (void*)c->pw, (void*)c->pctl, (void*)c->plist[0], (void*)c->plist[1], (void*)c->pcount})
+                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount})
     if (p) cudaFree(p);
+  for (auto& l : c->plist)
+    for (int* p : l)
+      if (p) cudaFree(p);
   if (c->hcount) cudaFreeHost(c->hcount);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto e : c->tev)
     if (e) cudaEventDestroy(e);
   if (c->stream) cudaStreamDestroy(c->stream);
+  for (int h = 1; h < PASS_CHUNKS; ++h) {
+    if (c->cstream[h]) cudaStreamDestroy(c->cstream[h]);
+    if (c->join[h]) cudaEventDestroy(c->join[h]);
+  }
+  if (c->fork) cudaEventDestroy(c->fork);
   delete c->pc12;
   delete c->pc18;
   delete c->pc24;

@@ -5,6 +5,7 @@
 namespace dmk {
 
 constexpr int CONST_THREADS = 128;   // block size of the per-voxel partial sums of P
+constexpr int PASS_CHUNKS = 4;       // voxel chunks whose constitutive passes run on their own streams
 constexpr int SPEC_THREADS = 256;    // spectral pointwise kernels
 
 // Solver scalars living in device memory (grid_mech_spectral_basic.f90:30-45 module state
@@ -38,7 +39,8 @@ struct Numerics2 {
 // constitutive passes (constitutive.cu)
 template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                      const PassWork& w, double dt, int apply_update, cudaStream_t s);
+                                      const PassWork& w, double dt, int apply_update, int64_t v_begin, int64_t v_end,
+                                      cudaStream_t s);
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
