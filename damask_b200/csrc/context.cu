@@ -227,9 +227,9 @@ cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o
 }
 cudaError_t run_pick(dmk_ctx* c, const Fields& f, double dt) {
   switch (c->NS) {
-    case 12: return launch_tangent_pick<12>(*c->pc12, f, dt, c->tan_idx, c->tan_out, c->stream);
-    case 18: return launch_tangent_pick<18>(*c->pc18, f, dt, c->tan_idx, c->tan_out, c->stream);
-    case 24: return launch_tangent_pick<24>(*c->pc24, f, dt, c->tan_idx, c->tan_out, c->stream);
+    case 12: return launch_tangent_pick<12>(*c->pc12, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
+    case 18: return launch_tangent_pick<18>(*c->pc18, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
+    case 24: return launch_tangent_pick<24>(*c->pc24, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
   }
   return cudaErrorInvalidValue;
 }
@@ -450,8 +450,10 @@ int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
   TangentOut o = c->tan;
   o.per_voxel = per_voxel_dev;
   CKL(run_dPdF(c, f, dt, o));
+  ++c->launches;                                           // tangent and its column sums
+  if (per_voxel_dev) CKL(launch_from_planes(c->tan.planes, per_voxel_dev, c->N, 81, c->stream));
   CKL(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
-  c->launches += 1;   // finalize + first-index kernels
+  c->launches += 2;   // reduce, finalize and first-index kernels
   CKL(run_pick(c, f, dt));
   double h[243];
   CK(cudaMemcpyAsync(h, c->tan_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
@@ -672,7 +674,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     if ((rc = dalloc(&c->specf, 2 * 9 * plane)) || (rc = dalloc(&c->Pf, 9 * N))) return bail(rc);
   c->tan_blocks = dPdF_blocks(N);
   if ((rc = dalloc(&c->tan.partials, 81 * (size_t)c->tan_blocks)) || (rc = dalloc(&c->tan.nmax, c->tan_blocks)) ||
-      (rc = dalloc(&c->tan.nmin, c->tan_blocks)) || (rc = dalloc(&c->tan.norms, N)))
+      (rc = dalloc(&c->tan.nmin, c->tan_blocks)) || (rc = dalloc(&c->tan.norms, N)) ||
+      (rc = dalloc(&c->tan.l2, size_t(tangent_reduce_doubles()))) || (rc = dalloc(&c->tan.planes, 81 * size_t(N))))
     return bail(rc);
   if (num->snes_type == 1) {
     c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
@@ -1188,7 +1191,8 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->Fdot, (void*)c->state, (void*)c->state0, (void*)c->spec, (void*)c->specf, (void*)c->Pf,
                   (void*)c->partials, (void*)c->sums, (void*)c->div_partials, (void*)c->status, (void*)c->iter,
                   (void*)c->counters, (void*)c->sc, (void*)c->scratch, (void*)c->tan_out, (void*)c->tan_idx,
-                  (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, c->fft_work,
+                  (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, (void*)c->tan.l2, (void*)c->tan.planes,
+                  c->fft_work,
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
                   (void*)c->pw, (void*)c->pctl, (void*)c->pcount})
     if (p) cudaFree(p);

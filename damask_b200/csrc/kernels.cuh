@@ -80,14 +80,17 @@ struct TangentOut {
   double* nmin;
   double* per_voxel;     // optional: 81 per voxel, voxel-major (Fortran layout)
   double* norms;         // per voxel Frobenius norm^2
+  double* planes;        // dPdF of every voxel, 81 planes (component i + 3j + 9k + 27l)
+  double* l2;            // second-level reduction buffer (tangent_reduce_doubles())
 };
+int tangent_reduce_doubles();
 template <int NS>
 cudaError_t launch_dPdF(const PhaseConst<NS>& pc, const Fields& f, double dt, const TangentOut& o, int64_t first,
                         int64_t count, cudaStream_t s);
 int dPdF_blocks(int64_t count);
 template <int NS>
 cudaError_t launch_tangent_pick(const PhaseConst<NS>& pc, const Fields& f, double dt, const long long* idx, double* out,
-                                cudaStream_t s);
+                                const double* planes, cudaStream_t s);
 cudaError_t launch_tangent_finalize(const TangentOut& o, int nparts, double wgt,
                                     double* out /* 81 vol, 81 max, 81 min, max/min norm */, long long* idx /* 2 */,
                                     int64_t first, int64_t count, cudaStream_t s);
