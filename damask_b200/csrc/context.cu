@@ -726,6 +726,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   c->q_rot[0] = 1.0; c->q_rot[1] = c->q_rot[2] = c->q_rot[3] = 0.0;
   if ((rc = upload_scalars(c, true))) return bail(rc);
 
+  // staging buffer of the field transfers, allocated here so that no transfer allocates
+  if ((rc = ensure_scratch(c, 9))) return bail(rc);
   // grid_mechanical_spectral_basic_init: constitutive response at F = I, dt = 0, then updateGamma
   int st = 0;
   if ((rc = response(c, 0.0, &st))) return bail(rc);
