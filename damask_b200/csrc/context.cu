@@ -679,7 +679,7 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     return bail(rc);
   if (num->snes_type == 1) {
     c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
-    c->aa_blocks = c->nsm * 4;
+    c->aa_blocks = c->nsm * 8;
     if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * 9 * N)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * 9 * N)) ||
         (rc = dalloc(&c->aa_Rprev, 9 * N)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
         (rc = dalloc(&c->aa_out, 4 * AA_MAX)))

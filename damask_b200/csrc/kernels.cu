@@ -556,6 +556,7 @@ aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, d
   double g[AA_CHUNK], b[AA_CHUNK];
 #pragma unroll
   for (int q = 0; q < AA_CHUNK; ++q) { g[q] = 0.0; b[q] = 0.0; }
+#pragma unroll 2
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
     const double r = R[e];
     double dn = 0.0;
@@ -590,12 +591,20 @@ aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, d
   }
 }
 
-__global__ void aa_reduce_kernel(const double* __restrict__ partials, int nblocks, double* __restrict__ out) {
-  const int t = threadIdx.x;
-  if (t >= 2 * AA_CHUNK) return;
+// 16 lanes per output, each summing every 16th block partial, then a fixed-order combine
+__global__ void __launch_bounds__(256) aa_reduce_kernel(const double* __restrict__ partials, int nblocks,
+                                                        double* __restrict__ out) {
+  __shared__ double acc[16][2 * AA_CHUNK];
+  const int t = threadIdx.x, q = t % (2 * AA_CHUNK), lane = t / (2 * AA_CHUNK);
   double s = 0.0;
-  for (int b = 0; b < nblocks; ++b) s += partials[int64_t(b) * 2 * AA_CHUNK + t];
-  out[t] = s;
+  for (int b = lane; b < nblocks; b += 16) s += partials[int64_t(b) * 2 * AA_CHUNK + q];
+  acc[lane][q] = s;
+  __syncthreads();
+  if (t < 2 * AA_CHUNK) {
+    double tot = 0.0;
+    for (int l = 0; l < 16; ++l) tot += acc[l][t];
+    out[t] = tot;
+  }
 }
 
 cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,
@@ -610,7 +619,7 @@ cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int
     // recompute it from R - Rprev without writing
     const int ws = write_slot;
     aa_dots_kernel<<<nblocks, 256, 0, s>>>(R, Rprev, dR, n, ws, sl, partials);
-    aa_reduce_kernel<<<1, 32, 0, s>>>(partials, nblocks, out + chunk * 2 * AA_CHUNK);
+    aa_reduce_kernel<<<1, 256, 0, s>>>(partials, nblocks, out + chunk * 2 * AA_CHUNK);
     done += sl.n;
     ++chunk;
   } while (done < nslots);
@@ -627,6 +636,7 @@ __global__ void __launch_bounds__(256)
 aa_update_kernel(double* __restrict__ X, const double* __restrict__ R, double* __restrict__ Rprev,
                  double* __restrict__ dX, const double* __restrict__ dR, int64_t n, int new_slot,
                  const __grid_constant__ AAUpdate u) {
+#pragma unroll 2
   for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
     const double x = X[e], r = R[e];
     double xn = x - r;
