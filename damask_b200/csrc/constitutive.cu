@@ -106,7 +106,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
       double s6[6];
 #pragma unroll
       for (int k = 0; k < 6; ++k) s6[k] = f.S0[k * N + v];
-      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state0, N, v, xs);
+      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state0, N, v, xs, nullptr);
       if (bad) {
         // STATUS_FAIL_PHASE_MECHANICAL_STATE: restore as the cutback branch does and continue
         // with the general control flow
@@ -176,6 +176,8 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
       }
 #pragma unroll
       for (int k = 0; k < 6; ++k) f.S[k * N + v] = S[k];
+#pragma unroll
+      for (int s = 0; s < NS; ++s) w.adg[s * N + v] = xs[(2 * NS + s) * PASS_THREADS];
     }
     w.ctl[v] = st == 0 ? PH_DOT1 : PH_CTRL;
     w.ctl[N + v] = st;
@@ -241,7 +243,7 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
-  const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(2 * NS + 27) * PASS_THREADS * sizeof(double);
+  const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * PASS_THREADS * sizeof(double);
   const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem_s));

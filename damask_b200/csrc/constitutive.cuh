@@ -109,15 +109,16 @@ __device__ __forceinline__ bool qr_solve(double* A, double* b) {
 // F and Fp0 point at voxel v's planes (stride N); they are read at the start and again
 // for the final Fp / P so that no copy stays in registers through the Newton loop.
 // xs: this thread's shared-memory slots (stride PASS_THREADS): 1/xi (NS entries), the
-// Newton weights dt*dgamma (NS), then A, the last accepted Lp guess and the Newton
-// step (9 each).  Lp (in/out) is the warm start and, on success, the result; S, Fp,
-// P and Fe are written only on success.
+// Newton weights dt*dgamma (NS), |dot_gamma| of the last residual evaluation (NS), then
+// A, the last accepted Lp guess and the Newton step (9 each).  Lp (in/out) is the warm
+// start and, on success, the result; S, Fp, P and Fe are written only on success.
 template <int NS>
 __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __restrict__ sc, const Numerics& nm,
                                 const double* Fg, const double* Fp0g, int64_t N, double* xs, double dt, double* Lp,
                                 double* S, double* Fp, double* Pout, double* Feout, int& newton) {
   double* const sw = xs + NS * PASS_THREADS;
-  double* const sA = xs + 2 * NS * PASS_THREADS;
+  double* const sg = xs + 2 * NS * PASS_THREADS;
+  double* const sA = xs + 3 * NS * PASS_THREADS;
   double* const sLo = sA + 9 * PASS_THREADS;
   double* const sdL = sLo + 9 * PASS_THREADS;
   {
@@ -179,6 +180,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
       if (!(g > 0.0)) neg |= 1u << s;
       sw[s * PASS_THREADS] = dt * dg;
+      sg[s * PASS_THREADS] = fabs(g);
       double2 P[5];
 #pragma unroll
       for (int k = 0; k < 5; ++k) P[k] = c.P[k];
@@ -314,23 +316,36 @@ __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double
   for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.h[i / NS][i % NS];
 }
 
+// Slots of the stress kernel (stride PASS_THREADS): 1/xi [0, NS), Newton weights
+// [NS, 2NS), |dot_gamma| [2NS, 3NS), Newton 3x3 scratch [3NS, 3NS + 27).
+template <int NS>
+__host__ __device__ constexpr int stress_slots() { return 3 * NS + 27; }
+
 // phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0) at the stored
 // stress and state of voxel v, written to this thread's slots: xi rates first, then
-// |dot_gamma|.  hs: the hardening matrix in shared memory.  Returns true if any rate is NaN.
+// |dot_gamma|.  hs: the hardening matrix in shared memory.  adg_in (stride N), when given,
+// holds |dot_gamma| at this stress and state already (the kinetics of the converged
+// integrateStress); otherwise the kinetics are evaluated.  Returns true if any rate is NaN.
 template <int NS>
 __device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double* __restrict__ hs, const double s6[6],
-                                const double* __restrict__ state, int64_t N, int64_t v, double* xs) {
+                                const double* __restrict__ state, int64_t N, int64_t v, double* xs,
+                                const double* __restrict__ adg_in) {
   double adg[NS];
+  if (adg_in) {
 #pragma unroll
-  for (int s = 0; s < NS; ++s) {
-    const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
-    const double tmax = tp > tn ? tp : tn;
-    adg[s] = fabs(pc.dg0[s] * powr(tmax / state[s * N + v], pc.n[s], pc.n_int[s]));
+    for (int s = 0; s < NS; ++s) adg[s] = adg_in[s * N];
+  } else {
+#pragma unroll
+    for (int s = 0; s < NS; ++s) {
+      const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
+      const double tmax = tp > tn ? tp : tn;
+      adg[s] = fabs(pc.dg0[s] * powr(tmax / state[s * N + v], pc.n[s], pc.n_int[s]));
+    }
   }
   bool bad = false;
 #pragma unroll 2
   for (int l = 0; l < NS; ++l) {
-    const double x = 1.0 - state[l * N + v] / pc.xiinf[l];
+    const double x = fma(-state[l * N + v], pc.ixiinf[l], 1.0);  // 1 - xi/xi_inf
     const double left = copysign(powr(fabs(x), pc.a[l], pc.a_int[l]), x);
     const double2* hrow = reinterpret_cast<const double2*>(hs + l * NS);
     double hg = 0.0;
@@ -429,11 +444,14 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         w.Fs[k * N + v] = fma(c.step, f.F[k * N + v] - f.F0[k * N + v], F0s[k * N + v]);
       c.phase = PH_DOT0;
     } else {
-      // dotState at the current stress and state: start (DOT0) or update (DOT1) of a state iteration
+      // dotState at the current stress and state: start (DOT0) or update (DOT1) of a state
+      // iteration; after a converged integrateStress its kinetics are stored already
       double s6[6];
+      const bool after_stress = c.phase == PH_DOT1;
+      if (!after_stress)
 #pragma unroll
-      for (int k = 0; k < 6; ++k) s6[k] = f.S[k * N + v];
-      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state, N, v, xs);
+        for (int k = 0; k < 6; ++k) s6[k] = f.S[k * N + v];
+      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state, N, v, xs, after_stress ? w.adg + v : nullptr);
       const double dts = c.step * dt;
       if (c.phase == PH_DOT0) {
         // integrateStateFPI:616-620

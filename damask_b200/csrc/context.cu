@@ -149,13 +149,14 @@ PassWork pass_work(dmk_ctx* c, int half, int out) {
   w.Lp0s = w.Fp0s + 9 * N;
   w.st0s = w.Lp0s + 9 * N;
   w.D = w.st0s + NST * N;
-  w.sub = w.D + 2 * NST * N;
+  w.adg = w.D + 2 * NST * N;
+  w.sub = w.adg + int64_t(c->NS) * N;
   w.ctl = c->pctl;
   w.list_out = c->plist[half][out];
   w.count_out = c->pcount + 2 * half + out;
   return w;
 }
-size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 6 * NS + 2); }
+size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 7 * NS + 2); }
 
 template <int NS>
 int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, double dt, int apply) {
@@ -270,6 +271,7 @@ void fill_phase_const(const HostPhase& hp, PhaseConst<NS>& pc) {
     pc.a[s] = hp.a[s];
     pc.h0f[s] = hp.h0f[s];
     pc.xiinf[s] = hp.xiinf[s];
+    pc.ixiinf[s] = 1.0 / hp.xiinf[s];
     pc.n_int[s] = (hp.n[s] == std::floor(hp.n[s]) && hp.n[s] >= 1.0 && hp.n[s] <= 64.0) ? int(hp.n[s]) : -1;
     pc.a_int[s] = (hp.a[s] == std::floor(hp.a[s]) && hp.a[s] >= 0.0 && hp.a[s] <= 64.0) ? int(hp.a[s]) : -1;
     for (int k = 0; k < NS; ++k) pc.h[s][k] = hp.h[s * NS + k];

@@ -24,7 +24,7 @@ struct PhaseConst {
   double q6[2][NS][6];     // Q = C : P_nS, symmetric (11,22,33,23,13,12)
   double PnS[2][NS][9];    // P_nS (pos/neg sense), column-major
   double dn[NS][6];        // slip direction d and plane normal n (unit): P = d (x) n
-  double dg0[NS], n[NS], a[NS], h0f[NS], xiinf[NS];
+  double dg0[NS], n[NS], a[NS], h0f[NS], xiinf[NS], ixiinf[NS];
   double h[NS][NS];        // slip-slip hardening matrix, row = reacting system
   int n_int[NS];           // stress exponent as integer if integral, else -1
   int a_int[NS];           // hardening exponent as integer if integral, else -1
@@ -71,6 +71,7 @@ struct PassWork {
   double* Lp0s;    // 9: subLp0
   double* st0s;    // 2 NS: subState0
   double* D;       // 2 x 2 NS: (damped) dotState of the last two state iterations
+  double* adg;     // NS: |dot_gamma| at the stress of the last converged integrateStress
   double* sub;     // 2: stepFrac (subFrac), step (subStep)
   int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
   int* list_out;   // voxels that continue into the next pass
