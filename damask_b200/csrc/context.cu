@@ -95,6 +95,10 @@ struct dmk_ctx {
   int tan_blocks = 0;
   void* fft_work = nullptr;
   cufftHandle plan_fwd = 0, plan_bwd = 0, plan_fwd_f = 0, plan_bwd_f = 0;
+  cufftHandle plan_vec_bwd = 0; // Z2D of a 3-component (vector) spectrum, updateCoords
+  double* xp = nullptr;         // cell-centre coordinates, 3 per voxel (discretization_IPcoords)
+  double* xn = nullptr;         // node coordinates, 3 per node (discretization_NodeCoords)
+  double* favg = nullptr;       // average F of the last updateCoords (9)
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   // host copy of the solver module state (grid_mech_spectral_basic.f90:30-45)
@@ -128,6 +132,8 @@ struct dmk_ctx {
 };
 
 namespace {
+
+int64_t node_count(const dmk_ctx* c) { return int64_t(c->cells[0] + 1) * (c->cells[1] + 1) * (c->cells[2] + 1); }
 
 Fields make_fields(dmk_ctx* c, const double* r) {
   Fields f;
@@ -393,13 +399,16 @@ int make_plans(dmk_ctx* c) {
   int inemb[3] = {c->cells[2], c->cells[1], c->cells[0]};
   int onemb[3] = {c->cells[2], c->cells[1], red0};
   const long long plane = (long long)red0 * c->cells[1] * c->cells[2];
-  size_t w1 = 0, w2 = 0, w3 = 0, w4 = 0;
+  size_t w1 = 0, w2 = 0, w3 = 0, w4 = 0, w5 = 0;
   CKF(cufftCreate(&c->plan_fwd));
   CKF(cufftCreate(&c->plan_bwd));
+  CKF(cufftCreate(&c->plan_vec_bwd));
   CKF(cufftSetAutoAllocation(c->plan_fwd, 0));
   CKF(cufftSetAutoAllocation(c->plan_bwd, 0));
+  CKF(cufftSetAutoAllocation(c->plan_vec_bwd, 0));
   CKF(cufftMakePlanMany(c->plan_fwd, 3, n, inemb, 1, int(c->N), onemb, 1, int(plane), CUFFT_D2Z, 9, &w1));
   CKF(cufftMakePlanMany(c->plan_bwd, 3, n, onemb, 1, int(plane), inemb, 1, int(c->N), CUFFT_Z2D, 9, &w2));
+  CKF(cufftMakePlanMany(c->plan_vec_bwd, 3, n, onemb, 1, int(plane), inemb, 1, int(c->N), CUFFT_Z2D, 3, &w5));
   if (c->precision == DMK_PRECISION_MIXED) {
     CKF(cufftCreate(&c->plan_fwd_f));
     CKF(cufftCreate(&c->plan_bwd_f));
@@ -408,12 +417,14 @@ int make_plans(dmk_ctx* c) {
     CKF(cufftMakePlanMany(c->plan_fwd_f, 3, n, inemb, 1, int(c->N), onemb, 1, int(plane), CUFFT_R2C, 9, &w3));
     CKF(cufftMakePlanMany(c->plan_bwd_f, 3, n, onemb, 1, int(plane), inemb, 1, int(c->N), CUFFT_C2R, 9, &w4));
   }
-  const size_t w = std::max(std::max(w1, w2), std::max(w3, w4));
+  const size_t w = std::max(std::max(std::max(w1, w2), std::max(w3, w4)), w5);
   if (w) CK(cudaMalloc(&c->fft_work, w));
   CKF(cufftSetWorkArea(c->plan_fwd, c->fft_work));
   CKF(cufftSetWorkArea(c->plan_bwd, c->fft_work));
+  CKF(cufftSetWorkArea(c->plan_vec_bwd, c->fft_work));
   CKF(cufftSetStream(c->plan_fwd, c->stream));
   CKF(cufftSetStream(c->plan_bwd, c->stream));
+  CKF(cufftSetStream(c->plan_vec_bwd, c->stream));
   if (c->precision == DMK_PRECISION_MIXED) {
     CKF(cufftSetWorkArea(c->plan_fwd_f, c->fft_work));
     CKF(cufftSetWorkArea(c->plan_bwd_f, c->fft_work));
@@ -662,7 +673,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
       (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)) ||
       (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 6 * size_t(N))) ||
-      (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)))
+      (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)) || (rc = dalloc(&c->xp, 3 * size_t(N))) ||
+      (rc = dalloc(&c->xn, 3 * size_t(node_count(c)))) || (rc = dalloc(&c->favg, 9)))
     return bail(rc);
   for (int h = 0; h < PASS_CHUNKS; ++h) {
     const size_t len = size_t(N * (h + 1) / PASS_CHUNKS - N * h / PASS_CHUNKS);
@@ -730,6 +742,12 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
 
   // staging buffer of the field transfers, allocated here so that no transfer allocates
   if ((rc = ensure_scratch(c, 9))) return bail(rc);
+  // discretization_init: current coordinates = undeformed coordinates (IPcoordinates0, nodes0)
+  {
+    const double step[3] = {geomSize[0] / cells[0], geomSize[1] / cells[1], geomSize[2] / cells[2]};
+    cudaError_t e = launch_coords(nullptr, nullptr, c->cells, step, c->wgt, c->xp, c->xn, c->stream);
+    if (e != cudaSuccess) return bail(fail(DMK_ERR_CUDA, std::string("init coordinates: ") + cudaGetErrorString(e)));
+  }
   // grid_mechanical_spectral_basic_init: constitutive response at F = I, dt = 0, then updateGamma
   int st = 0;
   if ((rc = response(c, 0.0, &st))) return bail(rc);
@@ -979,7 +997,30 @@ int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
   return 0;
 }
 
-int dmk_mech_update_coords(dmk_ctx* c) { return c ? 0 : fail(DMK_ERR_ARG, "null argument"); }
+// grid_mechanical_spectral_basic_updateCoords -> utilities_updateCoords
+// (spectral_utilities.f90:857-968) on the solver's F field: D2Z of F, u_hat = F_hat xi / (conj(-xi) . xi),
+// Z2D of u into the staging buffer, then cell-centre and node coordinates.
+int dmk_mech_update_coords(dmk_ctx* c) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (int rc = ensure_scratch(c, 3)) return rc;
+  const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
+  const double step[3] = {c->geom[0] / c->cells[0], c->geom[1] / c->cells[1], c->geom[2] / c->cells[2]};
+  CKF(cufftExecD2Z(c->plan_fwd, c->Fsol, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
+  CKL(launch_coords_spec(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->wgt, c->favg, c->stream));
+  CKF(cufftExecZ2D(c->plan_vec_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), c->scratch));
+  CKL(launch_coords(c->scratch, c->favg, c->cells, step, c->wgt, c->xp, c->xn, c->stream));
+  c->launches += 2;   // each launcher above issues two kernels
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_get_coords(dmk_ctx* c, double* ip, double* nodes) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (ip) CK(cudaMemcpyAsync(ip, c->xp, sizeof(double) * 3 * c->N, cudaMemcpyDeviceToHost, c->stream));
+  if (nodes) CK(cudaMemcpyAsync(nodes, c->xn, sizeof(double) * 3 * node_count(c), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
 
 int dmk_field_size(dmk_ctx* c, int field) {
   if (!c) return fail(DMK_ERR_ARG, "null argument");
@@ -1188,7 +1229,7 @@ void dmk_destroy(dmk_ctx* c) {
   if (c->stream) cudaStreamSynchronize(c->stream);
   for (int h = 1; h < PASS_CHUNKS; ++h)
     if (c->cstream[h]) cudaStreamSynchronize(c->cstream[h]);
-  for (cufftHandle p : {c->plan_fwd, c->plan_bwd, c->plan_fwd_f, c->plan_bwd_f})
+  for (cufftHandle p : {c->plan_fwd, c->plan_bwd, c->plan_fwd_f, c->plan_bwd_f, c->plan_vec_bwd})
     if (p) cufftDestroy(p);
   for (void* p : {(void*)c->Fsol, (void*)c->r, (void*)c->F, (void*)c->F0, (void*)c->Fp, (void*)c->Fp0, (void*)c->Lp,
                   (void*)c->Lp0, (void*)c->S, (void*)c->S0, (void*)c->Fe, (void*)c->P, (void*)c->Pnew, (void*)c->Flast,
@@ -1198,7 +1239,7 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, (void*)c->tan.l2, (void*)c->tan.planes,
                   c->fft_work,
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
-                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount})
+                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->xp, (void*)c->xn, (void*)c->favg})
     if (p) cudaFree(p);
   for (auto& l : c->plist)
     for (int* p : l)

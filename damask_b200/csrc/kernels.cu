@@ -659,3 +659,147 @@ cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* 
 }
 
 }  // namespace dmk
+
+namespace dmk {
+
+// ------------------------------------------------------------------ coordinates
+// utilities_updateCoords (spectral_utilities.f90:857-968).  Fourier part: with the
+// second-derivative frequencies xi = i a, a = 2 pi k / L (Nyquist kept, :315-333),
+// u_hat = F_hat xi / (conj(-xi) . xi) = -i (F_hat a) / |a|^2 per stored point, written to
+// planes 0..2 of the spectrum; k = 0 gives 0 and the average F = Re F_hat(0) wgt.
+__global__ void __launch_bounds__(SPEC_THREADS)
+coords_spec_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                   double wgt, double* __restrict__ favg) {
+  const int red0 = n0 / 2 + 1;
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (idx >= plane) return;
+  const int kx = int(idx % red0);
+  const int64_t rest = idx / red0;
+  const int ky = int(rest % n1);
+  const int kz = int(rest / n1);
+  const double TAU = 6.283185307179586;
+  const double a[3] = {TAU * double(kx) / L0, TAU * double(ky > n1 / 2 ? ky - n1 : ky) / L1,
+                       TAU * double(kz > n2 / 2 ? kz - n2 : kz) / L2};
+  double2 F[9];
+#pragma unroll
+  for (int c = 0; c < 9; ++c) F[c] = S[c * plane + idx];
+  if (idx == 0) {
+#pragma unroll
+    for (int c = 0; c < 9; ++c) favg[c] = F[c].x * wgt;
+#pragma unroll
+    for (int l = 0; l < 3; ++l) S[l * plane] = make_double2(0.0, 0.0);
+    return;
+  }
+  const double a2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    double sr = 0.0, si = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+      sr = fma(F[l + 3 * m].x, a[m], sr);
+      si = fma(F[l + 3 * m].y, a[m], si);
+    }
+    // -i (sr + i si) / a2
+    S[l * plane + idx] = make_double2(si / a2, -sr / a2);
+  }
+}
+
+// The stored planes kx = 0 and kx = n0/2 (even n0) of u_hat are not Hermitian in (ky, kz) at
+// Nyquist frequencies (a keeps its sign there).  The reference's C2R uses their real part after
+// the (ky, kz) inverse, i.e. their Hermitian part H = (u(k) + conj(u(-k))) / 2; writing H makes
+// the input exactly Hermitian, so the transform below is defined by the data alone.
+__global__ void __launch_bounds__(SPEC_THREADS)
+coords_hermitian_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n2) {
+  const int red0 = n0 / 2 + 1;
+  const int kx = blockIdx.y == 0 ? 0 : n0 / 2;
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= int64_t(n1) * n2) return;
+  const int ky = int(t % n1), kz = int(t / n1);
+  const int py = (n1 - ky) % n1, pz = (n2 - kz) % n2;
+  const int64_t tp = int64_t(pz) * n1 + py;
+  if (tp < t) return;
+  const int64_t i0 = t * red0 + kx, i1 = tp * red0 + kx;
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    const double2 u = S[l * plane + i0], v = S[l * plane + i1];
+    const double hr = 0.5 * (u.x + v.x), hi = 0.5 * (u.y - v.y);
+    S[l * plane + i0] = make_double2(hr, hi);
+    S[l * plane + i1] = make_double2(hr, -hi);
+  }
+}
+
+// Cell centres x_p = u + Favg (step (ijk - 1/2)) (:955-959), u = C2R output * wgt (planes,
+// stride N; null = 0).  Output 3 per voxel, x fastest.
+__global__ void coords_point_kernel(const double* __restrict__ u, const double* __restrict__ favg, int n0, int n1,
+                                    int n2, double s0, double s1, double s2, double wgt, double* __restrict__ xp) {
+  const int64_t N = int64_t(n0) * n1 * n2;
+  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (v >= N) return;
+  const double p[3] = {s0 * (double(v % n0 + 1) - 0.5), s1 * (double((v / n0) % n1 + 1) - 0.5),
+                       s2 * (double(v / (int64_t(n0) * n1) + 1) - 0.5)};
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    double x = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) x = fma(favg ? favg[l + 3 * m] : double(l == m), p[m], x);
+    xp[3 * v + l] = (u ? u[l * N + v] * wgt : 0.0) + x;
+  }
+}
+
+// Nodes x_n = Favg (step ijk) + mean of u over the 8 cells sharing the node, periodic
+// (:944-952).  Nodes (n0+1)(n1+1)(n2+1), x fastest, 3 per node.
+__global__ void coords_node_kernel(const double* __restrict__ u, const double* __restrict__ favg, int n0, int n1,
+                                   int n2, double s0, double s1, double s2, double wgt, double* __restrict__ xn) {
+  const int64_t N = int64_t(n0) * n1 * n2;
+  const int64_t M = int64_t(n0 + 1) * (n1 + 1) * (n2 + 1);
+  const int64_t t = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  if (t >= M) return;
+  const int i = int(t % (n0 + 1)), j = int((t / (n0 + 1)) % (n1 + 1)), k = int(t / (int64_t(n0 + 1) * (n1 + 1)));
+  const double p[3] = {s0 * double(i), s1 * double(j), s2 * double(k)};
+  double x[3];
+#pragma unroll
+  for (int l = 0; l < 3; ++l) {
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < 3; ++m) s = fma(favg ? favg[l + 3 * m] : double(l == m), p[m], s);
+    x[l] = s;
+  }
+  if (u) {
+    // neighbour order of the reference: (0,0,0) (1,0,0) (1,1,0) (0,1,0) (0,0,1) (1,0,1) (1,1,1) (0,1,1)
+    const int di[8] = {0, 1, 1, 0, 0, 1, 1, 0}, dj[8] = {0, 0, 1, 1, 0, 0, 1, 1}, dk[8] = {0, 0, 0, 0, 1, 1, 1, 1};
+#pragma unroll
+    for (int n = 0; n < 8; ++n) {
+      const int a = (i + di[n] - 1 + n0) % n0, b = (j + dj[n] - 1 + n1) % n1, c = (k + dk[n] - 1 + n2) % n2;
+      const int64_t w = (int64_t(c) * n1 + b) * n0 + a;
+#pragma unroll
+      for (int l = 0; l < 3; ++l) x[l] += (u[l * N + w] * wgt) * 0.125;
+    }
+  }
+#pragma unroll
+  for (int l = 0; l < 3; ++l) xn[3 * t + l] = x[l];
+}
+
+cudaError_t launch_coords_spec(double* spec, int n0, int n1, int n2, const double L[3], double wgt, double* favg,
+                               cudaStream_t s) {
+  const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
+  double2* S = reinterpret_cast<double2*>(spec);
+  coords_spec_kernel<<<unsigned((plane + SPEC_THREADS - 1) / SPEC_THREADS), SPEC_THREADS, 0, s>>>(
+      S, plane, n0, n1, n2, L[0], L[1], L[2], wgt, favg);
+  const int64_t yz = int64_t(n1) * n2;
+  const dim3 grid(unsigned((yz + SPEC_THREADS - 1) / SPEC_THREADS), (n0 % 2 == 0 && n0 > 1) ? 2u : 1u);
+  coords_hermitian_kernel<<<grid, SPEC_THREADS, 0, s>>>(S, plane, n0, n1, n2);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_coords(const double* u, const double* favg, const int n[3], const double step[3], double wgt,
+                          double* xp, double* xn, cudaStream_t s) {
+  const int64_t N = int64_t(n[0]) * n[1] * n[2];
+  const int64_t M = int64_t(n[0] + 1) * (n[1] + 1) * (n[2] + 1);
+  coords_point_kernel<<<unsigned((N + 255) / 256), 256, 0, s>>>(u, favg, n[0], n[1], n[2], step[0], step[1], step[2],
+                                                                 wgt, xp);
+  coords_node_kernel<<<unsigned((M + 255) / 256), 256, 0, s>>>(u, favg, n[0], n[1], n[2], step[0], step[1], step[2],
+                                                                wgt, xn);
+  return cudaGetLastError();
+}
+
+}  // namespace dmk

@@ -66,6 +66,13 @@ cudaError_t launch_orientations(const double* Fe, int64_t N, double* out /* 4 pe
 cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s);
 cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
 
+// utilities_updateCoords (kernels.cu): u_hat from the spectrum of F (planes 0..2, Hermitian), then
+// cell-centre and node coordinates from the C2R output u (null: undeformed coordinates)
+cudaError_t launch_coords_spec(double* spec, int n0, int n1, int n2, const double L[3], double wgt, double* favg,
+                               cudaStream_t s);
+cudaError_t launch_coords(const double* u, const double* favg, const int n[3], const double step[3], double wgt,
+                          double* xp, double* xn, cudaStream_t s);
+
 // Anderson acceleration of the fixed point (kernels.cu)
 constexpr int AA_MAX = 32;
 cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,

@@ -31,6 +31,26 @@ def _dp(a: np.ndarray):
     return a.ctypes.data_as(C.POINTER(C.c_double))
 
 
+def node_count(cells) -> int:
+    return int(np.prod([c + 1 for c in cells]))
+
+
+def coordinates0(cells, size) -> tuple[np.ndarray, np.ndarray]:
+    """Undeformed cell centres and nodes, x fastest (IPcoordinates0 and nodes0,
+    src/grid/discretization_grid.f90:270-313)."""
+    step = np.asarray(size, float) / np.asarray(cells)
+    ijk = np.stack(np.meshgrid(*[np.arange(c) for c in cells], indexing='ij'), -1).reshape(-1, 3, order='F')
+    nodes = np.stack(np.meshgrid(*[np.arange(c + 1) for c in cells], indexing='ij'), -1).reshape(-1, 3, order='F')
+    return step * (ijk + 0.5), step * nodes
+
+
+def displacements(cells, size, ip: np.ndarray, nodes: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
+    """u_p and u_n of the result file: current minus undeformed coordinates
+    (discretization_result, src/discretization.f90:81-96)."""
+    ip0, nodes0 = coordinates0(cells, size)
+    return ip - ip0, nodes - nodes0
+
+
 class SpectralBasic:
     """grid_mechanical_spectral_basic on one GPU (B200, sm_100a)."""
 
@@ -84,6 +104,13 @@ class SpectralBasic:
 
     def update_coords(self) -> None:
         _lib.check(self.lib.dmk_mech_update_coords(self.ctx))
+
+    def get_coords(self) -> tuple[np.ndarray, np.ndarray]:
+        """Cell-centre (N, 3) and node ((c1+1)(c2+1)(c3+1), 3) coordinates, x fastest."""
+        ip = np.empty((self.N, 3))
+        nodes = np.empty((node_count(self.cells), 3))
+        _lib.check(self.lib.dmk_get_coords(self.ctx, _dp(ip), _dp(nodes)))
+        return ip, nodes
 
     # -- fields and diagnostics -----------------------------------------------------------------
     def get_field(self, name: str, out: np.ndarray | None = None) -> np.ndarray:

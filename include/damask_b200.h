@@ -147,10 +147,19 @@ int dmk_mech_solution(dmk_ctx* ctx, dmk_solution_state* out);
 /* materialpoint_forward -> mechanical_forward, phase_mechanical.f90:987-1002 */
 int dmk_materialpoint_forward(dmk_ctx* ctx);
 
-/* grid_mechanical_spectral_basic_updateCoords, grid_mech_spectral_basic.f90:361-372.
-   Nodal coordinates are an output-only quantity and are not produced on this path;
-   the call is accepted so that the host driver is unchanged. */
+/* grid_mechanical_spectral_basic_updateCoords, grid_mech_spectral_basic.f90:361-372, which
+   calls utilities_updateCoords (spectral_utilities.f90:857-968) on the solver's F field:
+   cell-centre and node coordinates of the current configuration by integration of F in
+   Fourier space (average part Favg times the undeformed position plus the periodic
+   fluctuation).  The result replaces discretization_setIPcoords / _setNodeCoords
+   (discretization.f90:102-122) and is read with dmk_get_coords. */
 int dmk_mech_update_coords(dmk_ctx* ctx);
+
+/* discretization_IPcoords and discretization_NodeCoords (discretization.f90:23-26) as set
+   by the last dmk_mech_update_coords; before the first call the undeformed coordinates
+   IPcoordinates0 / nodes0 (discretization_grid.f90:270-313).  ip: (3, cells1*cells2*cells3),
+   nodes: (3, (cells1+1)*(cells2+1)*(cells3+1)), x fastest; either may be NULL. */
+int dmk_get_coords(dmk_ctx* ctx, double* ip, double* nodes);
 
 /* Field transfer to/from host buffers (Fortran layout). */
 int dmk_get_field(dmk_ctx* ctx, int field, double* host_out);

@@ -470,6 +470,7 @@ struct orc_ctx {
   std::vector<double> xi;         // 3 per Fourier point (imaginary part of xi1st), index ((z*n1+y)*red+x)
   T4 C_ref;
   std::vector<cd> work;           // full complex workspace, 9 components
+  std::vector<double> xp, xn;     // discretization_IPcoords / _NodeCoords, 3 per point
   // basic solver (grid_mech_spectral_basic.f90:30-45)
   std::vector<M3> Fsol, F_lastinc, Fdot;
   M3 F_aim, F_aim_lastinc, F_aimDot, P_aim, P_av;
@@ -980,9 +981,25 @@ double divergence_rms(orc_ctx* c) {
   return res;
 }
 
+// C2R of one component given by its stored half spectrum (kx in [0, cells1/2], index fidx):
+// Hermitian extension of the stored half, complex inverse transform, real part.  The real part
+// makes the planes kx = 0 and kx = cells1/2 count with their Hermitian part, as a C2R does.
+// w: workspace of N complex values.
+void c2r(orc_ctx* c, const cd* half, cd* w, double* out) {
+  const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
+  for (int z = 0; z < n2; ++z) for (int y = 0; y < n1; ++y) for (int x = 0; x < n0; ++x) {
+    cd v;
+    if (x < c->red) v = half[fidx(c, x, y, z)];
+    else v = std::conj(half[fidx(c, n0 - x, (n1 - y) % n1, (n2 - z) % n2)]);
+    w[(long(z) * n1 + y) * n0 + x] = v;
+  }
+  fft3(w, c->cells, +1);
+  for (long v = 0; v < c->N; ++v) out[v] = w[v].real();
+}
+
 // utilities_GammaConvolution, spectral_utilities.f90:436-501 (spectrum in c->work; result to field)
 void gamma_convolution(orc_ctx* c, M3* field, const M3& aim) {
-  const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
+  const int n1 = c->cells[1], n2 = c->cells[2];
   const long N = c->N;
   std::vector<cd> half(size_t(9) * c->red * n1 * n2);
   #pragma omp parallel for collapse(2) schedule(static) num_threads(c->nthreads)
@@ -1024,19 +1041,75 @@ void gamma_convolution(orc_ctx* c, M3* field, const M3& aim) {
     }
     for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) half[(i + 3 * j) * (long(c->red) * n1 * n2) + f] = R[i][j];
   }
-  // C2R: Hermitian extension of the stored half, inverse transform, real part
   const long H = long(c->red) * n1 * n2;
+  std::vector<double> out(N);
   for (int comp = 0; comp < 9; ++comp) {
-    cd* w = c->work.data() + comp * N;
-    for (int z = 0; z < n2; ++z) for (int y = 0; y < n1; ++y) for (int x = 0; x < n0; ++x) {
-      cd v;
-      if (x < c->red) v = half[comp * H + fidx(c, x, y, z)];
-      else v = std::conj(half[comp * H + fidx(c, n0 - x, (n1 - y) % n1, (n2 - z) % n2)]);
-      w[(long(z) * n1 + y) * n0 + x] = v;
-    }
-    fft3(w, c->cells, +1);
+    c2r(c, half.data() + comp * H, c->work.data() + comp * N, out.data());
     int i = comp % 3, j = comp / 3;
-    for (long v = 0; v < N; ++v) field[v].a[i][j] = w[v].real();
+    for (long v = 0; v < N; ++v) field[v].a[i][j] = out[v];
+  }
+}
+
+// utilities_updateCoords, spectral_utilities.f90:857-968 (single process: the z padding of the
+// cell-centre fluctuations is the periodic wrap)
+void update_coords(orc_ctx* c) {
+  const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
+  const long N = c->N;
+  const double* g = c->geomSize;
+  const double step[3] = {g[0] / n0, g[1] / n1, g[2] / n2};
+  r2c(c, c->Fsol.data());
+  M3 Favg;
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Favg.a[i][j] = spec(c, i + 3 * j, 0, 0, 0).real() * c->wgt;
+  // vectorField_fourier = F_hat . xi2nd / sum(conjg(-xi2nd) xi2nd), zero at k = 0 (:899-909)
+  const long H = long(c->red) * n1 * n2;
+  std::vector<cd> half(size_t(3) * H);
+  for (int z = 0; z < n2; ++z) for (int y = 0; y < n1; ++y) for (int x = 0; x < c->red; ++x) {
+    const long f = fidx(c, x, y, z);
+    if (x == 0 && y == 0 && z == 0) { for (int l = 0; l < 3; ++l) half[l * H + f] = 0.0; continue; }
+    int ks[3] = {x, y > n1 / 2 ? y - n1 : y, z > n2 / 2 ? z - n2 : z};
+    cd xi2[3];
+    for (int d = 0; d < 3; ++d) xi2[d] = cd(0.0, TAU * double(ks[d]) / g[d]);   // no Nyquist zeroing
+    cd den = 0.0;
+    for (int d = 0; d < 3; ++d) den += std::conj(-xi2[d]) * xi2[d];
+    for (int l = 0; l < 3; ++l) {
+      cd s = 0.0;
+      for (int m = 0; m < 3; ++m) s += spec(c, l + 3 * m, x, y, z) * xi2[m];
+      half[l * H + f] = s / den;
+    }
+  }
+  std::vector<double> u(size_t(3) * N);
+  for (int l = 0; l < 3; ++l) {
+    c2r(c, half.data() + l * H, c->work.data() + l * N, u.data() + l * N);
+    for (long v = 0; v < N; ++v) u[l * N + v] *= c->wgt;
+  }
+  // nodal positions (:940-952): Favg (step ijk) + mean of the 8 surrounding cell fluctuations
+  static const int nb[8][3] = {{0, 0, 0}, {1, 0, 0}, {1, 1, 0}, {0, 1, 0}, {0, 0, 1}, {1, 0, 1}, {1, 1, 1}, {0, 1, 1}};
+  auto mod = [](int a, int n) { return ((a % n) + n) % n; };
+  c->xn.assign(size_t(3) * (n0 + 1) * (n1 + 1) * (n2 + 1), 0.0);
+  long t = 0;
+  for (int k = 0; k <= n2; ++k) for (int j = 0; j <= n1; ++j) for (int i = 0; i <= n0; ++i, ++t) {
+    const double p[3] = {step[0] * i, step[1] * j, step[2] * k};
+    for (int l = 0; l < 3; ++l) {
+      double x = 0.0;
+      for (int m = 0; m < 3; ++m) x += Favg.a[l][m] * p[m];
+      for (int n = 0; n < 8; ++n) {
+        const long w = (long(mod(k + nb[n][2] - 1, n2)) * n1 + mod(j + nb[n][1] - 1, n1)) * n0 + mod(i + nb[n][0] - 1, n0);
+        x += u[l * N + w] * 0.125;
+      }
+      c->xn[3 * t + l] = x;
+    }
+  }
+  // cell centres (:955-959): fluctuation + Favg (step (ijk - 1/2))
+  c->xp.assign(size_t(3) * N, 0.0);
+  for (long v = 0; v < N; ++v) {
+    const long idx[3] = {v % n0, (v / n0) % n1, v / (long(n0) * n1)};
+    double p[3];
+    for (int d = 0; d < 3; ++d) p[d] = step[d] * (double(idx[d] + 1) - 0.5);
+    for (int l = 0; l < 3; ++l) {
+      double x = 0.0;
+      for (int m = 0; m < 3; ++m) x += Favg.a[l][m] * p[m];
+      c->xp[3 * v + l] = u[l * N + v] + x;
+    }
   }
 }
 
@@ -1155,6 +1228,20 @@ orc_ctx* orc_create(const int cells[3], const double geomSize[3], const int* mat
   c->F0 = c->F; c->Fp0 = c->Fp; c->Fi0 = c->Fi;
   c->state0 = c->state;
   spectral_init(c);
+  // discretization_init: current coordinates start as the undeformed ones
+  // (IPcoordinates0 / nodes0, discretization_grid.f90:270-313)
+  {
+    const double step[3] = {geomSize[0] / cells[0], geomSize[1] / cells[1], geomSize[2] / cells[2]};
+    c->xp.assign(size_t(3) * N, 0.0);
+    for (long v = 0; v < N; ++v) {
+      const long idx[3] = {v % cells[0], (v / cells[0]) % cells[1], v / (long(cells[0]) * cells[1])};
+      for (int d = 0; d < 3; ++d) c->xp[3 * v + d] = step[d] * (double(idx[d] + 1) - 0.5);
+    }
+    c->xn.clear();
+    for (int k = 0; k <= cells[2]; ++k) for (int j = 0; j <= cells[1]; ++j) for (int i = 0; i <= cells[0]; ++i) {
+      c->xn.push_back(step[0] * i); c->xn.push_back(step[1] * j); c->xn.push_back(step[2] * k);
+    }
+  }
   c->Fsol.assign(N, eye3()); c->F_lastinc.assign(N, eye3()); c->Fdot.assign(N, zero3());
   c->F_aim = eye3(); c->F_aim_lastinc = eye3(); c->F_aimDot = zero3(); c->P_aim = zero3(); c->P_av = zero3();
   std::memset(&c->C_volAvg, 0, sizeof(T4)); c->C_volAvgLastInc = c->C_volAvg; c->C_minMaxAvg = c->C_volAvg;
@@ -1320,6 +1407,14 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
   for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) out->P_av[3 * j + i] = c->P_av.a[i][j];
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) if (c->stress_mask[i][j]) c->P_aim.a[i][j] = c->P_av.a[i][j];
   return 0;
+}
+
+// grid_mechanical_spectral_basic_updateCoords, grid_mech_spectral_basic.f90:361-372
+void orc_update_coords(orc_ctx* c) { update_coords(c); }
+
+void orc_get_coords(orc_ctx* c, double* ip, double* nodes) {
+  if (ip) std::memcpy(ip, c->xp.data(), sizeof(double) * c->xp.size());
+  if (nodes) std::memcpy(nodes, c->xn.data(), sizeof(double) * c->xn.size());
 }
 
 // materialpoint_forward -> mechanical_forward, phase_mechanical.f90:987-1002

@@ -46,6 +46,8 @@ def load() -> C.CDLL:
                                        C.POINTER(BCStruct), C.POINTER(BCStruct), dp]),
         'orc_mech_solution': (C.c_int, [vp, C.POINTER(SolutionStruct)]),
         'orc_materialpoint_forward': (None, [vp]),
+        'orc_update_coords': (None, [vp]),
+        'orc_get_coords': (None, [vp, dp, dp]),
         'orc_constitutive_response': (C.c_int, [vp, dp, C.c_double, dp, dp, dp, dp, C.POINTER(C.c_int)]),
         'orc_update_gamma': (None, [vp, dp]),
         'orc_gamma_convolution': (None, [vp, dp, dp]),
@@ -111,7 +113,13 @@ class OracleSpectralBasic:
         self.lib.orc_materialpoint_forward(self.ctx)
 
     def update_coords(self) -> None:
-        pass
+        self.lib.orc_update_coords(self.ctx)
+
+    def get_coords(self) -> tuple[np.ndarray, np.ndarray]:
+        ip = np.empty((self.N, 3))
+        nodes = np.empty((int(np.prod([c + 1 for c in self.cells])), 3))
+        self.lib.orc_get_coords(self.ctx, _p(ip), _p(nodes))
+        return ip, nodes
 
     def get_field(self, name: str) -> np.ndarray:
         k = self.n_slip if name in ('xi_sl', 'gamma_sl') else 4 if name == 'O' else 9

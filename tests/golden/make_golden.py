@@ -14,7 +14,12 @@ functions used here touches them.  Fixtures written:
   from one generator ``default_rng(0)`` (``seeds.from_random``, ``Rotation.from_random``);
 * ``div_field``, ``div_rms``: a seeded random tensor field on an 8x6x4 grid of size
   (1, 2, 3) mm and the RMS of its spectral divergence ``grid.divergence``
-  (``python/damask/grid.py:143-167``).
+  (``python/damask/grid.py:143-167``);
+* ``coords_<case>_{F,size,ip,nodes}``: deformation gradient fields and their current
+  cell-centre and node coordinates ``grid.coordinates_point`` / ``grid.coordinates_node``
+  (``python/damask/grid.py:298-330,445-470``, the Python form of ``utilities_updateCoords``),
+  case ``odd`` a random field on 5x7x9 and case ``smooth`` a band-limited field on 8x6x4 (no
+  content at the Nyquist frequencies, where the Python form transforms a different axis).
 """
 import importlib
 import sys
@@ -61,6 +66,22 @@ def main(root: str) -> None:
     out['div_field'] = f
     out['div_size'] = size
     out['div_rms'] = np.sqrt(np.mean(np.sum(d ** 2, axis=-1)))
+    for case, cells in (('odd', (5, 7, 9)), ('smooth', (8, 6, 4))):
+        size = np.array([1.0e-3, 2.0e-3, 1.5e-3])
+        g = np.random.default_rng(3)
+        if case == 'odd':
+            F = np.eye(3) + 0.05 * g.normal(size=cells + (3, 3))
+        else:
+            X = np.stack(np.meshgrid(*[np.arange(c) / c for c in cells], indexing='ij'), -1)
+            F = np.broadcast_to(np.eye(3) + 0.02 * g.normal(size=(3, 3)), cells + (3, 3)).copy()
+            for _ in range(3):
+                A = 0.03 * g.normal(size=(3, 3))
+                kv = g.integers(-1, 2, size=3)
+                F += A * np.cos(2 * np.pi * (X @ kv) + g.uniform())[..., None, None]
+        out[f'coords_{case}_F'] = F
+        out[f'coords_{case}_size'] = size
+        out[f'coords_{case}_ip'] = grid.coordinates_point(size, F)
+        out[f'coords_{case}_nodes'] = grid.coordinates_node(size, F)
     np.savez_compressed(Path(__file__).with_name('golden.npz'), **out)
     print({k: np.shape(v) for k, v in out.items()})
 

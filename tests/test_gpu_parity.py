@@ -105,6 +105,9 @@ def test_solver_parity(gpu, oracle_lib, case):
     for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'O'):
         assert rel(g.get_field(name), o.get_field(name)) < TOL, name
     assert rel(g.aims()['C_volAvg'], o.aims()['C_volAvg']) < TOL
+    # coordinates of the last updateCoords (after every converged increment)
+    for a, b in zip(g.get_coords(), o.get_coords()):
+        assert rel(a, b) < TOL
     g.close()
 
 
@@ -140,4 +143,40 @@ def test_stress_field_as_first_read(gpu, oracle_lib):
     g, o = pair(oracle_lib, (4, 3, 2), 2)
     Sg, So = g.get_field('S'), o.get_field('S')
     assert np.isfinite(Sg).all() and np.abs(Sg - So).max() < 1e-3
+    g.close()
+
+
+@pytest.mark.parametrize('case', ['odd', 'smooth'])
+def test_update_coords_golden(gpu, oracle_lib, golden, case):
+    """utilities_updateCoords on the device against the reference's Python form."""
+    from test_oracle import voxel_tensors
+    F = golden[f'coords_{case}_F']
+    cells = F.shape[:3]
+    g = SpectralBasic(cells, tuple(golden[f'coords_{case}_size']), np.zeros(int(np.prod(cells))),
+                      np.array([[1.0, 0, 0, 0]]), workloads.fcc_al(), workloads.numerics_default())
+    g.set_field('F_solver', voxel_tensors(F))
+    g.update_coords()
+    ip, nodes = g.get_coords()
+    g.close()
+    assert rel(ip, golden[f'coords_{case}_ip'].reshape(-1, 3, order='F')) < 1e-13
+    assert rel(nodes, golden[f'coords_{case}_nodes'].reshape(-1, 3, order='F')) < 1e-13
+
+
+@pytest.mark.parametrize("cells", [(8, 6, 4), (5, 7, 9), (6, 3, 2), (16, 16, 16)])
+def test_update_coords_random_field(gpu, oracle_lib, cells):
+    """Random F fields (content at every frequency, Nyquist included on even edges): device and
+    oracle coordinates agree, and before the first update both are the undeformed ones."""
+    from damask_b200.grid import coordinates0
+    size = (1.0e-3, 2.0e-3, 1.5e-3)
+    N = int(np.prod(cells))
+    g, o = pair(oracle_lib, cells, 1, size=size)
+    ip0, n0 = coordinates0(cells, size)
+    for a, b in zip(g.get_coords(), (ip0, n0)):
+        assert rel(a, b) < 1e-15
+    F = np.tile(np.eye(3).reshape(-1), (N, 1)) + 0.05 * np.random.default_rng(11).normal(size=(N, 9))
+    for s in (g, o):
+        s.set_field('F_solver', F)
+        s.update_coords()
+    for a, b in zip(g.get_coords(), o.get_coords()):
+        assert rel(a, b) < 1e-12
     g.close()

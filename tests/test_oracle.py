@@ -162,3 +162,43 @@ def test_orientation_output(oracle_lib):
     o.set_field('F_e', Fs)
     assert np.abs(o.get_field('O') - q).max() < 1e-12
     o.close()
+
+
+def voxel_tensors(F: np.ndarray) -> np.ndarray:
+    """(x, y, z, 3, 3) -> (N, 9): column-major 3x3 per voxel, x fastest."""
+    return np.transpose(F, (0, 1, 2, 4, 3)).reshape(F.shape[:3] + (9,)).reshape(-1, 9, order='F')
+
+
+@pytest.mark.parametrize('case', ['odd', 'smooth'])
+def test_update_coords_matches_reference_python(golden, oracle_lib, case):
+    """utilities_updateCoords against the reference's Python form (coordinates_point/_node)."""
+    F = golden[f'coords_{case}_F']
+    cells = F.shape[:3]
+    o = oracle_lib.OracleSpectralBasic(cells, tuple(golden[f'coords_{case}_size']), np.zeros(int(np.prod(cells))),
+                                       np.array([[1.0, 0, 0, 0]]), workloads.fcc_al(), init=False, threads=1)
+    o.set_field('F_solver', voxel_tensors(F))
+    o.update_coords()
+    ip, nodes = o.get_coords()
+    o.close()
+    assert rel(ip, golden[f'coords_{case}_ip'].reshape(-1, 3, order='F')) < 1e-13
+    assert rel(nodes, golden[f'coords_{case}_nodes'].reshape(-1, 3, order='F')) < 1e-13
+
+
+def test_coordinates_start_undeformed_and_follow_uniform_F(oracle_lib):
+    """Before any update the coordinates are IPcoordinates0 / nodes0; a uniform F maps them
+    affinely (no fluctuation) and the displacements are (F - I) x0."""
+    from damask_b200.grid import coordinates0, displacements
+    cells, size = (4, 3, 2), (1.0e-3, 2.0e-3, 3.0e-3)
+    o = oracle_lib.OracleSpectralBasic(cells, size, np.zeros(24), np.array([[1.0, 0, 0, 0]]), workloads.fcc_al(),
+                                       init=False, threads=1)
+    ip0, n0 = coordinates0(cells, size)
+    ip, nodes = o.get_coords()
+    assert np.array_equal(ip, ip0) and np.array_equal(nodes, n0)
+    Fu = np.array([[1.1, 0.02, 0.0], [0.0, 0.95, 0.01], [0.03, 0.0, 1.0]])
+    o.set_field('F_solver', np.tile(Fu.T.reshape(-1), (24, 1)))
+    o.update_coords()
+    ip, nodes = o.get_coords()
+    o.close()
+    up, un = displacements(cells, size, ip, nodes)
+    assert rel(up, ip0 @ (Fu - np.eye(3)).T) < 1e-12
+    assert rel(un, n0 @ (Fu - np.eye(3)).T) < 1e-12
