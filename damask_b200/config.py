@@ -42,7 +42,9 @@ class NumericsStruct(C.Structure):
                 ('eps_abs_Lp', C.c_double), ('f_update_jacobi_Lp', C.c_int),
                 ('N_iter_Li_max', C.c_int), ('r_linesearch_Li', C.c_double), ('eps_rel_Li', C.c_double),
                 ('eps_abs_Li', C.c_double), ('f_update_jacobi_Li', C.c_int),
-                ('snes_type', C.c_int), ('anderson_m', C.c_int)]
+                ('snes_type', C.c_int), ('anderson_m', C.c_int),
+                ('solver', C.c_int), ('alpha', C.c_double), ('beta', C.c_double),
+                ('eps_abs_curl', C.c_double), ('eps_rel_curl', C.c_double)]
 
 
 class BCStruct(C.Structure):
@@ -56,7 +58,8 @@ class RestartStruct(C.Structure):
                 ('L_p', C.POINTER(C.c_double)), ('omega_plastic', C.POINTER(C.c_double)),
                 ('P_aim', C.c_double * 9), ('F_aim', C.c_double * 9), ('F_aim_lastinc', C.c_double * 9),
                 ('F_aimDot', C.c_double * 9), ('C_volAvg', C.c_double * 81), ('C_volAvgLastInc', C.c_double * 81),
-                ('C_minMaxAvg', C.c_double * 81)]
+                ('C_minMaxAvg', C.c_double * 81), ('F_tau', C.POINTER(C.c_double)),
+                ('F_tau_lastinc', C.POINTER(C.c_double))]
 
 
 class SolutionStruct(C.Structure):
@@ -66,6 +69,7 @@ class SolutionStruct(C.Structure):
 
 
 LATTICES = {'cF': 0, 'cI': 1}
+SOLVERS = {'spectral_basic': 0, 'spectral_polarization': 1}
 BC_TYPES = {'L': 1, 'dot_F': 2, 'F_dot': 2, 'F': 3, 'P': 4, 'dot_P': 5, 'P_dot': 5}
 
 
@@ -183,6 +187,12 @@ class Numerics:
     f_update_jacobi_Li: int | None = None
     PETSc_options: str = ''
     anderson_m: int = 8
+    # spectral_polarization only (grid_mech_spectral_polarization.f90:137-148)
+    solver: str = 'spectral_basic'
+    alpha: float = 1.0
+    beta: float = 1.0
+    eps_abs_curl: float = 1.0e-10
+    eps_rel_curl: float = 5.0e-4
 
     @property
     def snes_type(self) -> int:
@@ -214,6 +224,10 @@ class Numerics:
                           ('eps_abs_P', 'eps_abs_P'), ('eps_rel_P', 'eps_rel_P'), ('update_gamma', 'update_gamma')):
             if k_yaml in mech:
                 setattr(n, k, mech[k_yaml])
+        for k_yaml, k in (('alpha', 'alpha'), ('beta', 'beta'), ('eps_abs_curl(F)', 'eps_abs_curl'),
+                          ('eps_rel_curl(F)', 'eps_rel_curl')):
+            if k_yaml in mech:
+                setattr(n, k, float(mech[k_yaml]))
         if 'PETSc_options' in mech:
             n.PETSc_options = str(mech['PETSc_options'])
         if 'anderson_m' in mech:
@@ -249,6 +263,12 @@ class Numerics:
         if self.N_iter_state_max < 1: bad.append('N_iter_state_max')
         if self.derivative != 'continuous': bad.append('derivative')
         if not 1 <= self.anderson_m <= 32: bad.append('anderson_m')
+        if self.solver not in SOLVERS: bad.append('solver')
+        if self.solver == 'spectral_polarization':
+            if self.eps_abs_curl <= 0: bad.append('eps_abs_curl(F)')
+            if self.eps_rel_curl <= 0: bad.append('eps_rel_curl(F)')
+            if not 0.0 < self.alpha <= 2.0: bad.append('alpha')
+            if not 0.0 <= self.beta <= 2.0: bad.append('beta')
         self.snes_type
         if bad:
             raise ValueError('invalid numerics: ' + ' '.join(bad))
@@ -272,7 +292,19 @@ class Numerics:
         s.f_update_jacobi_Li = int(self.f_update_jacobi_Lp if self.f_update_jacobi_Li is None else self.f_update_jacobi_Li)
         s.snes_type = self.snes_type
         s.anderson_m = int(self.anderson_m)
+        s.solver = SOLVERS[self.solver]
+        s.alpha, s.beta = float(self.alpha), float(self.beta)
+        s.eps_abs_curl, s.eps_rel_curl = float(self.eps_abs_curl), float(self.eps_rel_curl)
         return s
+
+
+def mechanical_solver(load: dict) -> str:
+    """The grid mechanical solver a load file selects (``solver: mechanical:``,
+    DAMASK_grid.f90:171-206); this path provides spectral_basic and spectral_polarization."""
+    name = load.get('solver', {}).get('mechanical', 'spectral_basic')
+    if name not in SOLVERS:
+        raise ValueError(f"unsupported mechanical solver '{name}'")
+    return name
 
 
 def masked_tensor(rows) -> tuple[np.ndarray, np.ndarray]:

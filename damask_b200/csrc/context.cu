@@ -99,6 +99,12 @@ struct dmk_ctx {
   double* xp = nullptr;         // cell-centre coordinates, 3 per voxel (discretization_IPcoords)
   double* xn = nullptr;         // node coordinates, 3 per node (discretization_NodeCoords)
   double* favg = nullptr;       // average F of the last updateCoords (9)
+  // spectral polarization scheme (solver 1): Fsol and r hold [F; F_tau] (18 planes)
+  int solver = 0;
+  double *Ftau = nullptr, *Ftau_last = nullptr, *Ftau_dot = nullptr, *Feval = nullptr, *curl_partials = nullptr;
+  PolConst polc{};
+  double err_curl = 0.0;
+  double h_aim[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};   // host source of the DC term upload
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
 
   // host copy of the solver module state (grid_mech_spectral_basic.f90:30-45)
@@ -437,9 +443,11 @@ int make_plans(dmk_ctx* c) {
 // One constitutive sweep + commit of P (homogenization_mechanical_response + the P part of
 // utilities_constitutiveResponse).  On a failed sweep the previous P field is kept (the
 // reference skips mechanical_homogenize when any cell fails, homogenization.f90:343).
-int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int* status_out) {
+int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int* status_out,
+                          const double* Fsrc = nullptr) {
   CK(cudaMemsetAsync(c->status, 0, sizeof(int), c->stream));
   Fields f = make_fields(c, r);
+  if (Fsrc) f.Fsol = const_cast<double*>(Fsrc);   // read only when apply == 0
   CK(cudaEventRecord(c->ev[0], c->stream));
   if (int rc = run_constitutive(c, f, dt, apply)) return rc;
   CK(cudaEventRecord(c->ev[1], c->stream));
@@ -475,6 +483,50 @@ int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
     c->C_volAvg[k] = h[k];
     c->C_minMaxAvg[k] = 0.5 * (h[81 + k] + h[162 + k]);
   }
+  return 0;
+}
+
+// math_invSym3333 (math.f90:511-532): Mandel 6x6 of A (math_sym3333to66, :826-845), its inverse,
+// expanded with minor symmetry (math_66toSym3333, :851-900).  Column-major 3x3x3x3.
+bool inv_sym3333_host(const double* A, double* out) {
+  const int pi[6] = {0, 1, 2, 1, 0, 0}, pj[6] = {0, 1, 2, 2, 2, 1};
+  const double SQ2 = std::sqrt(2.0);
+  auto w = [&](int r) { return r < 3 ? 1.0 : SQ2; };
+  double M[6][12];
+  for (int r = 0; r < 6; ++r)
+    for (int q = 0; q < 6; ++q) {
+      M[r][q] = A[pi[r] + 3 * pj[r] + 9 * pi[q] + 27 * pj[q]] * w(r) * w(q);
+      M[r][6 + q] = r == q ? 1.0 : 0.0;
+    }
+  for (int j = 0; j < 6; ++j) {     // Gauss-Jordan with partial pivoting
+    int p = j;
+    for (int i = j + 1; i < 6; ++i) if (std::fabs(M[i][j]) > std::fabs(M[p][j])) p = i;
+    if (M[p][j] == 0.0) return false;
+    for (int k = 0; k < 12; ++k) std::swap(M[j][k], M[p][k]);
+    const double d = M[j][j];
+    for (int k = 0; k < 12; ++k) M[j][k] /= d;
+    for (int i = 0; i < 6; ++i)
+      if (i != j) {
+        const double l = M[i][j];
+        for (int k = 0; k < 12; ++k) M[i][k] -= l * M[j][k];
+      }
+  }
+  for (int r = 0; r < 6; ++r)
+    for (int q = 0; q < 6; ++q) {
+      const double v = M[r][6 + q] / (w(r) * w(q));
+      for (int a : {0, 1})
+        for (int b : {0, 1}) {
+          const int i = a ? pj[r] : pi[r], j = a ? pi[r] : pj[r], k = b ? pj[q] : pi[q], l = b ? pi[q] : pj[q];
+          out[i + 3 * j + 9 * k + 27 * l] = v;
+        }
+    }
+  return true;
+}
+
+// C_scale = C_minMaxAvg, S_scale = invSym3333(C_minMaxAvg) (grid_mech_spectral_polarization.f90:266-268, 292-296)
+int set_polarization_scale(dmk_ctx* c) {
+  std::memcpy(c->polc.C, c->C_minMaxAvg, sizeof c->polc.C);
+  if (!inv_sym3333_host(c->C_minMaxAvg, c->polc.S)) return fail(DMK_ERR_STATE, "matrix inversion error (S_scale)");
   return 0;
 }
 
@@ -589,6 +641,171 @@ std::vector<double> anderson_coefficients(const std::vector<double>& G, int m, c
   return gam;
 }
 
+// grid_mech_spectral_polarization_solution (grid_mech_spectral_polarization.f90:273-309) with its
+// form_residual (:562-632) and converged (:521-556) on the solution vector [F; F_tau]; the masked
+// compliance S and the Gamma stiffness are set by the caller.  Fixed point as for the basic
+// scheme: Richardson X <- X - r, or Anderson acceleration over both fields.
+int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
+  if (c->num.update_gamma)
+    if (int rc = set_polarization_scale(c)) return rc;
+  const int64_t N = c->N, n18 = 18 * N;
+  const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
+  const bool anderson = c->num.snes_type == 1;
+  const int m = c->aa_m;
+  const int nspec = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
+  const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
+  const double beta = c->polc.beta;
+  double* rF = c->r;
+  double* rtau = c->r + 9 * N;
+  auto* spec = reinterpret_cast<cufftDoubleComplex*>(c->spec);
+  int evals = 0, reason = 0, totalIter = -1, status = 0;
+  std::vector<double> G(size_t(m > 0 ? m : 1) * (m > 0 ? m : 1), 0.0), bvec, divp(nspec), curlp(nspec);
+  std::vector<int> slots_b;
+  double dots[4 * AA_MAX];
+  int count = 0, new_slot = -1;
+  double F_av[9], P_av[9];
+
+  auto residual = [&]() -> int {
+    ++totalIter;
+    CKL(launch_sum9(c->Fsol, N, c->partials, c->stream));             // F_av
+    CKL(launch_reduce9(c->partials, nblocks_const(c), c->sums, c->stream));
+    CKL(launch_pol_pre(c->Fsol, c->Ftau, N, c->polc, rF, c->stream));
+    double bF[9];
+    for (int k = 0; k < 9; ++k) bF[k] = beta * c->F_aim[k];
+    h_rot33(c->q_rot, bF, c->h_aim, true);
+    CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_rot), c->h_aim, sizeof c->h_aim,
+                       cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ev[2], c->stream));
+    CKF(cufftExecD2Z(c->plan_fwd, rF, spec));
+    CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, 1, 0,
+                                c->stream));
+    ++c->launches;
+    CKF(cufftExecZ2D(c->plan_bwd, spec, rtau));
+    CKL(launch_pol_tau(c->Fsol, rtau, N, beta, c->Feval, c->stream));
+    CKF(cufftExecD2Z(c->plan_fwd, c->Fsol, spec));                      // curl of F
+    CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->curl_partials, c->stream));
+    CK(cudaEventRecord(c->ev[3], c->stream));
+    int st = 0;                                                          // constitutive at F - r_F_tau / beta
+    if (int e = evaluate_constitutive(c, c->dt, nullptr, 0, &st, c->Feval)) return e;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+    c->last_ms[1] += ms;
+    CKL(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 0, c->stream));
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    if (int e = evaluate_tangent(c, c->dt, nullptr)) return e;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CKF(cufftExecD2Z(c->plan_fwd, c->P, spec));                         // divergence of P
+    CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, 0, 1,
+                                c->stream));
+    ++c->launches;
+    CKL(launch_pol_rF(c->Fsol, c->Ftau, c->P, c->tan.planes, rtau, N, c->polc, rF, c->stream));
+    int nsl = 0;
+    if (anderson && new_slot >= 0) {
+      slots_b.clear();
+      const int mk = std::min(count, m);
+      for (int q = count - mk; q < count; ++q) slots_b.push_back(q % m);
+      nsl = int(slots_b.size());
+      CKL(launch_aa_dots(c->r, c->aa_Rprev, c->aa_dR, n18, new_slot, slots_b.data(), nsl, c->aa_partials, c->aa_blocks,
+                        c->aa_out, c->stream));
+      c->launches += 2 * ((nsl + AA_CHUNK_HOST - 1) / AA_CHUNK_HOST) - 1;
+      CK(cudaMemcpyAsync(dots, c->aa_out, sizeof(double) * 2 * AA_CHUNK_HOST * ((nsl + AA_CHUNK_HOST - 1) / AA_CHUNK_HOST),
+                         cudaMemcpyDeviceToHost, c->stream));
+    }
+    CK(cudaMemcpyAsync(F_av, c->sums, sizeof F_av, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(P_av, reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, P_av), sizeof P_av,
+                       cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(divp.data(), c->div_partials, sizeof(double) * nspec, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpyAsync(curlp.data(), c->curl_partials, sizeof(double) * nspec, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    c->last_ms[2] += ms;
+    ++evals;
+    status = st;
+    if (nsl > 0) {
+      bvec.assign(nsl, 0.0);
+      for (int q = 0; q < nsl; ++q) {
+        const int ch = q / AA_CHUNK_HOST, k = q % AA_CHUNK_HOST;
+        const double g = dots[ch * 2 * AA_CHUNK_HOST + k], b = dots[ch * 2 * AA_CHUNK_HOST + AA_CHUNK_HOST + k];
+        G[size_t(new_slot) * m + slots_b[q]] = G[size_t(slots_b[q]) * m + new_slot] = g;
+        bvec[q] = b;
+      }
+    }
+    double sdiv = 0.0, scurl = 0.0;
+    for (int b = 0; b < nspec; ++b) { sdiv += divp[b]; scurl += curlp[b]; }
+    c->err_curl = std::sqrt(scurl) * c->wgt * (c->cells[0] == 1 ? 0.5 : 1.0);
+    const double err_div = std::sqrt(sdiv) * c->wgt * (c->cells[0] == 1 ? 0.5 : 1.0);
+    for (int k = 0; k < 9; ++k) F_av[k] *= c->wgt;
+    std::memcpy(c->P_av, P_av, sizeof P_av);
+    // F_aim = F_aim - S : (P_av - P_aim); err_BC (:625-630)
+    double d[9], e[9], t[9], Rav[9];
+    for (int k = 0; k < 9; ++k) d[k] = P_av[k] - c->P_aim[k];
+    for (int ij = 0; ij < 9; ++ij) {
+      double s = 0.0;
+      for (int kl = 0; kl < 9; ++kl) s += c->Scomp[ij + 9 * kl] * d[kl];
+      c->F_aim[ij] -= s;
+    }
+    h_rot33(c->q_rot, F_av, Rav, false);
+    for (int k = 0; k < 9; ++k) t[k] = c->F_aim[k] - Rav[k];
+    for (int ij = 0; ij < 9; ++ij) {
+      double s = 0.0;
+      for (int kl = 0; kl < 9; ++kl) s += c->polc.C[ij + 9 * kl] * t[kl];
+      e[ij] = s;
+    }
+    double err_BC = 0.0;
+    for (int k = 0; k < 9; ++k) err_BC = std::max(err_BC, std::fabs(c->stress_mask[k] ? e[k] : d[k]));
+    // converged (:521-556)
+    double pmax = 0.0, fmax = 0.0;
+    for (int k = 0; k < 9; ++k) {
+      pmax = std::max(pmax, std::fabs(P_av[k]));
+      fmax = std::max(fmax, std::fabs(c->F_aim[k] - ((k % 4 == 0) ? 1.0 : 0.0)));
+    }
+    const double curlTol = std::max(fmax * c->num.eps_rel_curl, c->num.eps_abs_curl);
+    const double divTol = std::max(pmax * c->num.eps_rel_div, c->num.eps_abs_div);
+    const double BCTol = std::max(pmax * c->num.eps_rel_P, c->num.eps_abs_P);
+    reason = 0;
+    if (totalIter >= c->num.N_iter_min && err_div / divTol < 1.0 && c->err_curl / curlTol < 1.0 && err_BC / BCTol < 1.0 &&
+        status == 0)
+      reason = 1;
+    else if (totalIter >= c->num.N_iter_max)
+      reason = -1;
+    if (!std::isfinite(err_div) || !std::isfinite(c->err_curl)) reason = -1;
+    out->err_div = err_div;
+    out->err_BC = err_BC;
+    return 0;
+  };
+
+  if (int rc = residual()) return rc;
+  if (anderson) { bvec.clear(); slots_b.clear(); }
+  for (int it = 1; reason == 0; ++it) {
+    if (it > snes_max_its) { reason = -1; break; }
+    if (!anderson) {
+      CKL(launch_sub(c->Fsol, c->r, n18, c->nsm, c->stream));
+    } else {
+      std::vector<double> gam = anderson_coefficients(G, m, slots_b, bvec);
+      new_slot = count % m;
+      CKL(launch_aa_update(c->Fsol, c->r, c->aa_Rprev, c->aa_dX, c->aa_dR, n18, new_slot, slots_b.data(), gam.data(),
+                          int(slots_b.size()), c->aa_blocks, c->stream));
+      ++count;
+    }
+    if (int rc = residual()) return rc;
+  }
+  out->converged = reason > 0;
+  out->iterationsNeeded = totalIter;
+  out->stagConverged = 1;
+  out->residualEvals = evals;
+  std::memcpy(out->P_av, c->P_av, sizeof out->P_av);
+  for (int k = 0; k < 9; ++k)
+    if (c->stress_mask[k]) c->P_aim[k] = c->P_av[k];
+  unsigned long long hc[4];
+  CK(cudaMemcpyAsync(hc, c->counters, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_counters[0] = int64_t(evals) * c->N;
+  c->last_counters[1] = int64_t(hc[1]);
+  c->last_counters[2] = int64_t(hc[2]);
+  c->last_counters[3] = evals;
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -608,6 +825,11 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   if (num->N_iter_Lp_max < 1 || num->N_iter_state_max < 1 || num->f_update_jacobi_Lp < 1 || !(num->r_cutback > 0.0) ||
       !(num->r_cutback_min > 0.0) || !(num->r_increase > 0.0) || !(num->r_linesearch_Lp > 0.0))
     return fail(DMK_ERR_CONFIG, "invalid phase.mechanical numerics");
+  if (num->solver != 0 && num->solver != 1) return fail(DMK_ERR_CONFIG, "solver must be 0 (spectral_basic) or 1 (spectral_polarization)");
+  // grid_mech_spectral_polarization.f90:150-161
+  if (num->solver == 1 && (!(num->eps_abs_curl > 0.0) || !(num->eps_rel_curl > 0.0) || !(num->alpha > 0.0) ||
+                           num->alpha > 2.0 || num->beta < 0.0 || num->beta > 2.0))
+    return fail(DMK_ERR_CONFIG, "invalid polarization numerics (eps_abs_curl(F), eps_rel_curl(F), alpha, beta)");
   dmk_ctx* c = new dmk_ctx();
   int rc = build_host_phase(*phase, c->hp, g_err);
   if (rc) { delete c; return DMK_ERR_CONFIG; }
@@ -619,6 +841,9 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   c->device = device;
   c->precision = precision;
   c->num = *num;
+  c->solver = num->solver;
+  c->polc.alpha = num->alpha;
+  c->polc.beta = num->beta;
   for (int i = 0; i < 3; ++i) { c->cells[i] = cells[i]; c->geom[i] = geomSize[i]; }
   c->N = int64_t(cells[0]) * cells[1] * cells[2];
   c->wgt = 1.0 / double(c->N);
@@ -661,7 +886,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
 
   const int NST = 2 * c->NS;
   const int64_t plane = int64_t(cells[0] / 2 + 1) * cells[1] * cells[2];
-  if ((rc = dalloc(&c->Fsol, 9 * N)) || (rc = dalloc(&c->r, 9 * N)) || (rc = dalloc(&c->F, 9 * N)) ||
+  const int64_t nvec = (c->solver == 1 ? 18 : 9) * N;   // solution vector: F, or [F; F_tau]
+  if ((rc = dalloc(&c->Fsol, nvec)) || (rc = dalloc(&c->r, nvec)) || (rc = dalloc(&c->F, 9 * N)) ||
       (rc = dalloc(&c->F0, 9 * N)) || (rc = dalloc(&c->Fp, 9 * N)) || (rc = dalloc(&c->Fp0, 9 * N)) ||
       (rc = dalloc(&c->Lp, 9 * N)) || (rc = dalloc(&c->Lp0, 9 * N)) || (rc = dalloc(&c->S, 6 * N)) ||
       (rc = dalloc(&c->S0, 6 * N)) || (rc = dalloc(&c->Fe, 9 * N)) || (rc = dalloc(&c->P, 9 * N)) ||
@@ -686,6 +912,12 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   }
   if (precision == DMK_PRECISION_MIXED)
     if ((rc = dalloc(&c->specf, 2 * 9 * plane)) || (rc = dalloc(&c->Pf, 9 * N))) return bail(rc);
+  if (c->solver == 1) {
+    c->Ftau = c->Fsol + 9 * N;
+    if ((rc = dalloc(&c->Ftau_last, 9 * N)) || (rc = dalloc(&c->Ftau_dot, 9 * N)) || (rc = dalloc(&c->Feval, 9 * N)) ||
+        (rc = dalloc(&c->curl_partials, (size_t)gamma_div_blocks(cells[0], cells[1], cells[2]))))
+      return bail(rc);
+  }
   c->tan_blocks = dPdF_blocks(N);
   if ((rc = dalloc(&c->tan.partials, 81 * (size_t)c->tan_blocks)) || (rc = dalloc(&c->tan.nmax, c->tan_blocks)) ||
       (rc = dalloc(&c->tan.nmin, c->tan_blocks)) || (rc = dalloc(&c->tan.norms, N)) ||
@@ -694,8 +926,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   if (num->snes_type == 1) {
     c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
     c->aa_blocks = c->nsm * 8;
-    if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * 9 * N)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * 9 * N)) ||
-        (rc = dalloc(&c->aa_Rprev, 9 * N)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
+    if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * nvec)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * nvec)) ||
+        (rc = dalloc(&c->aa_Rprev, nvec)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
         (rc = dalloc(&c->aa_out, 4 * AA_MAX)))
       return bail(rc);
   } else if (num->snes_type != 0) {
@@ -721,6 +953,7 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * 9 * N, c->stream);
     for (double* p : {c->S, c->S0})
       if (e == cudaSuccess) e = cudaMemsetAsync(p, 0, sizeof(double) * 6 * N, c->stream);
+    if (c->solver == 1 && e == cudaSuccess) e = cudaMemsetAsync(c->Ftau_dot, 0, sizeof(double) * 9 * N, c->stream);
     if (e == cudaSuccess) e = cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     cudaFree(dmat); cudaFree(dq); cudaFree(dxi);
@@ -752,6 +985,16 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   int st = 0;
   if ((rc = response(c, 0.0, &st))) return bail(rc);
   update_gamma_host(c, c->C_minMaxAvg);
+  if (c->solver == 1) {
+    if ((rc = set_polarization_scale(c))) return bail(rc);
+    // F_tau = F_tau_lastinc = 2 F with F = I (grid_mech_spectral_polarization.f90:250-253)
+    std::vector<double> two(9 * size_t(N));
+    for (int64_t v = 0; v < N; ++v)
+      for (int k = 0; k < 9; ++k) two[size_t(k) * N + v] = (k % 4 == 0) ? 2.0 : 0.0;
+    if (cudaMemcpy(c->Ftau, two.data(), sizeof(double) * two.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+        cudaMemcpy(c->Ftau_last, two.data(), sizeof(double) * two.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(DMK_ERR_CUDA, "init: F_tau upload failed"));
+  }
   *out = c;
   return 0;
 }
@@ -808,6 +1051,10 @@ int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_ol
                     dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->partials, c->sums, c->wgt,
                     dsc + offsetof(SolverScalars, aim_fwd) / sizeof(double), c->stream));
   c->launches += 2;   // forward, partial reduction, shift
+  if (c->solver == 1) {
+    CKL(launch_pol_forward_tau(c->Fsol, c->Ftau, c->Ftau_last, c->Ftau_dot, c->N, cutBack, guess, dt, dt_old,
+                              dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->polc, c->stream));
+  }
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -820,6 +1067,7 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
   if ((rc = upload_scalars(c, true))) return rc;
   CK(cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream));
   c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
+  if (c->solver == 1) return solution_polarization(c, out);
   const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
   const bool mixed = c->precision == DMK_PRECISION_MIXED;
   const bool anderson = c->num.snes_type == 1;
@@ -962,6 +1210,10 @@ int dmk_restart_write(dmk_ctx* c, dmk_restart* r) {
   std::memcpy(r->C_volAvg, c->C_volAvg, sizeof r->C_volAvg);
   std::memcpy(r->C_volAvgLastInc, c->C_volAvgLastInc, sizeof r->C_volAvgLastInc);
   std::memcpy(r->C_minMaxAvg, c->C_gamma, sizeof r->C_minMaxAvg);
+  if (c->solver == 1) {   // grid_mech_spectral_polarization_restartWrite (:412-415)
+    if (!r->F_tau || !r->F_tau_lastinc) return fail(DMK_ERR_ARG, "F_tau / F_tau_lastinc buffers are required");
+    if ((rc = d2h_planes(c, c->Ftau, r->F_tau, 9)) || (rc = d2h_planes(c, c->Ftau_last, r->F_tau_lastinc, 9))) return rc;
+  }
   return 0;
 }
 
@@ -975,6 +1227,10 @@ int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
       (rc = h2d_planes(c, r->L_p, c->Lp0, 9)) || (rc = h2d_planes(c, r->omega_plastic, c->state0, 2 * c->NS)) ||
       (rc = h2d_planes(c, r->F, c->Fsol, 9)) || (rc = h2d_planes(c, r->F_lastinc, c->Flast, 9)))
     return rc;
+  if (c->solver == 1) {   // grid_mech_spectral_polarization.f90:236-245
+    if (!r->F_tau || !r->F_tau_lastinc) return fail(DMK_ERR_ARG, "F_tau / F_tau_lastinc buffers are required");
+    if ((rc = h2d_planes(c, r->F_tau, c->Ftau, 9)) || (rc = h2d_planes(c, r->F_tau_lastinc, c->Ftau_last, 9))) return rc;
+  }
   CK(cudaMemcpyAsync(c->F, c->F0, b9, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Fp, c->Fp0, b9, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->Lp, c->Lp0, b9, cudaMemcpyDeviceToDevice, c->stream));
@@ -994,6 +1250,8 @@ int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
   std::memcpy(c->C_volAvgLastInc, r->C_volAvgLastInc, sizeof c->C_volAvgLastInc);
   std::memcpy(c->C_minMaxAvg, r->C_minMaxAvg, sizeof c->C_minMaxAvg);
   update_gamma_host(c, c->C_minMaxAvg);
+  if (c->solver == 1)
+    if ((rc = set_polarization_scale(c))) return rc;
   return 0;
 }
 
@@ -1027,6 +1285,7 @@ int dmk_field_size(dmk_ctx* c, int field) {
   if (field == DMK_FIELD_XI_SL || field == DMK_FIELD_GAMMA_SL) return c->NS;
   if (field == DMK_FIELD_O) return 4;
   if (field >= 0 && field <= DMK_FIELD_F_SOLVER) return 9;
+  if ((field == DMK_FIELD_F_TAU || field == DMK_FIELD_F_TAU_LASTINC) && c->solver == 1) return 9;
   return fail(DMK_ERR_ARG, "unknown field");
 }
 
@@ -1041,6 +1300,12 @@ int dmk_get_field(dmk_ctx* c, int field, double* host) {
     case DMK_FIELD_LP: return d2h_planes(c, c->Lp, host, 9);
     case DMK_FIELD_F_LASTINC: return d2h_planes(c, c->Flast, host, 9);
     case DMK_FIELD_F_SOLVER: return d2h_planes(c, c->Fsol, host, 9);
+    case DMK_FIELD_F_TAU:
+      if (c->solver != 1) break;
+      return d2h_planes(c, c->Ftau, host, 9);
+    case DMK_FIELD_F_TAU_LASTINC:
+      if (c->solver != 1) break;
+      return d2h_planes(c, c->Ftau_last, host, 9);
     case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NS);
     case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NS);
     case DMK_FIELD_S:
@@ -1075,6 +1340,11 @@ int dmk_set_field(dmk_ctx* c, int field, const double* host) {
   switch (field) {
     case DMK_FIELD_F_SOLVER: rc = h2d_planes(c, host, c->Fsol, 9); break;
     case DMK_FIELD_F_LASTINC: rc = h2d_planes(c, host, c->Flast, 9); break;
+    case DMK_FIELD_F_TAU:
+    case DMK_FIELD_F_TAU_LASTINC:
+      if (c->solver != 1) return fail(DMK_ERR_ARG, "F_tau exists for the polarization solver only");
+      rc = h2d_planes(c, host, field == DMK_FIELD_F_TAU ? c->Ftau : c->Ftau_last, 9);
+      break;
     default: return fail(DMK_ERR_ARG, "field is not settable");
   }
   if (rc) return rc;
@@ -1128,6 +1398,24 @@ int dmk_gamma_convolution(dmk_ctx* c, double* field, const double aim[9]) {
                      cudaMemcpyHostToDevice, c->stream));
   if ((rc = spectral_pass(c, false, 1, 0, c->r))) return rc;
   return d2h_planes(c, c->r, field, 9);
+}
+
+// utilities_curlRMS (spectral_utilities.f90:695-757) of a host tensor field; the solver's spectrum
+// and staging buffers are used as scratch.
+int dmk_curl_rms(dmk_ctx* c, const double* F, double* out) {
+  if (!c || !F || !out) return fail(DMK_ERR_ARG, "null argument");
+  if (int rc = h2d_planes(c, F, c->r, 9)) return rc;
+  CKF(cufftExecD2Z(c->plan_fwd, c->r, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
+  const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
+  CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->div_partials, c->stream));
+  const int nb = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
+  std::vector<double> h(nb);
+  CK(cudaMemcpyAsync(h.data(), c->div_partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  double s = 0.0;
+  for (double x : h) s += x;
+  *out = std::sqrt(s) * c->wgt * (c->cells[0] == 1 ? 0.5 : 1.0);
+  return 0;
 }
 
 int dmk_divergence_rms(dmk_ctx* c, const double* P, double* out) {
@@ -1239,7 +1527,8 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, (void*)c->tan.l2, (void*)c->tan.planes,
                   c->fft_work,
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
-                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->xp, (void*)c->xn, (void*)c->favg})
+                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->xp, (void*)c->xn, (void*)c->favg,
+                  (void*)c->Ftau_last, (void*)c->Ftau_dot, (void*)c->Feval, (void*)c->curl_partials})
     if (p) cudaFree(p);
   for (auto& l : c->plist)
     for (int* p : l)

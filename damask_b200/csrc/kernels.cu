@@ -381,6 +381,10 @@ __global__ void shift2_kernel(double* __restrict__ Fsol, int64_t N, const double
 #pragma unroll
   for (int k = 0; k < 9; ++k) Fsol[k * N + v] -= sums[k] * wgt - aim[k];
 }
+cudaError_t launch_reduce9(const double* partials, int nparts, double* out9, cudaStream_t s) {
+  reduce_partials9_kernel<<<1, 32, 0, s>>>(partials, nparts, out9);
+  return cudaGetLastError();
+}
 // stage 2: F -= (<F> * wgt - aim)
 cudaError_t launch_forward(double* Fsol, double* Flast, double* Fdot, int64_t N, int cutBack, int guess, double dt,
                            double dt_old, const double* avRate, double* partials, double* sums, double wgt,

@@ -66,6 +66,26 @@ cudaError_t launch_orientations(const double* Fe, int64_t N, double* out /* 4 pe
 cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaStream_t s);
 cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
 
+cudaError_t launch_reduce9(const double* partials, int nparts, double* out9, cudaStream_t s);
+
+// spectral polarization scheme (polarization.cu)
+struct PolConst {
+  double C[81];          // C_scale (column-major 3x3x3x3)
+  double S[81];          // S_scale = invSym3333(C_scale)
+  double alpha, beta;
+};
+cudaError_t launch_pol_pre(const double* F, const double* Ftau, int64_t N, const PolConst& pc, double* out,
+                           cudaStream_t s);
+cudaError_t launch_pol_tau(const double* F, double* G, int64_t N, double beta, double* Feval, cudaStream_t s);
+cudaError_t launch_pol_rF(const double* F, const double* Ftau, const double* P, const double* dPdF, const double* rtau,
+                          int64_t N, const PolConst& pc, double* rF, cudaStream_t s);
+cudaError_t launch_curl(const double* spec, int n0, int n1, int n2, const double L[3], const double rg[3],
+                        double* partials, cudaStream_t s);
+cudaError_t launch_pol_forward_tau(const double* F, double* Ftau, double* Flast, double* Fdot, int64_t N, int cutBack,
+                                   int guess, double dt, double dt_old, const double* avRate, const PolConst& pc,
+                                   cudaStream_t s);
+cudaError_t launch_sub(double* X, const double* r, int64_t n, int nsm, cudaStream_t s);
+
 // utilities_updateCoords (kernels.cu): u_hat from the spectrum of F (planes 0..2, Hermitian), then
 // cell-centre and node coordinates from the C2R output u (null: undeformed coordinates)
 cudaError_t launch_coords_spec(double* spec, int n0, int n1, int n2, const double L[3], double wgt, double* favg,

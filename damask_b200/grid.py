@@ -12,6 +12,7 @@ host logic drives the CUDA path and, in tests, the CPU oracle.
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import time
 from dataclasses import dataclass, field
@@ -22,7 +23,7 @@ from . import _lib
 from .config import LoadCase, Numerics, Phase, RestartStruct, SolutionStruct, geometric_fraction
 
 FIELDS = {'F': 0, 'P': 1, 'F_e': 2, 'F_p': 3, 'L_p': 4, 'S': 5, 'xi_sl': 6, 'gamma_sl': 7,
-          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12}
+          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12, 'F_tau': 13, 'F_tau_lastinc': 14}
 
 PRECISIONS = {'fp64': 0, 'mixed': 1}
 
@@ -129,13 +130,18 @@ class SpectralBasic:
     RESTART_FIELDS = ('F', 'F_lastinc', 'F_phase', 'F_p', 'L_p')
     RESTART_AIMS = ('P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot', 'C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg')
 
+    @property
+    def restart_fields(self) -> tuple:
+        pol = ('F_tau', 'F_tau_lastinc') if self.numerics.solver == 'spectral_polarization' else ()
+        return self.RESTART_FIELDS + pol
+
     def restart_write(self) -> dict:
         """The data the reference writes to its restart file, as numpy arrays (per voxel,
         voxel-major)."""
-        d = {k: np.empty((self.N, 9)) for k in self.RESTART_FIELDS}
+        d = {k: np.empty((self.N, 9)) for k in self.restart_fields}
         d['omega_plastic'] = np.empty((self.N, 2 * self.phase.n_slip))
         r = RestartStruct()
-        for k in self.RESTART_FIELDS + ('omega_plastic',):
+        for k in self.restart_fields + ('omega_plastic',):
             setattr(r, k, _dp(d[k]))
         _lib.check(self.lib.dmk_restart_write(self.ctx, C.byref(r)))
         for k in self.RESTART_AIMS:
@@ -144,9 +150,9 @@ class SpectralBasic:
 
     def restart_read(self, d: dict) -> None:
         """Resume from restart data on this (freshly initialised) context."""
-        keep = {k: np.ascontiguousarray(d[k], dtype=np.float64) for k in self.RESTART_FIELDS + ('omega_plastic',)}
+        keep = {k: np.ascontiguousarray(d[k], dtype=np.float64) for k in self.restart_fields + ('omega_plastic',)}
         if keep['omega_plastic'].shape != (self.N, 2 * self.phase.n_slip) or \
-                any(keep[k].shape != (self.N, 9) for k in self.RESTART_FIELDS):
+                any(keep[k].shape != (self.N, 9) for k in self.restart_fields):
             raise ValueError('restart data do not match the grid and phase of this context')
         r = RestartStruct()
         for k, v in keep.items():
@@ -210,6 +216,12 @@ class SpectralBasic:
         _lib.check(self.lib.dmk_gamma_convolution(self.ctx, _dp(f), _dp(a)))
         return f
 
+    def curl_rms(self, F: np.ndarray) -> float:
+        f = np.ascontiguousarray(F, dtype=np.float64).reshape(self.N, 9)
+        out = C.c_double()
+        _lib.check(self.lib.dmk_curl_rms(self.ctx, _dp(f), C.byref(out)))
+        return out.value
+
     def divergence_rms(self, P: np.ndarray) -> float:
         p = np.ascontiguousarray(P, dtype=np.float64).reshape(self.N, 9)
         out = C.c_double()
@@ -231,6 +243,22 @@ class SpectralBasic:
             self.close()
         except Exception:
             pass
+
+
+class SpectralPolarization(SpectralBasic):
+    """grid_mech_spectral_polarization on one GPU: the augmented-Lagrangian / polarization
+    scheme with F and F_tau as solution fields (alpha, beta, eps_*_curl(F) from numerics)."""
+
+    def __init__(self, cells, size, material: np.ndarray, quaternions: np.ndarray, phase: Phase,
+                 numerics: Numerics | None = None, precision: str = 'fp64', device: int = 0):
+        num = copy.copy(numerics or Numerics())
+        num.solver = 'spectral_polarization'
+        super().__init__(cells, size, material, quaternions, phase, num, precision, device)
+
+
+def mechanical_solver(name: str):
+    """The plugin class for load.yaml ``solver: mechanical: <name>`` (DAMASK_grid.f90:171-206)."""
+    return {'spectral_basic': SpectralBasic, 'spectral_polarization': SpectralPolarization}[name]
 
 
 def save_restart(path, data: dict, increment: int) -> None:

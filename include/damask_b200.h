@@ -86,6 +86,11 @@ typedef struct {
   int snes_type;               /* fixed-point iteration of the residual: 0 Richardson F <- F - r
                                   (PETSc -snes_type nrichardson), 1 Anderson-accelerated */
   int anderson_m;              /* Anderson history depth (1..32) */
+  /* mechanical solver, selected by load.yaml solver: mechanical: (DAMASK_grid.f90:171-206):
+     0 spectral_basic, 1 spectral_polarization (grid_mech_spectral_polarization.f90) */
+  int solver;
+  double alpha, beta;          /* polarization parameters: 0 < alpha <= 2, 0 <= beta <= 2 */
+  double eps_abs_curl, eps_rel_curl;   /* eps_abs_curl(F), eps_rel_curl(F) (polarization) */
 } dmk_numerics;
 
 /* tBCmech (grid_utilities.f90:35-39): values/mask column-major, mask 1 = 'x' */
@@ -121,15 +126,22 @@ enum {
   DMK_FIELD_FI = 9,
   DMK_FIELD_LI = 10,
   DMK_FIELD_F_SOLVER = 11, /* solution field F of the spectral solver */
-  DMK_FIELD_O = 12         /* orientation (4,N): unit quaternion w,x,y,z of the rotational part of Fe,
+  DMK_FIELD_O = 12,        /* orientation (4,N): unit quaternion w,x,y,z of the rotational part of Fe,
                               as crystallite_orientations (phase.f90:659-673); get only.  A voxel whose
                               rotation has |det - 1| > 1e-5 makes the call fail with DMK_ERR_STATE
                               (IO_error 402 of rotations.f90:221-222). */
+  DMK_FIELD_F_TAU = 13,    /* polarization solver: F_tau and F_tau_lastinc (3,3,N) */
+  DMK_FIELD_F_TAU_LASTINC = 14
 };
 
 /* Create a context and run grid_mechanical_spectral_basic_init
    (grid_mech_spectral_basic.f90:103-237; mechanical_init phase_mechanical.f90:184-338):
    F := I, one constitutive sweep at dt = 0, Gamma reference stiffness := C_minMaxAvg.
+   With num->solver = 1 the context is grid_mech_spectral_polarization instead (init
+   grid_mech_spectral_polarization.f90:115-270: also F_tau := 2 I, C_scale := C_minMaxAvg,
+   S_scale := invSym3333(C_minMaxAvg)); forward, solution, updateCoords and the restart calls
+   then follow that module, with F_tau as a second solution field.  The polarization scheme
+   runs its spectral steps in FP64 for either precision.
    materialAt: N entries, 0-based material index; quaternions: 4 per material (w,x,y,z).
    precision: DMK_PRECISION_FP64 or DMK_PRECISION_MIXED. device: CUDA ordinal. */
 int dmk_mech_init(dmk_ctx** ctx, const int cells[3], const double geomSize[3], const int* materialAt,
@@ -181,6 +193,8 @@ typedef struct {
   double P_aim[9], F_aim[9], F_aim_lastinc[9], F_aimDot[9];
   double C_volAvg[81], C_volAvgLastInc[81];
   double C_minMaxAvg[81];   /* the Gamma reference stiffness in use (C_minMaxAvgRestart) */
+  double* F_tau;            /* polarization solver only (else unused): F_tau, F_tau_lastinc (9 N each), */
+  double* F_tau_lastinc;    /* grid_mech_spectral_polarization.f90:412-415 */
 } dmk_restart;
 
 /* Fill r (caller-allocated arrays) from the context, after a converged increment and
@@ -211,6 +225,9 @@ int dmk_update_gamma(dmk_ctx* ctx, const double C[81]);
 int dmk_gamma_convolution(dmk_ctx* ctx, double* field, const double aim[9]);
 /* utilities_divergenceRMS, spectral_utilities.f90:650-691 */
 int dmk_divergence_rms(dmk_ctx* ctx, const double* P, double* out);
+/* utilities_curlRMS, spectral_utilities.f90:695-757 (the polarization scheme's compatibility
+   criterion); uses the solver's scratch buffers, so call it between solutions */
+int dmk_curl_rms(dmk_ctx* ctx, const double* F, double* out);
 /* phase_mechanical_dPdF, phase_mechanical.f90:1121-1242, for every voxel (81 per voxel) */
 int dmk_dPdF(dmk_ctx* ctx, double dt, double* dPdF);
 

@@ -473,6 +473,10 @@ struct orc_ctx {
   std::vector<double> xp, xn;     // discretization_IPcoords / _NodeCoords, 3 per point
   // basic solver (grid_mech_spectral_basic.f90:30-45)
   std::vector<M3> Fsol, F_lastinc, Fdot;
+  // polarization solver (grid_mech_spectral_polarization.f90:61-95)
+  std::vector<M3> Ftau, Ftau_lastinc, Ftaudot;
+  T4 C_scale, S_scale;
+  double err_curl = 0.0;
   M3 F_aim, F_aim_lastinc, F_aimDot, P_aim, P_av;
   T4 C_volAvg, C_volAvgLastInc, C_minMaxAvg, C_minMaxAvgLastInc, C_minMaxAvgRestart, Scomp;
   bool stress_mask[3][3];
@@ -1152,6 +1156,110 @@ void form_residual(orc_ctx* c, std::vector<M3>& r) {
   gamma_convolution(c, r.data(), rot33(c->rot_q, deltaF_aim, true));
 }
 
+// math_sym3333to66, math.f90:826-845: rows/columns in the Mandel order (11,22,33,23,13,12),
+// weights 1 for normal and sqrt(2) for shear pairs; the (i<j) components are the ones read.
+void sym3333to66(const T4& m, double out[6][6]) {
+  const int p[6][2] = {{0, 0}, {1, 1}, {2, 2}, {1, 2}, {0, 2}, {0, 1}};
+  for (int r = 0; r < 6; ++r) for (int q = 0; q < 6; ++q)
+    out[r][q] = m.a[p[r][0]][p[r][1]][p[q][0]][p[q][1]] * (r < 3 ? 1.0 : SQRT2) * (q < 3 ? 1.0 : SQRT2);
+}
+// math_invSym3333, math.f90:511-532 (dgetrf + dgetri of the Mandel 6x6)
+T4 inv_sym3333(const T4& A) {
+  double m[6][6], inv[36], mi[6][6];
+  sym3333to66(A, m);
+  invert_n(inv, &m[0][0], 6);
+  for (int r = 0; r < 6; ++r) for (int q = 0; q < 6; ++q) mi[r][q] = inv[r * 6 + q];
+  return m66toSym3333(mi);
+}
+
+// utilities_curlRMS, spectral_utilities.f90:695-757 (spectrum of the field in c->work).  The
+// planes kx = 0 and kx = cells1/2 (stored index cells1Red) assign every entry of curl_fourier
+// the last of the nine expressions (l = 3, third column), as the reference does.
+double curl_rms(orc_ctx* c) {
+  const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
+  const double rg[3] = {c->geomSize[0] / c->scaledGeomSize[0], c->geomSize[1] / c->scaledGeomSize[1],
+                        c->geomSize[2] / c->scaledGeomSize[2]};
+  auto xi = [&](int x, int y, int z, int d) { return cd(0.0, c->xi[fidx(c, x, y, z) * 3 + d]) * cd(rg[d], 0.0); };
+  auto T = [&](int l, int m, int x, int y, int z) { return spec(c, l + 3 * m, x, y, z); };
+  double res = 0.0;
+  for (int y = 0; y < n1; ++y) for (int z = 0; z < n2; ++z) {
+    for (int x = 1; x < c->red - 1; ++x) {
+      double s = 0.0;
+      for (int l = 0; l < 3; ++l) {
+        const cd c1 = T(l, 2, x, y, z) * xi(x, y, z, 1) - T(l, 1, x, y, z) * xi(x, y, z, 2);
+        const cd c2 = T(l, 0, x, y, z) * xi(x, y, z, 2) - T(l, 2, x, y, z) * xi(x, y, z, 0);
+        const cd c3 = T(l, 1, x, y, z) * xi(x, y, z, 0) - T(l, 0, x, y, z) * xi(x, y, z, 1);
+        s += c1.real() * c1.real() + c2.real() * c2.real() + c3.real() * c3.real();
+        s += c1.imag() * c1.imag() + c2.imag() * c2.imag() + c3.imag() * c3.imag();
+      }
+      res += 2.0 * s;
+    }
+    for (int x : {0, c->red - 1}) {
+      const cd last = T(2, 1, x, y, z) * xi(x, y, z, 0) - T(2, 0, x, y, z) * xi(x, y, z, 1);
+      res += 9.0 * (last.real() * last.real() + last.imag() * last.imag());
+    }
+  }
+  res = std::sqrt(res) * c->wgt;
+  if (n0 == 1) res *= 0.5;
+  return res;
+}
+
+// volume average sum(sum(sum(field,dim=5),dim=4),dim=3) * wgt
+M3 field_average(const orc_ctx* c, const std::vector<M3>& f) {
+  const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
+  M3 a = zero3();
+  for (int x = 0; x < n0; ++x) {
+    M3 sy = zero3();
+    for (int y = 0; y < n1; ++y) { M3 sz = zero3(); for (int z = 0; z < n2; ++z) sz = add(sz, f[(long(z) * n1 + y) * n0 + x]); sy = add(sy, sz); }
+    a = add(a, sy);
+  }
+  return scl(c->wgt, a);
+}
+
+// form_residual of the polarization scheme, grid_mech_spectral_polarization.f90:562-632.
+// F in c->Fsol, F_tau in c->Ftau; r = [r_F (N); r_F_tau (N)].
+void form_residual_pol(orc_ctx* c, std::vector<M3>& r) {
+  const long N = c->N;
+  const double alpha = c->num.alpha, beta = c->num.beta;
+  const M3 I = eye3();
+  const M3 F_av = field_average(c, c->Fsol);
+  c->totalIter++;
+  std::vector<M3> t(N), rtau(N), Feval(N);
+  for (long v = 0; v < N; ++v) {
+    const M3& F = c->Fsol[v];
+    t[v] = sub(scl(beta, mul4x2(c->C_scale, sub(F, I))),
+               scl(alpha, mm(F, mul4x2(c->C_scale, sub(sub(c->Ftau[v], F), I)))));
+  }
+  r2c(c, t.data());
+  gamma_convolution(c, t.data(), rot33(c->rot_q, scl(beta, c->F_aim), true));
+  for (long v = 0; v < N; ++v) {
+    rtau[v] = sub(scl(beta, c->Fsol[v]), t[v]);
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) Feval[v].a[i][j] = c->Fsol[v].a[i][j] - rtau[v].a[i][j] / beta;
+  }
+  r2c(c, c->Fsol.data());
+  c->err_curl = curl_rms(c);
+  std::swap(c->Fsol, Feval);
+  c->status = constitutive_response(c, c->dt, true);
+  std::swap(c->Fsol, Feval);
+  r2c(c, c->homP.data());
+  c->err_div = divergence_rms(c);
+  #pragma omp parallel for schedule(static) num_threads(c->nthreads)
+  for (long v = 0; v < N; ++v) {
+    const M3& F = c->Fsol[v];
+    T4 A = c->homdPdF[v];
+    for (int i = 0; i < 81; ++i) (&A.a[0][0][0][0])[i] += (&c->C_scale.a[0][0][0][0])[i];
+    const M3 rhs = sub(c->homP[v], mm(F, mul4x2(c->C_scale, sub(sub(c->Ftau[v], F), I))));
+    r[v] = add(mul4x2(inv_sym3333(A), rhs), rtau[v]);
+    r[N + v] = rtau[v];
+  }
+  const M3 d = sub(c->P_av, c->P_aim);
+  c->F_aim = sub(c->F_aim, mul4x2(c->Scomp, d));
+  const M3 e = mul4x2(c->C_scale, sub(c->F_aim, rot33(c->rot_q, F_av, false)));
+  double eb = 0.0;
+  for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) eb = std::max(eb, std::fabs(c->stress_mask[i][j] ? e.a[i][j] : d.a[i][j]));
+  c->err_BC = eb;
+}
+
 // Least-squares coefficients of the Anderson update: solve G_S gamma = b_S on the
 // slots S (oldest first) by Cholesky; while a pivot is not safely positive
 // (< 1e-13 of the largest diagonal), drop the oldest slot and retry.
@@ -1257,11 +1365,22 @@ orc_ctx* orc_create(const int cells[3], const double geomSize[3], const int* mat
 void orc_destroy(orc_ctx* c) { delete c; }
 
 // grid_mechanical_spectral_basic_init, grid_mech_spectral_basic.f90:103-237 (no restart)
+// grid_mech_spectral_polarization_init, grid_mech_spectral_polarization.f90:115-270 (no restart):
+// in addition F_tau = F_tau_lastinc = 2 I, C_scale = C_minMaxAvg, S_scale = its Mandel inverse
 int orc_mech_init(orc_ctx* c) {
   for (long v = 0; v < c->N; ++v) { c->F_lastinc[v] = eye3(); c->Fsol[v] = eye3(); }
+  if (c->num.solver == 1) {
+    c->Ftau.assign(c->N, scl(2.0, eye3()));
+    c->Ftau_lastinc = c->Ftau;
+    c->Ftaudot.assign(c->N, zero3());
+  }
   int status = constitutive_response(c, 0.0, false);
   update_gamma(c, c->C_minMaxAvg);
   c->C_minMaxAvgRestart = c->C_minMaxAvg;
+  if (c->num.solver == 1) {
+    c->C_scale = c->C_minMaxAvg;
+    c->S_scale = inv_sym3333(c->C_minMaxAvg);
+  }
   return status;
 }
 
@@ -1294,6 +1413,13 @@ int orc_mech_forward(orc_ctx* c, int cutBack, int guess, double dt, double dt_ol
     for (long v = 0; v < N; ++v) c->Fdot[v] = avRate;
     if (guess) for (long v = 0; v < N; ++v) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j)
       c->Fdot[v].a[i][j] = (c->Fsol[v].a[i][j] - c->F_lastinc[v].a[i][j]) / dt_old;
+    if (c->num.solver == 1) {
+      // F_tauDot = utilities_calculateRate(guess, F_tau_lastinc, F_tau, ...), polarization.f90:366-368
+      for (long v = 0; v < N; ++v) c->Ftaudot[v] = avRate;
+      if (guess) for (long v = 0; v < N; ++v) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j)
+        c->Ftaudot[v].a[i][j] = (c->Ftau[v].a[i][j] - c->Ftau_lastinc[v].a[i][j]) / dt_old;
+      c->Ftau_lastinc = c->Ftau;
+    }
     c->F_lastinc = c->Fsol;
   }
   c->F_aim = add(c->F_aim_lastinc, scl(dt, c->F_aimDot));
@@ -1315,6 +1441,19 @@ int orc_mech_forward(orc_ctx* c, int cutBack, int guess, double dt, double dt_ol
   }
   diff = sub(scl(c->wgt, diff), aim);
   for (long v = 0; v < N; ++v) c->Fsol[v] = sub(c->Fsol[v], diff);
+  if (c->num.solver == 1) {
+    // grid_mech_spectral_polarization.f90:384-396
+    if (guess) {
+      for (long v = 0; v < N; ++v) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j)
+        c->Ftau[v].a[i][j] = c->Ftau_lastinc[v].a[i][j] + c->Ftaudot[v].a[i][j] * dt;
+    } else {
+      for (long v = 0; v < N; ++v) {
+        const M3 Fl = sub(c->Ftau[v], c->Fsol[v]);
+        const M3 t = add(eye3(), mul4x2(c->S_scale, scl(0.5, mm(Fl, mul4x2(c->C_scale, sub(mm(tr(Fl), Fl), eye3()))))));
+        c->Ftau[v] = add(t, c->Fsol[v]);
+      }
+    }
+  }
   for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) c->stress_mask[i][j] = msk(stress->mask, i, j);
   for (int i = 0; i < 4; ++i) c->rot_q[i] = q_rot[i];
   c->dt = dt;
@@ -1325,32 +1464,57 @@ int orc_mech_forward(orc_ctx* c, int cutBack, int guess, double dt, double dt_ol
 // residual iterated as SNES nrichardson + basic line search: F <- F - r(F).
 int orc_mech_solution(orc_ctx* c, orc_solution* out) {
   std::memset(c->counters, 0, sizeof c->counters);
+  const bool pol = c->num.solver == 1;
   c->Scomp = masked_compliance(c, c->C_volAvg);
-  if (c->num.update_gamma) update_gamma(c, c->C_minMaxAvg);
+  if (c->num.update_gamma) {
+    update_gamma(c, c->C_minMaxAvg);
+    if (pol) { c->C_scale = c->C_minMaxAvg; c->S_scale = inv_sym3333(c->C_minMaxAvg); }
+  }
   const int snes_max_its = 50;    // PETSc SNES default maximum number of iterations
-  std::vector<M3> r(c->N);
+  // iteration vector X: F (basic), or [F; F_tau] (polarization), with its residual r
+  const long NX = pol ? 2 * c->N : c->N;
+  std::vector<M3> X(NX), r(NX);
+  auto load = [&]() {
+    for (long v = 0; v < c->N; ++v) X[v] = c->Fsol[v];
+    if (pol) for (long v = 0; v < c->N; ++v) X[c->N + v] = c->Ftau[v];
+  };
+  auto residual = [&]() {
+    for (long v = 0; v < c->N; ++v) c->Fsol[v] = X[v];
+    if (pol) {
+      for (long v = 0; v < c->N; ++v) c->Ftau[v] = X[c->N + v];
+      form_residual_pol(c, r);
+    } else {
+      form_residual(c, r);
+    }
+  };
+  load();
   c->totalIter = -1;
   int evals = 0;
   int reason = 0;   // 0 iterating, 1 converged, -1 diverged
   auto converged = [&]() {
-    double pmax = 0.0;
-    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) pmax = std::max(pmax, std::fabs(c->P_av.a[i][j]));
+    double pmax = 0.0, fmax = 0.0;
+    for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) {
+      pmax = std::max(pmax, std::fabs(c->P_av.a[i][j]));
+      fmax = std::max(fmax, std::fabs(c->F_aim.a[i][j] - (i == j ? 1.0 : 0.0)));
+    }
     double divTol = std::max(pmax * c->num.eps_rel_div, c->num.eps_abs_div);
     double BCTol = std::max(pmax * c->num.eps_rel_P, c->num.eps_abs_P);
-    if (c->totalIter >= c->num.N_iter_min && c->err_div / divTol < 1.0 && c->err_BC / BCTol < 1.0 && c->status == ST_OK) return 1;
+    bool ok = c->err_div / divTol < 1.0 && c->err_BC / BCTol < 1.0;
+    if (pol) ok = ok && c->err_curl / std::max(fmax * c->num.eps_rel_curl, c->num.eps_abs_curl) < 1.0;   // polarization.f90:530-541
+    if (c->totalIter >= c->num.N_iter_min && ok && c->status == ST_OK) return 1;
     if (c->totalIter >= c->num.N_iter_max) return -1;
     return 0;
   };
   auto finite = [&]() {
-    for (long v = 0; v < c->N; ++v) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) if (!std::isfinite(r[v].a[i][j])) return false;
+    for (long v = 0; v < NX; ++v) for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) if (!std::isfinite(r[v].a[i][j])) return false;
     return true;
   };
-  form_residual(c, r); evals++;
+  residual(); evals++;
   if (!finite()) reason = -1; else reason = converged();
   if (c->num.snes_type == 0) {
     for (int it = 1; reason == 0 && it <= snes_max_its; ++it) {
-      for (long v = 0; v < c->N; ++v) c->Fsol[v] = sub(c->Fsol[v], r[v]);
-      form_residual(c, r); evals++;
+      for (long v = 0; v < NX; ++v) X[v] = sub(X[v], r[v]);
+      residual(); evals++;
       if (!finite()) { reason = -1; break; }
       reason = converged();
       if (reason == 0 && it == snes_max_its) reason = -1;
@@ -1360,7 +1524,7 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
     // gamma = argmin |r_k - dR gamma|, X_{k+1} = X_k - r_k - (dX - dR) gamma, where dX, dR hold
     // the last m differences of iterates and residuals.
     const int m = std::max(1, std::min(c->num.anderson_m, 32));
-    const long N = c->N;
+    const long N = NX;
     std::vector<std::vector<M3>> dX(m, std::vector<M3>(N)), dR(m, std::vector<M3>(N));
     std::vector<M3> Rprev(N);
     std::vector<double> G(size_t(m) * m, 0.0);
@@ -1377,16 +1541,16 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
       std::vector<double> gam = anderson_coefficients(G, m, slots, [&](int sl) { return dot(dR[sl], r); });
       const int slot = count % m;
       for (long v = 0; v < N; ++v) {
-        M3 xn = sub(c->Fsol[v], r[v]);
+        M3 xn = sub(X[v], r[v]);
         for (size_t q = 0; q < slots.size(); ++q) {
           if (gam[q] == 0.0) continue;
           xn = sub(xn, scl(gam[q], sub(dX[slots[q]][v], dR[slots[q]][v])));
         }
-        dX[slot][v] = sub(xn, c->Fsol[v]);
-        c->Fsol[v] = xn;
+        dX[slot][v] = sub(xn, X[v]);
+        X[v] = xn;
         Rprev[v] = r[v];
       }
-      form_residual(c, r); evals++;
+      residual(); evals++;
       if (!finite()) { reason = -1; break; }
       for (long v = 0; v < N; ++v) dR[slot][v] = sub(r[v], Rprev[v]);
       ++count;
@@ -1453,6 +1617,13 @@ void orc_gamma_convolution(orc_ctx* c, double* field, const double aim[9]) {
   for (long v = 0; v < c->N; ++v) for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) field[9 * v + 3 * j + i] = f[v].a[i][j];
 }
 
+double orc_curl_rms(orc_ctx* c, const double* F) {
+  std::vector<M3> f(c->N);
+  for (long v = 0; v < c->N; ++v) for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) f[v].a[i][j] = F[9 * v + 3 * j + i];
+  r2c(c, f.data());
+  return curl_rms(c);
+}
+
 double orc_divergence_rms(orc_ctx* c, const double* P) {
   std::vector<M3> f(c->N);
   for (long v = 0; v < c->N; ++v) for (int j = 0; j < 3; ++j) for (int i = 0; i < 3; ++i) f[v].a[i][j] = P[9 * v + 3 * j + i];
@@ -1472,7 +1643,8 @@ static std::vector<M3>* field_ptr(orc_ctx* c, int field) {
   switch (field) {
     case 0: return &c->F; case 1: return &c->P; case 2: return &c->Fe; case 3: return &c->Fp;
     case 4: return &c->Lp; case 5: return &c->S; case 8: return &c->F_lastinc; case 9: return &c->Fi;
-    case 10: return &c->Li; case 11: return &c->Fsol;
+    case 10: return &c->Li; case 11: return &c->Fsol; case 13: return &c->Ftau;
+    case 14: return &c->Ftau_lastinc;
     default: return nullptr;
   }
 }
@@ -1573,6 +1745,8 @@ void orc_get_aims(orc_ctx* c, double F_aim[9], double P_aim[9], double C_volAvg[
     C_minMaxAvg[i + 3 * j + 9 * k + 27 * l] = c->C_minMaxAvg.a[i][j][k][l];
   }
 }
+
+double orc_err_curl(orc_ctx* c) { return c->err_curl; }
 
 void orc_counters(orc_ctx* c, int64_t out[4]) { for (int i = 0; i < 4; ++i) out[i] = c->counters[i]; }
 

@@ -56,6 +56,9 @@ typedef struct {
   int f_update_jacobi_Li;
   int snes_type;               /* 0 Richardson (nrichardson), 1 Anderson-accelerated */
   int anderson_m;              /* Anderson history depth */
+  int solver;                  /* 0 spectral_basic, 1 spectral_polarization */
+  double alpha, beta;          /* polarization scheme parameters */
+  double eps_abs_curl, eps_rel_curl;
 } orc_numerics;
 
 typedef struct {
@@ -80,7 +83,8 @@ orc_ctx* orc_create(const int cells[3], const double geomSize[3], const int* mat
                     const orc_numerics* num, int n_threads);
 void orc_destroy(orc_ctx*);
 
-/* grid_mechanical_spectral_basic_* (grid_mech_spectral_basic.f90:103-355) */
+/* grid_mechanical_spectral_basic_* (grid_mech_spectral_basic.f90:103-355), or with
+   num->solver = 1 grid_mech_spectral_polarization_* (grid_mech_spectral_polarization.f90:115-636) */
 int  orc_mech_init(orc_ctx*);
 int  orc_mech_forward(orc_ctx*, int cutBack, int guess, double dt, double dt_old, double t_remaining,
                       const orc_bc* deformation, const orc_bc* stress, const double q_rot[4]);
@@ -97,13 +101,18 @@ int  orc_constitutive_response(orc_ctx*, const double* F, double dt, double* P, 
 void orc_update_gamma(orc_ctx*, const double C[81]);
 void orc_gamma_convolution(orc_ctx*, double* field, const double aim[9]);
 double orc_divergence_rms(orc_ctx*, const double* P);
+double orc_curl_rms(orc_ctx*, const double* F);   /* utilities_curlRMS, spectral_utilities.f90:695-757 */
 void orc_dPdF(orc_ctx*, double dt, double* dPdF /* 81 per voxel */);
 
 /* field access: 0 F, 1 P, 2 Fe, 3 Fp, 4 Lp, 5 S, 6 xi_sl, 7 gamma_sl, 8 F_lastinc, 9 Fi, 10 Li,
-   11 F of the solver, 12 O (orientation quaternion w,x,y,z per voxel; get only) */
+   11 F of the solver, 12 O (orientation quaternion w,x,y,z per voxel; get only),
+   13 F_tau and 14 F_tau_lastinc of the polarization solver */
 int  orc_get_field(orc_ctx*, int field, double* out);
 int  orc_set_field(orc_ctx*, int field, const double* in);
 void orc_get_aims(orc_ctx*, double F_aim[9], double P_aim[9], double C_volAvg[81], double C_minMaxAvg[81]);
+
+/* err_curl of the last polarization residual */
+double orc_err_curl(orc_ctx*);
 
 /* counters for the last call: constitutive calls, Newton iterations, state iterations */
 void orc_counters(orc_ctx*, int64_t out[4]);

@@ -19,7 +19,7 @@ from damask_b200.config import BCStruct, LoadCase, Numerics, NumericsStruct, Pha
 HERE = Path(__file__).resolve().parent
 LIB = HERE / 'build' / 'liboracle.so'
 FIELDS = {'F': 0, 'P': 1, 'F_e': 2, 'F_p': 3, 'L_p': 4, 'S': 5, 'xi_sl': 6, 'gamma_sl': 7,
-          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12}
+          'F_lastinc': 8, 'F_i': 9, 'L_i': 10, 'F_solver': 11, 'O': 12, 'F_tau': 13, 'F_tau_lastinc': 14}
 _lib = None
 dp = C.POINTER(C.c_double)
 
@@ -52,6 +52,7 @@ def load() -> C.CDLL:
         'orc_update_gamma': (None, [vp, dp]),
         'orc_gamma_convolution': (None, [vp, dp, dp]),
         'orc_divergence_rms': (C.c_double, [vp, dp]),
+        'orc_curl_rms': (C.c_double, [vp, dp]),
         'orc_dPdF': (None, [vp, C.c_double, dp]),
         'orc_get_field': (C.c_int, [vp, C.c_int, dp]),
         'orc_set_field': (C.c_int, [vp, C.c_int, dp]),
@@ -60,6 +61,7 @@ def load() -> C.CDLL:
         'orc_schmid': (C.c_int, [C.POINTER(PhaseStruct), C.c_int, dp]),
         'orc_interaction': (C.c_int, [C.POINTER(PhaseStruct), dp]),
         'orc_fft3': (None, [dp, C.POINTER(C.c_int), C.c_int]),
+        'orc_err_curl': (C.c_double, [vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
@@ -160,6 +162,9 @@ class OracleSpectralBasic:
         a = np.ascontiguousarray(aim, dtype=np.float64).reshape(9)
         self.lib.orc_gamma_convolution(self.ctx, _p(f), _p(a))
         return f
+
+    def curl_rms(self, F) -> float:
+        return self.lib.orc_curl_rms(self.ctx, _p(np.ascontiguousarray(F, dtype=np.float64)))
 
     def divergence_rms(self, P) -> float:
         p = np.ascontiguousarray(P, dtype=np.float64).reshape(self.N, 9)
