@@ -1473,6 +1473,17 @@ int dmk_phase_schmid(const dmk_phase* phase, int sense, double* out) {
   return hp.Ns;
 }
 
+int dmk_phase_slip_systems(const dmk_phase* phase, int* out) {
+  if (!phase || !out) return fail(DMK_ERR_ARG, "invalid argument");
+  HostPhase hp;
+  std::string err;
+  if (build_host_phase(*phase, hp, err)) return fail(DMK_ERR_CONFIG, err);
+  const auto m = slip_miller(*phase);
+  for (size_t s = 0; s < m.size(); ++s)
+    for (int k = 0; k < 6; ++k) out[6 * s + k] = m[s][k];
+  return int(m.size());
+}
+
 int dmk_phase_interaction(const dmk_phase* phase, double* h) {
   if (!phase || !h) return fail(DMK_ERR_ARG, "invalid argument");
   HostPhase hp;

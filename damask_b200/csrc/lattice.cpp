@@ -231,4 +231,19 @@ bool invert_dense(const double* A, double* Ainv, int n) {
   return false;
 }
 
+// Miller indices (direction, plane normal) of the active systems, in system order
+std::vector<std::array<int, 6>> slip_miller(const dmk_phase& p) {
+  const int* famMax = p.lattice == 0 ? CF_NSLIP_FAMILY : CI_NSLIP_FAMILY;
+  std::vector<std::array<int, 6>> out;
+  int base = 0;
+  for (int f = 0; f < p.n_families; ++f) {
+    for (int s = 0; s < p.N_sl[f]; ++s) {
+      const signed char* row = p.lattice == 0 ? CF_SLIP_SYSTEMS[base + s] : CI_SLIP_SYSTEMS[base + s];
+      out.push_back({row[0], row[1], row[2], row[3], row[4], row[5]});
+    }
+    base += famMax[f];
+  }
+  return out;
+}
+
 }  // namespace dmk

@@ -23,6 +23,9 @@ struct HostPhase {
 // Returns 0 on success; err describes invalid input otherwise.
 int build_host_phase(const dmk_phase& p, HostPhase& hp, std::string& err);
 
+// Miller indices (direction d1 d2 d3, plane normal n1 n2 n3) of the active slip systems
+std::vector<std::array<int, 6>> slip_miller(const dmk_phase& p);
+
 // Unit quaternion (w,x,y,z) -> orientation matrix, column-major (rotations.f90:399-423, P = -1)
 void quaternion_to_matrix(const double* q, double* om);
 

@@ -248,6 +248,10 @@ int dmk_get_timings(dmk_ctx* ctx, double out[3]);
    reacting system).  Return the number of systems Ns, or an error code < 0. */
 int dmk_phase_schmid(const dmk_phase* phase, int sense, double* out);
 int dmk_phase_interaction(const dmk_phase* phase, double* h);
+/* Miller indices of the active slip systems (6 per system: direction d1 d2 d3, plane normal
+   n1 n2 n3, the rows of CF_SYSTEMSLIP / CI_SYSTEMSLIP, crystal.f90:43,125) for the 'systems'
+   labels of slip outputs (crystal_labels_slip, crystal.f90:1642-1676).  Returns Ns. */
+int dmk_phase_slip_systems(const dmk_phase* phase, int* out);
 
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);

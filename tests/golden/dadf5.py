@@ -130,6 +130,36 @@ class DADF5:
             raise KeyError(f'{path} is not a group')
         return sorted(self._group_members(*tab))
 
+    def attrs(self, path=''):
+        """Attributes of an object: {name: value} (strings decoded, numbers as numpy values)."""
+        out = {}
+        for mtype, d, _ in self._messages(self._resolve(path)):
+            if mtype != 0x0C:
+                continue
+            ver = self.b[d]
+            nlen, tlen, slen = self._u(d + 2, 2), self._u(d + 4, 2), self._u(d + 6, 2)
+            pad = (lambda x: (x + 7) // 8 * 8) if ver == 1 else (lambda x: x)
+            off = d + 8 + (1 if ver == 3 else 0)
+            name = self.b[off:off + nlen].split(b'\x00')[0].decode()
+            off += pad(nlen)
+            vlen = self.b[off] & 0x0F == 9
+            dt = np.dtype([('len', '<u4'), ('addr', '<u8'), ('idx', '<u4')]) if vlen else self._datatype(off)
+            off += pad(tlen)
+            shape = self._dataspace(off)
+            off += pad(slen)
+            n = int(np.prod(shape)) if shape else 1
+            val = np.frombuffer(self.b, dt, n, off)
+            if vlen:                                               # variable-length strings
+                val = [self._global_heap(int(e['addr']), int(e['idx']))[:int(e['len'])].decode() for e in val]
+                out[name] = val[0] if not shape else val
+                continue
+            if dt.kind == 'S':
+                val = [v.split(b'\x00')[0].decode() for v in val]
+                out[name] = val[0] if not shape else val
+            else:
+                out[name] = val[0] if not shape else val.reshape(shape).copy()
+        return out
+
     def read(self, path):
         addr = self._resolve(path)
         shape = dtype = layout = None
@@ -192,7 +222,42 @@ class DADF5:
             return np.dtype(f'{order}f{size}')
         if cls == 0:
             return np.dtype(f'{order}{"i" if bits0 & 8 else "u"}{size}')
+        if cls == 3:
+            return np.dtype(f'S{size}')
+        if cls == 6:                                               # compound, version 1 members
+            nmem = self._u(d + 1, 2)
+            off, fields = d + 8, []
+            for _ in range(nmem):
+                e = self.b.index(b'\x00', off)
+                name = self.b[off:e].decode()
+                off += (e - off + 1 + 7) // 8 * 8
+                moff = self._u(off, 4)
+                off += 4 + 1 + 3 + 4 + 4 + 16
+                mt = self._datatype(off)
+                fields.append((name, mt, moff))
+                off += self._dtype_msg_size(off)
+            return np.dtype({'names': [f[0] for f in fields], 'formats': [f[1] for f in fields],
+                             'offsets': [f[2] for f in fields], 'itemsize': size})
         raise ValueError(f'datatype class {cls} not supported')
+
+    def _global_heap(self, addr, index):
+        """Object `index` of the global heap collection at `addr`."""
+        if self.b[addr:addr + 4] != b'GCOL':
+            raise ValueError('global heap signature')
+        end = addr + self._u(addr + 8, 8)
+        off = addr + 16
+        while off + 16 <= end:
+            idx, size = self._u(off, 2), self._u(off + 8, 8)
+            if idx == index:
+                return self.b[off + 16:off + 16 + size]
+            if idx == 0:
+                break
+            off += 16 + (size + 7) // 8 * 8
+        raise KeyError(f'global heap object {index}')
+
+    def _dtype_msg_size(self, d):
+        cls = self.b[d] & 0x0F
+        return 8 + {0: 4, 1: 12, 3: 0}[cls]
 
     def _layout(self, d):
         b = self.b

@@ -16,7 +16,10 @@ compares every dataset at rtol 2.5 %, atol = max(1e-5 max|x|, 1e-6).
 Fixture contents: ``material`` (0-based material index per cell, x fastest), ``cells``,
 ``size``, ``quaternions`` (one per material), the phase, load and numerics dictionaries
 as JSON strings, and ``xi_sl_<inc>`` / ``gamma_sl_<inc>`` for the stored increments
-0, 75 and 150 (shape (cells, N_sl)).  Also ``vti_known``: the base64 known answers of
+0, 75 and 150 (shape (cells, N_sl)), ``u_p_<inc>`` / ``u_n_<inc>`` (displacements of cell
+centres and nodes) for 75 and 150, and ``layout_json``: the result file's group tree for the
+written phase (groups, datasets with shape, dtype and the attributes other than
+creator/created, the t/s of each increment, the root and geometry attributes).  Also ``vti_known``: the base64 known answers of
 the reference's VTI decoder tests (``tests/unit_cpp/test_VTI.cpp``) with their decoded
 bytes, for the reader in ``damask_b200/vti.py``.
 """
@@ -53,6 +56,32 @@ def vti_known_answers(root: Path) -> dict:
             'comp64': (consts['B64_COMP64'], 8, True, exp['EXPECTED_COMPRESSED'])}
 
 
+def _plain(v):
+    return v.tolist() if isinstance(v, np.ndarray) else (v.item() if isinstance(v, np.generic) else v)
+
+
+def layout(f: DADF5, phase: str) -> dict:
+    """Group tree of the reference's result file restricted to one phase."""
+    def attrs(path):
+        return {k: _plain(v) for k, v in f.attrs(path).items() if k not in ('creator', 'created', 'call')}
+
+    def walk(path):
+        out = {}
+        for k in f.keys(path):
+            p = f'{path}/{k}'.strip('/')
+            if p.count('/') == 2 and p.split('/')[1] == 'phase' and k != phase:
+                continue                                          # other phases of the file
+            try:
+                out[k] = {'groups': walk(p), 'attrs': attrs(p)}
+            except KeyError:
+                d = f.read(p)
+                out[k] = {'shape': list(d.shape), 'dtype': str(d.dtype) if not d.dtype.names else list(d.dtype.names),
+                          'attrs': attrs(p)}
+        return out
+
+    return {'root_attrs': sorted(f.attrs('')), 'tree': walk('')}
+
+
 def main(root: str) -> None:
     root = Path(root)
     res = root / 'tests' / 'integration' / 'resources' / 'plastic_detect_changes'
@@ -70,6 +99,10 @@ def main(root: str) -> None:
     for inc in (0, 75, 150):
         for name in ('xi_sl', 'gamma_sl'):
             out[f'{name}_{inc}'] = f.read(f'increment_{inc}/phase/phenopowerlawbcc/mechanical/{name}')
+    for inc in (75, 150):
+        for name in ('u_p', 'u_n'):
+            out[f'{name}_{inc}'] = f.read(f'increment_{inc}/geometry/{name}')
+    out['layout_json'] = json.dumps(layout(f, 'phenopowerlawbcc'))
     np.savez_compressed(HERE / 'golden_17grains_bcc.npz', **out)
     print('wrote', HERE / 'golden_17grains_bcc.npz', sorted(out))
 

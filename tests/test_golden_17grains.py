@@ -16,8 +16,10 @@ import numpy as np
 import pytest
 import yaml
 
-from damask_b200 import config, vti
+from damask_b200 import config, dadf5, vti
 from damask_b200.grid import run_load_cases
+
+from golden.dadf5 import DADF5
 
 GOLD = Path(__file__).resolve().parent / 'golden' / 'golden_17grains_bcc.npz'
 
@@ -96,19 +98,96 @@ def test_inputs_parse(gold):
     assert np.allclose(gold['xi_sl_0'], 405.8e6) and not gold['gamma_sl_0'].any()
 
 
-def test_oracle_reproduces_reference_result(gold, oracle_lib):
-    """The oracle over all 150 increments against the reference's stored result."""
+@pytest.fixture(scope='module')
+def oracle_run(gold, oracle_lib, tmp_path_factory):
+    """The oracle over all 150 increments, writing its result file like the reference job
+    (outputs xi_sl and gamma_sl of the phase, increments 0, 75, 150)."""
     cells, size, mat, q, phase, num, lcs = inputs(gold)
     o = oracle_lib.OracleSpectralBasic(cells, size, mat, q, phase, num)
-    out, stats = run(o, lcs)
+    path = tmp_path_factory.mktemp('dadf5') / '17grains_tensionX.hdf5'
+    rf = dadf5.ResultFile(path, cells, size, 'phenopowerlawbcc', 'cI', 'SX',
+                          setup_files={n: ('', 'input file') for n in ('17grains.vti', 'material.yaml',
+                                                                      'numerics.yaml', 'tensionX.yaml')})
+    systems = dadf5.phase_systems(phase)
+    outputs = ('xi_sl', 'gamma_sl')
+    dadf5.write_increment(rf, o, 0, 0.0, outputs, (), systems)
+    out = {}
+
+    def cb(rec):
+        if rec.converged and rec.inc % lcs[0].f_out == 0:
+            out[rec.inc] = (o.get_field('xi_sl').copy(), o.get_field('gamma_sl').copy(), o.get_coords())
+            dadf5.write_increment(rf, o, rec.inc, rec.t, outputs, (), systems)
+
+    stats = run_load_cases(o, lcs, on_increment=cb)
+    rf.close()
     o.close()
+    return out, stats, path
+
+
+def test_oracle_reproduces_reference_result(gold, oracle_run):
+    """The oracle over all 150 increments against the reference's stored result."""
+    out, stats, _ = oracle_run
     assert all(s.converged for s in stats) and len(stats) == 150
     for inc in (75, 150):
-        xi, ga = out[inc]
+        xi, ga, _ = out[inc]
         assert within_reference_tolerance(xi, gold[f'xi_sl_{inc}']).all()
         assert within_reference_tolerance(ga, gold[f'gamma_sl_{inc}']).all()
         # much closer than the tolerance in the hardening variable
         assert np.abs(xi / gold[f'xi_sl_{inc}'] - 1).max() < 1e-3
+
+
+def _tree(f: DADF5, path=''):
+    out = {}
+    for k in f.keys(path):
+        p = f'{path}/{k}'.strip('/')
+        try:
+            out[k] = {'groups': _tree(f, p), 'attrs': f.attrs(p)}
+        except KeyError:
+            d = f.read(p)
+            out[k] = {'shape': list(d.shape), 'dtype': str(d.dtype) if not d.dtype.names else list(d.dtype.names),
+                      'attrs': f.attrs(p), 'data': d}
+    return out
+
+
+def _contains(mine: dict, ref: dict, where=''):
+    """Every group, dataset (shape, dtype) and attribute of ref is in mine."""
+    for k, r in ref.items():
+        assert k in mine, f'{where}/{k} missing'
+        m = mine[k]
+        for name, v in r['attrs'].items():
+            assert name in m['attrs'], f'{where}/{k}@{name} missing'
+            if name == 't/s':
+                assert abs(m['attrs'][name] - v) <= 1e-12 * max(1.0, abs(v))
+            elif where.strip('/') != 'setup':
+                assert np.array_equal(np.asarray(m['attrs'][name]), np.asarray(v)), f'{where}/{k}@{name}'
+        if 'groups' in r:
+            _contains(m['groups'], r['groups'], f'{where}/{k}')
+        elif where.strip('/') != 'setup':
+            assert m['shape'] == r['shape'] and m['dtype'] == r['dtype'], f'{where}/{k}'
+
+
+def test_result_file_has_reference_layout(gold, oracle_run):
+    """The DADF5 file written for the job holds every group, dataset and attribute of the
+    reference's result file (restricted to the job's phase), with the reference's descriptions,
+    units, slip-system labels and times, and its data within the reference test's tolerance."""
+    out, _, path = oracle_run
+    f = DADF5(path)
+    ref = json.loads(str(gold['layout_json']))
+    assert set(ref['root_attrs']) <= set(f.attrs())
+    assert f.attrs()['DADF5_version_major'] == 1
+    mine = _tree(f)
+    _contains(mine, ref['tree'])
+    ph = f.read('cell_to/phase')
+    assert ph.shape == (1920, 1) and (ph['entry'][:, 0] == np.arange(1920)).all()
+    assert {x.decode().strip() for x in ph['label'].ravel()} == {'phenopowerlawbcc'}
+    for inc in (75, 150):
+        g = f'increment_{inc}'
+        xi = f.read(f'{g}/phase/phenopowerlawbcc/mechanical/xi_sl')
+        assert np.array_equal(xi, out[inc][0])
+        assert within_reference_tolerance(xi, gold[f'xi_sl_{inc}']).all()
+        for name in ('u_p', 'u_n'):
+            u = f.read(f'{g}/geometry/{name}')
+            assert within_reference_tolerance(u, gold[f'{name}_{inc}']).all(), (inc, name)
 
 
 @pytest.mark.gpu
