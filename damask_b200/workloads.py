@@ -82,3 +82,47 @@ def material_yaml(rve: RVE, phase_name: str, phase: dict) -> dict:
             'material': [{'homogenization': 'direct',
                           'constituents': [{'phase': phase_name, 'v': 1.0, 'O': [float(x) for x in q]}]}
                          for q in np.asarray(rve.quaternions)]}
+
+
+def simple_shear_xy(t: float, N: int, rate: float = 1.0e-3) -> list[LoadCase]:
+    """Simple shear dot_F_xy = rate, every component deformation-controlled."""
+    return parse_load({'loadstep': [{
+        'boundary_conditions': {'mechanical': {'dot_F': [[0, rate, 0], [0, 0, 0], [0, 0, 0]]}},
+        'discretization': {'t': t, 'N': N}}]})
+
+
+def tension_along(axis, t: float, N: int) -> list[LoadCase]:
+    """Uniaxial tension along a unit axis: the x-tension load case with the load-case rotation
+    R (DAMASK_grid.f90:524) that takes x to the axis."""
+    a = np.asarray(axis, float) / np.linalg.norm(axis)
+    ang = float(np.degrees(np.arccos(np.clip(a[0], -1.0, 1.0))))
+    rot = np.cross([1.0, 0.0, 0.0], a)
+    n = np.linalg.norm(rot)
+    ax = rot / n if n > 1e-12 else np.array([0.0, 0.0, 1.0])
+    lcs = parse_load({'loadstep': [{
+        'boundary_conditions': {'mechanical': {
+            'dot_F': [[1.0e-3, 0, 0], [0, 'x', 0], [0, 0, 'x']],
+            'P': [['x', 'x', 'x'], ['x', 0, 'x'], ['x', 'x', 0]],
+            'R': [float(ax[0]), float(ax[1]), float(ax[2]), ang]}},
+        'discretization': {'t': t, 'N': N}}]})
+    return lcs
+
+
+def batched_jobs(n: int = 512, seed: int = 4, t: float = 40.0, N: int = 40):
+    """The batched workload: n independent RVEs, edge uniform in {8, 12, 16, 24, 32}, grain count
+    uniform in [5, 100], orientations uniform on SO(3), the fcc material; each RVE gets uniaxial
+    tension along a random unit axis or simple shear dot_F_xy = 1e-3/s, 40 increments to 4 %.
+    Returns [(rve, phase, loadcases, numerics)]."""
+    rng = np.random.default_rng(seed)
+    jobs = []
+    for k in range(n):
+        edge = int(rng.choice([8, 12, 16, 24, 32]))
+        grains = int(rng.integers(5, 101))
+        rve = voronoi_rve((edge, edge, edge), SIZE_1MM, grains, int(rng.integers(2 ** 31)))
+        if rng.random() < 0.5:
+            axis = rng.normal(size=3)
+            lcs = tension_along(axis / np.linalg.norm(axis), t, N)
+        else:
+            lcs = simple_shear_xy(t, N)
+        jobs.append((rve, fcc_al(), lcs, numerics_default()))
+    return jobs
