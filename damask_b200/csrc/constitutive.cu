@@ -59,7 +59,7 @@ template <int NS>
 __global__ void __launch_bounds__(PASS_THREADS, 4)
 constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
-                          int apply_update, int64_t v_begin, int64_t v_end) {
+                          int apply_update, int use_dot0, int64_t v_begin, int64_t v_end) {
   extern __shared__ double slots[];
   constexpr int NST = 2 * NS;
   double* hs = slots;
@@ -102,12 +102,29 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         const double f0 = f.F0[k * N + v];
         w.Fs[k * N + v] = fma(c.step, Fn[k] - f0, f0);
       }
-      // start of the state iteration (integrateStateFPI:614-620) at S0 and state0
-      double s6[6];
+      // start of the state iteration (integrateStateFPI:614-620) at S0 and state0.  The rate
+      // depends on the increment-start values only, so every evaluation of an increment after
+      // the first reads it back (use_dot0) instead of evaluating the kinetics and hardening.
+      bool bad = false;
+      if (use_dot0) {
+#pragma unroll 12
+        for (int i = 0; i < NST; ++i) {
+          const double d = w.dot0[i * N + v];
+          bad |= isnan(d);
+          xs[i * PASS_THREADS] = d;
+        }
+      } else {
+        double s0[6];
 #pragma unroll
-      for (int k = 0; k < 6; ++k) s6[k] = f.S0[k * N + v];
-      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state0, N, v, xs, nullptr);
+        for (int k = 0; k < 6; ++k) s0[k] = f.S0[k * N + v];
+        bad = dot_state_slots<NS>(pc, hs, s0, f.state0, N, v, xs, nullptr);
+#pragma unroll 12
+        for (int i = 0; i < NST; ++i) w.dot0[i * N + v] = xs[i * PASS_THREADS];
+      }
       if (bad) {
+        double s6[6];
+#pragma unroll
+        for (int k = 0; k < 6; ++k) s6[k] = f.S0[k * N + v];
         // STATUS_FAIL_PHASE_MECHANICAL_STATE: restore as the cutback branch does and continue
         // with the general control flow
 #pragma unroll
@@ -228,15 +245,16 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
 
 template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                      const PassWork& w, double dt, int apply_update, int64_t v_begin, int64_t v_end,
-                                      cudaStream_t s) {
+                                      const PassWork& w, double dt, int apply_update, int use_dot0, int64_t v_begin,
+                                      int64_t v_end, cudaStream_t s) {
   const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
   if (v_end <= v_begin) return cudaSuccess;
   const int nb = int((v_end - v_begin + PASS_THREADS - 1) / PASS_THREADS);
-  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update, v_begin, v_end);
+  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update, use_dot0, v_begin,
+                                                                v_end);
   return cudaGetLastError();
 }
 
@@ -258,7 +276,8 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
 
 #define DMK_INSTANTIATE(NS)                                                                                         \
   template cudaError_t launch_constitutive_begin<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,          \
-                                                     const PassWork&, double, int, int64_t, int64_t, cudaStream_t); \
+                                                     const PassWork&, double, int, int, int64_t, int64_t,          \
+                                                     cudaStream_t);                                                 \
   template cudaError_t launch_constitutive_pass<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,           \
                                                     const PassWork&, double, const int*, int64_t, cudaStream_t);
 DMK_INSTANTIATE(12)

@@ -126,6 +126,8 @@ struct dmk_ctx {
   // constitutive pass scheme: per-voxel iteration state, voxel lists, pass counts
   double* pw = nullptr;          // Fs F0s Fp0s Lp0s (9 each), st0s dot last1 (2 NS each), stepFrac, step
   int* pctl = nullptr;           // 6 planes of per-voxel control integers
+  double* dot0 = nullptr;        // 2 NS planes: dotState at (S0, state0), see dot0_valid
+  bool dot0_valid = false;       // dot0 holds the rates of the current increment-start values
   // The voxels are split into PASS_CHUNKS chunks whose pass loops run on their own streams,
   // so that the latency-bound control kernel of one chunk overlaps the compute-bound stress
   // kernel of another.  Per chunk: two voxel lists alternating between passes, their counts.
@@ -162,6 +164,7 @@ PassWork pass_work(dmk_ctx* c, int half, int out) {
   w.st0s = w.Lp0s + 9 * N;
   w.D = w.st0s + NST * N;
   w.adg = w.D + 2 * NST * N;
+  w.dot0 = c->dot0;
   w.sub = w.adg + int64_t(c->NS) * N;
   w.ctl = c->pctl;
   w.list_out = c->plist[half][out];
@@ -187,11 +190,13 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
     // pass 0: restore and control up to the first integrateStress of every voxel of the chunk
     cur[h] = 0;
     CK(cudaMemsetAsync(c->pcount + 2 * h, 0, 2 * sizeof(int), c->cstream[h]));
-    CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, h, 0), dt, apply, lo[h], hi[h], c->cstream[h]));
+    CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, h, 0), dt, apply, c->dot0_valid ? 1 : 0, lo[h], hi[h],
+                                      c->cstream[h]));
     CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
     ++c->passes;
     active[h] = hi[h] > lo[h];
   }
+  c->dot0_valid = true;   // the begin kernels above stored (or read) the increment-start rates
   // each chunk advances as soon as its previous pass has ended, so the chunks pipeline
   for (int pass = 1;;) {
     bool any = false;
@@ -899,6 +904,7 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
       (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)) ||
       (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 6 * size_t(N))) ||
+      (rc = dalloc(&c->dot0, size_t(NST) * N)) ||
       (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)) || (rc = dalloc(&c->xp, 3 * size_t(N))) ||
       (rc = dalloc(&c->xn, 3 * size_t(node_count(c)))) || (rc = dalloc(&c->favg, 9)))
     return bail(rc);
@@ -1191,6 +1197,7 @@ int dmk_materialpoint_forward(dmk_ctx* c) {
   CK(cudaMemcpyAsync(c->Lp0, c->Lp, b9, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->S0, c->S, b6, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->state0, c->state, bs, cudaMemcpyDeviceToDevice, c->stream));
+  c->dot0_valid = false;                                   // new increment-start values
   CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
@@ -1236,6 +1243,7 @@ int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
   CK(cudaMemcpyAsync(c->Lp, c->Lp0, b9, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->state, c->state0, bs, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemsetAsync(c->S0, 0, sizeof(double) * 6 * c->N, c->stream));
+  c->dot0_valid = false;
   CK(cudaMemsetAsync(c->S, 0, sizeof(double) * 6 * c->N, c->stream));
   // solver module state (grid_mech_spectral_basic.f90:203-208)
   std::memcpy(c->P_aim, r->P_aim, sizeof c->P_aim);
@@ -1538,7 +1546,7 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->tan.partials, (void*)c->tan.nmax, (void*)c->tan.nmin, (void*)c->tan.norms, (void*)c->tan.l2, (void*)c->tan.planes,
                   c->fft_work,
                   (void*)c->aa_dX, (void*)c->aa_dR, (void*)c->aa_Rprev, (void*)c->aa_partials, (void*)c->aa_out,
-                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->xp, (void*)c->xn, (void*)c->favg,
+                  (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->dot0, (void*)c->xp, (void*)c->xn, (void*)c->favg,
                   (void*)c->Ftau_last, (void*)c->Ftau_dot, (void*)c->Feval, (void*)c->curl_partials})
     if (p) cudaFree(p);
   for (auto& l : c->plist)

@@ -72,6 +72,7 @@ struct PassWork {
   double* st0s;    // 2 NS: subState0
   double* D;       // 2 x 2 NS: (damped) dotState of the last two state iterations
   double* adg;     // NS: |dot_gamma| at the stress of the last converged integrateStress
+  double* dot0;    // 2 NS: dotState at the increment-start stress and state (S0, state0)
   double* sub;     // 2: stepFrac (subFrac), step (subStep)
   int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
   int* list_out;   // voxels that continue into the next pass

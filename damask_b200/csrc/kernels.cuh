@@ -39,8 +39,8 @@ struct Numerics2 {
 // constitutive passes (constitutive.cu)
 template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                      const PassWork& w, double dt, int apply_update, int64_t v_begin, int64_t v_end,
-                                      cudaStream_t s);
+                                      const PassWork& w, double dt, int apply_update, int use_dot0, int64_t v_begin,
+                                      int64_t v_end, cudaStream_t s);
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
