@@ -19,7 +19,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_dPdF', 'dmk_get_iteration_counts', 'dmk_get_counters', 'dmk_get_timings', 'dmk_destroy',
            'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop', 'dmk_phase_schmid',
            'dmk_phase_interaction', 'dmk_field_mean_noalloc', 'dmk_restart_write', 'dmk_restart_read',
-           'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems']
+           'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems', 'dmk_vti_open', 'dmk_vti_geometry',
+           'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close']
 
 _lib = None
 
@@ -54,6 +55,12 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_get_coords': (C.c_int, [vp, dp, dp]),
         'dmk_curl_rms': (C.c_int, [vp, dp, dp]),
         'dmk_phase_slip_systems': (C.c_int, [C.POINTER(PhaseStruct), C.POINTER(C.c_int)]),
+        'dmk_vti_open': (C.c_int, [C.c_char_p, C.POINTER(vp)]),
+        'dmk_vti_geometry': (C.c_int, [vp, ip, dp, dp]),
+        'dmk_vti_label': (C.c_int, [vp, C.c_int, C.c_char_p, C.c_int, ip]),
+        'dmk_vti_read_int': (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int64), C.c_int64]),
+        'dmk_vti_read_real': (C.c_int, [vp, C.c_char_p, dp, C.c_int64]),
+        'dmk_vti_close': (None, [vp]),
         'dmk_get_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_set_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_field_size': (C.c_int, [vp, C.c_int]),

@@ -14,7 +14,8 @@ from pathlib import Path
 HERE = Path(__file__).resolve().parent
 CSRC = HERE / 'csrc'
 LIB = HERE / 'libdamask_b200.so'
-SOURCES = ['kernels.cu', 'constitutive.cu', 'dpdf.cu', 'polarization.cu', 'context.cu', 'noalloc.cu', 'lattice.cpp']
+SOURCES = ['kernels.cu', 'constitutive.cu', 'dpdf.cu', 'polarization.cu', 'context.cu', 'noalloc.cu', 'lattice.cpp',
+           'vti.cpp']
 HEADERS = ['dmk_device.cuh', 'constitutive.cuh', 'kernels.cuh', 'lattice.h', 'lattice_tables.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
@@ -60,7 +61,7 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         subprocess.run(cmd, check=True)
         objs.append(str(obj))
     tmp = LIB.with_suffix('.so.tmp')
-    subprocess.run([nvcc] + ARCH + _host_cxx() + ['-shared', '-o', str(tmp)] + objs + ['-lcufft', '-lcudart'], check=True)
+    subprocess.run([nvcc] + ARCH + _host_cxx() + ['-shared', '-o', str(tmp)] + objs + ['-lcufft', '-lcudart', '-lz'], check=True)
     os.replace(tmp, LIB)
     return LIB
 

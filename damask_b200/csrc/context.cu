@@ -813,6 +813,10 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
 
 }  // namespace
 
+namespace dmk {
+int record_error(int code, const std::string& msg) { return fail(code, msg); }
+}  // namespace dmk
+
 extern "C" {
 
 const char* dmk_last_error(void) { return g_err.c_str(); }

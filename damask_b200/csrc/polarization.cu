@@ -2,6 +2,7 @@
 // curl criterion (utilities_curlRMS, spectral_utilities.f90:695-757).  Fields are planes
 // (component c of voxel v at c * N + v, column-major 3x3 components); fourth-order
 // constants are column-major, index i + 3j + 9k + 27l.
+#include "constitutive.cuh"
 #include "kernels.cuh"
 
 namespace dmk {
@@ -82,8 +83,9 @@ __global__ void pol_tau_kernel(const double* __restrict__ F, double* __restrict_
 // (math_sym3333to66: pairs 11,22,33,23,13,12, w = 1 for normal and sqrt(2) for shear pairs)
 // and expands it with minor symmetry (math_66toSym3333), so the contraction with a 3x3 B is
 // out(p_r) = y_r / w_r with M y = z, z_q = (B(k,l) [+ B(l,k) for k != l]) / w_q; out symmetric.
-// The 6x6 system is solved by LU with partial pivoting.  Only the 36 dPdF planes of the
-// Mandel pairs are read.
+// The 6x6 system is solved by Householder QR with compile-time indices (registers only); a
+// singular matrix gives NaN, as the reference's inversion error would stop.  Only the 36 dPdF
+// planes of the Mandel pairs are read.
 __global__ void __launch_bounds__(128)
 pol_rF_kernel(const double* __restrict__ F, const double* __restrict__ Ftau, const double* __restrict__ P,
               const double* __restrict__ dPdF, const double* __restrict__ rtau, int64_t N,
@@ -98,50 +100,20 @@ pol_rF_kernel(const double* __restrict__ F, const double* __restrict__ Ftau, con
   polarization_term(pc.C, f, ft, b);
 #pragma unroll
   for (int k = 0; k < 9; ++k) b[k] = P[k * N + v] - b[k];
-  double M[6][6], z[6];
+  double M[36], z[6];
 #pragma unroll
   for (int r = 0; r < 6; ++r)
 #pragma unroll
     for (int q = 0; q < 6; ++q) {
       const int c = pi[r] + 3 * pj[r] + 9 * pi[q] + 27 * pj[q];
-      M[r][q] = (dPdF[int64_t(c) * N + v] + pc.C[c]) * (r < 3 ? 1.0 : SQ2) * (q < 3 ? 1.0 : SQ2);
+      M[6 * r + q] = (dPdF[int64_t(c) * N + v] + pc.C[c]) * (r < 3 ? 1.0 : SQ2) * (q < 3 ? 1.0 : SQ2);
     }
 #pragma unroll
   for (int q = 0; q < 6; ++q)
     z[q] = q < 3 ? b[pi[q] + 3 * pj[q]] : (b[pi[q] + 3 * pj[q]] + b[pj[q] + 3 * pi[q]]) / SQ2;
-  // LU with partial pivoting (row interchanges applied to z as they happen)
+  if (qr_solve<6>(M, z))
 #pragma unroll
-  for (int j = 0; j < 6; ++j) {
-    int p = j;
-    double amax = fabs(M[j][j]);
-#pragma unroll
-    for (int i = j + 1; i < 6; ++i)
-      if (fabs(M[i][j]) > amax) { amax = fabs(M[i][j]); p = i; }
-    if (p != j) {
-#pragma unroll
-      for (int i = j + 1; i < 6; ++i)
-        if (i == p) {
-#pragma unroll
-          for (int k = 0; k < 6; ++k) { const double t = M[j][k]; M[j][k] = M[i][k]; M[i][k] = t; }
-          const double t = z[j]; z[j] = z[i]; z[i] = t;
-        }
-    }
-    const double rp = 1.0 / M[j][j];
-#pragma unroll
-    for (int i = j + 1; i < 6; ++i) {
-      const double l = M[i][j] * rp;
-#pragma unroll
-      for (int k = j + 1; k < 6; ++k) M[i][k] = fma(-l, M[j][k], M[i][k]);
-      z[i] = fma(-l, z[j], z[i]);
-    }
-  }
-#pragma unroll
-  for (int i = 5; i >= 0; --i) {
-    double s = z[i];
-#pragma unroll
-    for (int k = i + 1; k < 6; ++k) s = fma(-M[i][k], z[k], s);
-    z[i] = s / M[i][i];
-  }
+    for (int q = 0; q < 6; ++q) z[q] = __longlong_as_double(0x7ff8000000000000LL);
   double out[9];
 #pragma unroll
   for (int r = 0; r < 6; ++r) {

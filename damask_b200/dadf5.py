@@ -178,7 +178,7 @@ class H5Writer:
     def close(self) -> None:
         strings: list[bytes] = []                             # global heap objects (vlen strings)
 
-        def attr_message(name: str, value, refs: list) -> bytes:
+        def attr_message(name: str, value, refs: list) -> tuple[bytes, bytes]:
             if isinstance(value, str) or (isinstance(value, (list, tuple)) and value and isinstance(value[0], str)):
                 vals = [value] if isinstance(value, str) else list(value)
                 shape = () if isinstance(value, str) else (len(vals),)

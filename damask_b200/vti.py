@@ -81,6 +81,43 @@ def _decode(text: str, compressed: bool, word: int) -> bytes:
     return b''.join(out)
 
 
+def load_native(path, int_labels=('material',)) -> Geometry:
+    """The same file through the library's C++ reader (dmk_vti_*, the counterpart of the
+    reference's src/grid/VTI.cpp): arrays named in int_labels come back as int64, the others
+    as float64."""
+    import ctypes as C
+    from . import _lib
+    lib = _lib.load()
+    h = C.c_void_p()
+    rc = lib.dmk_vti_open(str(path).encode(), C.byref(h))
+    if rc != 0:
+        raise VTIError(lib.dmk_last_error().decode())
+    try:
+        cells = (C.c_int * 3)()
+        size, origin = (C.c_double * 3)(), (C.c_double * 3)()
+        lib.dmk_vti_geometry(h, cells, size, origin)
+        geom = Geometry(tuple(cells), tuple(size), tuple(origin))
+        buf = C.create_string_buffer(256)
+        ncomp = C.c_int()
+        n = lib.dmk_vti_label(h, 0, buf, 256, C.byref(ncomp))
+        N = int(np.prod(geom.cells))
+        for i in range(n):
+            lib.dmk_vti_label(h, i, buf, 256, C.byref(ncomp))
+            name, k = buf.value.decode(), ncomp.value
+            if name in int_labels:
+                out = np.empty(N * k, np.int64)
+                rc = lib.dmk_vti_read_int(h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_int64)), out.size)
+            else:
+                out = np.empty(N * k, np.float64)
+                rc = lib.dmk_vti_read_real(h, name.encode(), out.ctypes.data_as(C.POINTER(C.c_double)), out.size)
+            if rc != 0:
+                raise VTIError(lib.dmk_last_error().decode())
+            geom.cell_data[name] = out.reshape(N, k) if k > 1 else out
+        return geom
+    finally:
+        lib.dmk_vti_close(h)
+
+
 def load(path) -> Geometry:
     root = ET.parse(path).getroot()
     if root.tag != 'VTKFile':

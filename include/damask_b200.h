@@ -253,6 +253,20 @@ int dmk_phase_interaction(const dmk_phase* phase, double* h);
    labels of slip outputs (crystal_labels_slip, crystal.f90:1642-1676).  Returns Ns. */
 int dmk_phase_slip_systems(const dmk_phase* phase, int* out);
 
+/* Grid geometry files (.vti): the native reader that replaces the reference's C++ reader
+   (src/grid/VTI.cpp:417-445: C_VTI_new, C_VTI_readGeometry, C_VTI_readDatasetInt,
+   C_VTI_readDatasetReal, C_VTI_delete; descriptors there, pointers and sizes here).  Host code
+   only (no device needed).  Labels are the CellData array names in file order; the datasets
+   have cells1*cells2*cells3*NumberOfComponents values, x fastest. */
+typedef struct dmk_vti dmk_vti;
+int dmk_vti_open(const char* path, dmk_vti** out);
+int dmk_vti_geometry(const dmk_vti* vti, int cells[3], double size[3], double origin[3]);
+/* name (and NumberOfComponents) of label `index`; returns the label count */
+int dmk_vti_label(const dmk_vti* vti, int index, char* out, int cap, int* components);
+int dmk_vti_read_int(const dmk_vti* vti, const char* label, int64_t* out, int64_t n);
+int dmk_vti_read_real(const dmk_vti* vti, const char* label, double* out, int64_t n);
+void dmk_vti_close(dmk_vti* vti);
+
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 /* Device timer on the context's stream: CUDA events recorded at start and stop;
