@@ -174,9 +174,12 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     from damask_b200 import workloads
     from damask_b200.grid import IncrementDriver, SpectralBasic
 
+    import torch
     rve, phase, lcs, num = workloads.make(WORKLOAD, cells)
+    free0 = torch.cuda.mem_get_info(local)[0]
     solver = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision,
                            device=local)
+    device_gb = (free0 - torch.cuda.mem_get_info(local)[0]) / 1e9
     drv = IncrementDriver(solver, lcs)
     p_av = []
 
@@ -213,7 +216,6 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     barrier(world)
     # end to end through the public API: per step the BCs go in from host memory
     # and the stress field P comes back into pinned host memory
-    import torch
     pinned = torch.empty((solver.N, 9), dtype=torch.float64, pin_memory=True).numpy()
     barrier(world)
     solver.timer_start()
@@ -225,7 +227,7 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     barrier(world)
     out = {'updates': upd, 'ms': ms, 'newton': newton, 'state': state, 'evals': evals, 'const_ms': const_ms,
            'launches': launches, 'clocks': clk, 'updates_e2e': upd_e2e, 'ms_e2e': ms_e2e, 'N': solver.N,
-           'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8}
+           'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8, 'device_gb': device_gb}
     solver.close()
     return out
 
@@ -373,7 +375,7 @@ def main():
                                'tension dot_F_xx 1e-3/s, 100 increments to 10 %' if cells is None else
                                f'{WORKLOAD} at {cells}',
                    'solver': 'basic spectral, Anderson fixed point (m=8)', 'precision': 'mixed',
-                   'parallelism': f'replicas x{world}', 'l2': 'inputs larger than L2 (per-voxel state ~30 GB)',
+                   'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
                    'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
         'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
         'mixed_over_fp64': value / fp_value,
