@@ -48,7 +48,7 @@ def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> 
 # DRAM bytes that the constitutive kernels move per material-point update, from the ncu
 # capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (64^3 cut of this
 # workload; the traffic grows with the number of voxels)
-TRAFFIC_BYTES_PER_UPDATE = 8434
+TRAFFIC_BYTES_PER_UPDATE = 9428
 
 
 def bc_bytes() -> int:

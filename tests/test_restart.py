@@ -1,5 +1,6 @@
-"""Restart (grid_mech_spectral_basic.f90:198-235,378-416; phase_mechanical.f90:1248-1280):
-a run resumed from the restart data of increment k continues like the uninterrupted run."""
+"""Restart (grid_mech_spectral_basic.f90:198-235,378-416; grid_mech_spectral_polarization.f90:
+236-268,400-438; phase_mechanical.f90:1248-1280): a run resumed from the restart data of
+increment k continues like the uninterrupted run, for both solvers."""
 import numpy as np
 import pytest
 
@@ -9,9 +10,12 @@ from damask_b200.grid import IncrementDriver, SpectralBasic, load_restart, save_
 pytestmark = pytest.mark.gpu
 
 
-def test_restart_resumes_the_run(gpu, tmp_path):
+@pytest.mark.parametrize('solver', ['spectral_basic', 'spectral_polarization'])
+def test_restart_resumes_the_run(gpu, tmp_path, solver):
     rve = synthetic.voronoi_rve((8, 8, 8), workloads.SIZE_1MM, 6, 1)
-    args = (rve.cells, rve.size, rve.material, rve.quaternions, workloads.fcc_al(), workloads.numerics_default())
+    num = workloads.numerics_default()
+    num.solver = solver
+    args = (rve.cells, rve.size, rve.material, rve.quaternions, workloads.fcc_al(), num)
     lcs = workloads.tension_x(60.0, 60)
     a = SpectralBasic(*args)
     drv = IncrementDriver(a, lcs)
