@@ -199,7 +199,10 @@ gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2,
         s = fma(vr, vr, s);
         s = fma(vi, vi, s);
       }
-      const double weight = (kx >= 1 && kx < red0 - 1) ? 2.0 : 1.0;
+      // interior planes count twice (their conjugates are not stored); the planes kx = 0 and
+      // kx = cells1Red - 1 once each, so a single stored plane (cells(1) = 1) counts twice
+      // (spectral_utilities.f90:667-684; the result is halved for cells(1) = 1)
+      const double weight = ((kx >= 1 && kx < red0 - 1) || red0 == 1) ? 2.0 : 1.0;
       dsum = weight * s;
     }
     if (do_gamma) {

@@ -180,3 +180,22 @@ def test_update_coords_random_field(gpu, oracle_lib, cells):
     for a, b in zip(g.get_coords(), o.get_coords()):
         assert rel(a, b) < 1e-12
     g.close()
+
+
+@pytest.mark.parametrize('cells', [(16, 16, 1), (1, 16, 16), (16, 1, 16)])
+@pytest.mark.parametrize('solver', ['spectral_basic', 'spectral_polarization'])
+def test_quasi_2d_grids(gpu, oracle_lib, cells, solver):
+    """One-cell-thick grids (the reference halves the divergence and curl sums for cells(1) = 1)."""
+    num = workloads.numerics_default()
+    num.solver = solver
+    g, o = pair(oracle_lib, cells, 8, seed=2, num=num)
+    sg, so = run_both(g, o, 3)
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    assert all(s.converged for s in sg)
+    for a, b in zip(sg, so):
+        assert rel(a.P_av, b.P_av) < TOL
+    for name in ('P', 'F', 'F_p', 'xi_sl', 'gamma_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    for a, b in zip(g.get_coords(), o.get_coords()):
+        assert rel(a, b) < TOL
+    g.close()
