@@ -199,3 +199,34 @@ def test_quasi_2d_grids(gpu, oracle_lib, cells, solver):
     for a, b in zip(g.get_coords(), o.get_coords()):
         assert rel(a, b) < TOL
     g.close()
+
+
+LOADS = {
+    'simple_shear': {'dot_F': [[0, 1.0e-3, 0], [0, 0, 0], [0, 0, 0]]},
+    'L_tension': {'L': [[1.0e-3, 0, 0], [0, 'x', 0], [0, 0, 'x']], 'P': [['x', 'x', 'x'], ['x', 0, 'x'], ['x', 'x', 0]]},
+    'F_target': {'F': [[1.02, 0, 0], [0, 'x', 0], [0, 0, 'x']], 'P': [['x', 'x', 'x'], ['x', 0, 'x'], ['x', 'x', 0]]},
+    'dot_P_xx': {'dot_F': [['x', 0, 0], [0, 0, 0], [0, 0, 0]], 'dot_P': [[2.0e6, 'x', 'x'], ['x', 'x', 'x'], ['x', 'x', 'x']]},
+    'rotated_tension': {'dot_F': [[1.0e-3, 0, 0], [0, 'x', 0], [0, 0, 'x']],
+                        'P': [['x', 'x', 'x'], ['x', 0, 'x'], ['x', 'x', 0]], 'R': [0.0, 0.6, 0.8, 35.0]},
+}
+
+
+@pytest.mark.parametrize('load', sorted(LOADS))
+def test_boundary_condition_types(gpu, oracle_lib, load):
+    """Deformation BCs L / dot_F / F, stress BCs P / dot_P and the load-case rotation R
+    (DAMASK_grid.f90:472-689; forward grid_mech_spectral_basic.f90:284-355)."""
+    from damask_b200.config import parse_load
+    lcs = parse_load({'loadstep': [{'boundary_conditions': {'mechanical': LOADS[load]},
+                                    'discretization': {'t': 10.0, 'N': 10}}]})
+    g, o = pair(oracle_lib, (8, 8, 8), 5, seed=4)
+    sg = run_load_cases(g, lcs, max_increments=3)
+    so = run_load_cases(o, lcs, max_increments=3)
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    assert all(s.converged for s in sg)
+    for a, b in zip(sg, so):
+        assert rel(a.P_av, b.P_av) < TOL
+    for name in ('P', 'F', 'xi_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    for k in ('F_aim', 'P_aim'):
+        assert rel(g.aims()[k], o.aims()[k]) < TOL, k
+    g.close()
