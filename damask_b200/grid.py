@@ -16,6 +16,7 @@ import copy
 import ctypes as C
 import time
 from dataclasses import dataclass, field
+from pathlib import Path
 
 import numpy as np
 
@@ -375,15 +376,49 @@ class IncrementDriver:
         return out
 
 
+STA_HEADER = 'Increment Time CutbackLevel Converged IterationsNeeded StagIterationsNeeded'
+
+
+def sta_line(rec: IncrementStats) -> str:
+    """One row of the job's .sta file per converged (sub)increment (DAMASK_grid.f90:394-395):
+    total increment, time, cutback level, converged, iterations, staggered iterations (0 with
+    the mechanical field alone)."""
+    return f'{rec.inc:12d} {rec.t:24.16e} {rec.cutback_level:12d} {"T" if rec.converged else "F":>2} ' \
+           f'{rec.iterations:12d} {0:12d}'
+
+
 def run_load_cases(solver, loadcases: list[LoadCase], N_cutback_max: int = 3, max_increments: int | None = None,
-                   on_increment=None, sync=None, restart_inc: int = 0) -> list[IncrementStats]:
+                   on_increment=None, sync=None, restart_inc: int = 0, sta=None) -> list[IncrementStats]:
     """Run the whole load-case list (or its first ``max_increments`` increments); after a
-    restart, ``restart_inc`` increments are skipped (only the time advances)."""
+    restart, ``restart_inc`` increments are skipped (only the time advances).  With ``sta`` (a
+    path) the statistics table of DAMASK_grid.f90:268-278 is written (appended after a restart)."""
     drv = IncrementDriver(solver, loadcases, N_cutback_max, sync, restart_inc)
     stats: list[IncrementStats] = []
-    while not drv.done and (max_increments is None or drv.total < max_increments):
-        for rec in drv.step():
-            stats.append(rec)
-            if on_increment is not None:
-                on_increment(rec)
+    fh = None
+    if sta is not None:
+        exists = Path(sta).exists()
+        fh = open(sta, 'a' if (restart_inc and exists) else 'w')
+        if not (restart_inc and exists):
+            fh.write(STA_HEADER + '\n')
+    try:
+        while not drv.done and (max_increments is None or drv.total < max_increments):
+            for rec in drv.step():
+                stats.append(rec)
+                if fh is not None:
+                    fh.write(sta_line(rec) + '\n')
+                    fh.flush()
+                if on_increment is not None:
+                    on_increment(rec)
+    finally:
+        if fh is not None:
+            fh.close()
     return stats
+
+
+def read_sta(path) -> list[tuple]:
+    """Rows of a .sta file: (increment, time, cutback level, converged, iterations, staggered)."""
+    rows = []
+    for line in Path(path).read_text().splitlines()[1:]:
+        p = line.split()
+        rows.append((int(p[0]), float(p[1]), int(p[2]), p[3] == 'T', int(p[4]), int(p[5])))
+    return rows

@@ -230,3 +230,39 @@ def test_boundary_condition_types(gpu, oracle_lib, load):
     for k in ('F_aim', 'P_aim'):
         assert rel(g.aims()[k], o.aims()[k]) < TOL, k
     g.close()
+
+
+def test_displacements_of_the_converged_field(gpu, oracle_lib):
+    """After the reference's tests/integration/test_grid_displacements.py: at the end of a two-step
+    load (tension, then shear) on a random two-orientation grid, the cell-centre displacements the
+    solver reports equal the displacement field of its converged F (computed here by the oracle's
+    restatement of utilities_updateCoords, which matches the reference's
+    damask.grid.displacement_point)."""
+    from damask_b200.config import parse_load
+    from damask_b200.grid import displacements
+    rng = np.random.default_rng(8)
+    cells = tuple(int(c) for c in rng.integers(5, 12, 3))
+    size = tuple(float(x) for x in rng.random(3) + 1.0)
+    mat = rng.integers(0, 2, int(np.prod(cells))).astype(np.int32)
+    q = np.array([[1.0, 0, 0, 0], [0.0, 0.6, 0.8, 0.0]])
+    lcs = parse_load({'loadstep': [
+        {'boundary_conditions': {'mechanical': {'dot_F': [[1.0e-3, 0, 0], [0, 'x', 0], [0, 0, 'x']],
+                                                'P': [['x', 'x', 'x'], ['x', 0, 'x'], ['x', 'x', 0]]}},
+         'discretization': {'t': 10, 'N': 40}, 'f_out': 4},
+        {'boundary_conditions': {'mechanical': {'dot_F': [[0, 0, 0], [1.0e-3, 0, 0], [0, 0, 0]]}},
+         'discretization': {'t': 40, 'N': 80}, 'f_out': 20}]})
+    g = SpectralBasic(cells, size, mat, q, workloads.fcc_al(), workloads.numerics_default())
+    stats = run_load_cases(g, lcs)
+    assert len(stats) >= 120 and all(s.converged for s in stats)
+    ip, nodes = g.get_coords()
+    F = g.get_field('F')
+    g.close()
+    o = oracle_lib.OracleSpectralBasic(cells, size, mat, q, workloads.fcc_al(), init=False, threads=1)
+    o.set_field('F_solver', F)
+    o.update_coords()
+    ip_o, nodes_o = o.get_coords()
+    o.close()
+    u_p, _ = displacements(cells, size, ip, nodes)
+    u_o, _ = displacements(cells, size, ip_o, nodes_o)
+    assert np.allclose(u_p, u_o, rtol=1e-5, atol=1e-8)
+    assert rel(ip, ip_o) < 1e-12 and rel(nodes, nodes_o) < 1e-12

@@ -214,3 +214,21 @@ def test_plugin_object_interface():
         assert not missing, (cls.__name__, missing)
     for m in ('restart_write', 'restart_read', 'timer_start', 'timer_stop', 'launches', 'iteration_counts'):
         assert callable(getattr(SpectralBasic, m, None)), m
+
+
+def test_sta_file(oracle_lib, tmp_path):
+    """The statistics table of the driver (DAMASK_grid.f90:268-278, 394-395): header, one row per
+    converged increment, appended after a restart."""
+    from damask_b200 import synthetic, workloads
+    from damask_b200.grid import STA_HEADER, read_sta, run_load_cases
+    rve = synthetic.voronoi_rve((4, 4, 4), workloads.SIZE_1MM, 3, 0)
+    o = oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, workloads.fcc_al(),
+                                       workloads.numerics_default(), threads=1)
+    sta = tmp_path / 'job.sta'
+    stats = run_load_cases(o, workloads.tension_x(60.0, 60), max_increments=3, sta=sta)
+    o.close()
+    assert sta.read_text().splitlines()[0] == STA_HEADER
+    rows = read_sta(sta)
+    assert [r[0] for r in rows] == [s.inc for s in stats] == [1, 2, 3]
+    assert [r[4] for r in rows] == [s.iterations for s in stats] and all(r[3] for r in rows)
+    assert abs(rows[-1][1] - 3.0) < 1e-12
