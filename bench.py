@@ -312,7 +312,7 @@ def main():
     ap.add_argument('--batch', type=int, default=0,
                     help='measure the batched workload instead: this many independent RVEs (512 in the '
                          'workload definition), one JSON line of its own')
-    ap.add_argument('--batch-threads', type=int, default=16)
+    ap.add_argument('--batch-threads', type=int, default=48)
     args = ap.parse_args()
     if args.batch:
         return run_batch(args)

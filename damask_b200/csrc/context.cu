@@ -134,6 +134,7 @@ struct dmk_ctx {
   cudaStream_t cstream[PASS_CHUNKS] = {};   // [0] is `stream`
   cudaEvent_t fork = nullptr, join[PASS_CHUNKS] = {};
   int* plist[PASS_CHUNKS][2] = {};
+  int nchunks = PASS_CHUNKS;     // chunks in use: fewer for small RVEs (one host sync per chunk and pass)
   int* pcount = nullptr;         // [2 h + k]: entries appended to plist[h][k]
   int* hcount = nullptr;         // pinned host copies of the current counts of the chunks
   int64_t passes = 0;            // constitutive passes launched (all evaluations)
@@ -175,8 +176,8 @@ size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 7 *
 
 template <int NS>
 int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, double dt, int apply) {
-  constexpr int K = PASS_CHUNKS;
-  int64_t lo[K], hi[K];
+  const int K = c->nchunks;
+  int64_t lo[PASS_CHUNKS], hi[PASS_CHUNKS];
   for (int h = 0; h < K; ++h) {
     lo[h] = c->N * h / K;
     hi[h] = c->N * (h + 1) / K;
@@ -184,8 +185,8 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
   // the other streams start after everything queued on the first
   CK(cudaEventRecord(c->fork, c->stream));
   for (int h = 1; h < K; ++h) CK(cudaStreamWaitEvent(c->cstream[h], c->fork, 0));
-  int cur[K];
-  bool active[K];
+  int cur[PASS_CHUNKS];
+  bool active[PASS_CHUNKS];
   for (int h = 0; h < K; ++h) {
     // pass 0: restore and control up to the first integrateStress of every voxel of the chunk
     cur[h] = 0;
@@ -912,8 +913,10 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)) || (rc = dalloc(&c->xp, 3 * size_t(N))) ||
       (rc = dalloc(&c->xn, 3 * size_t(node_count(c)))) || (rc = dalloc(&c->favg, 9)))
     return bail(rc);
-  for (int h = 0; h < PASS_CHUNKS; ++h) {
-    const size_t len = size_t(N * (h + 1) / PASS_CHUNKS - N * h / PASS_CHUNKS);
+  // a chunk of at least 65536 voxels keeps a pass kernel wide enough to be worth its own stream
+  c->nchunks = int(std::max<int64_t>(1, std::min<int64_t>(PASS_CHUNKS, N / 65536)));
+  for (int h = 0; h < c->nchunks; ++h) {
+    const size_t len = size_t(N * (h + 1) / c->nchunks - N * h / c->nchunks);
     if ((rc = dalloc(&c->plist[h][0], len)) || (rc = dalloc(&c->plist[h][1], len))) return bail(rc);
   }
   if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), PASS_CHUNKS * sizeof(int)) != cudaSuccess) {
