@@ -15,6 +15,7 @@
 #include <cstring>
 #include <fstream>
 #include <map>
+#include <stdexcept>
 #include <sstream>
 #include <string>
 #include <vector>
@@ -282,7 +283,14 @@ int dmk_vti_open(const char* path, dmk_vti** out) {
   ss << in.rdbuf();
   auto* v = new dmk_vti();
   std::string err;
-  if (parse(ss.str(), *v, err)) {
+  int rc;
+  try {                                            // nothing is thrown across the C-ABI
+    rc = parse(ss.str(), *v, err);
+  } catch (const std::exception& e) {
+    rc = -1;
+    err = std::string("invalid VTI: ") + e.what();
+  }
+  if (rc) {
     delete v;
     return dmk::record_error(DMK_ERR_CONFIG, err);
   }
@@ -317,8 +325,12 @@ int dmk_vti_read_int(const dmk_vti* v, const char* label, int64_t* out, int64_t 
   if (n != cell_count(v) * it->second.components) return dmk::record_error(DMK_ERR_ARG, "output size does not match the cells");
   std::vector<uint8_t> b;
   std::string err;
-  if (decode(*v, it->second.text, b, err) || convert<int64_t>(it->second, b, out, n, err))
-    return dmk::record_error(DMK_ERR_CONFIG, err);
+  try {
+    if (decode(*v, it->second.text, b, err) || convert<int64_t>(it->second, b, out, n, err))
+      return dmk::record_error(DMK_ERR_CONFIG, err);
+  } catch (const std::exception& e) {
+    return dmk::record_error(DMK_ERR_CONFIG, std::string("invalid VTI data: ") + e.what());
+  }
   return 0;
 }
 
@@ -329,8 +341,12 @@ int dmk_vti_read_real(const dmk_vti* v, const char* label, double* out, int64_t 
   if (n != cell_count(v) * it->second.components) return dmk::record_error(DMK_ERR_ARG, "output size does not match the cells");
   std::vector<uint8_t> b;
   std::string err;
-  if (decode(*v, it->second.text, b, err) || convert<double>(it->second, b, out, n, err))
-    return dmk::record_error(DMK_ERR_CONFIG, err);
+  try {
+    if (decode(*v, it->second.text, b, err) || convert<double>(it->second, b, out, n, err))
+      return dmk::record_error(DMK_ERR_CONFIG, err);
+  } catch (const std::exception& e) {
+    return dmk::record_error(DMK_ERR_CONFIG, std::string("invalid VTI data: ") + e.what());
+  }
   return 0;
 }
 

@@ -150,6 +150,13 @@ class H5Writer:
                 raise KeyError(f'{path} is not a group')
         return g
 
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        if not self.fh.closed:
+            self.close()
+
     def group(self, path: str) -> _Group:
         return self._node(path)
 
@@ -486,6 +493,13 @@ class ResultFile:
 
     def close(self) -> None:
         self.w.close()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        if not self.w.fh.closed:
+            self.close()
 
 
 def phase_systems(phase) -> list[str]:

@@ -72,3 +72,11 @@ def test_native_errors(tmp_path):
         vti.load_native(p)
     with pytest.raises(vti.VTIError, match='cannot open'):
         vti.load_native(tmp_path / 'missing.vti')
+
+
+def test_native_rejects_malformed_attributes(tmp_path):
+    """Malformed numbers in the XML come back as errors, not as exceptions across the C-ABI."""
+    p = vti_file(tmp_path / 'g.vti', (2, 1, 1), [('material', 'Int64', 1, encode(np.zeros(2, '<i8').tobytes(), 4, False))])
+    p.write_text(p.read_text().replace('Name="material"', 'Name="material" NumberOfComponents="many"'))
+    with pytest.raises(vti.VTIError, match='invalid VTI'):
+        vti.load_native(p)
