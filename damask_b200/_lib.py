@@ -9,7 +9,8 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .config import BCStruct, NumericsStruct, PhaseStruct, RestartStruct, SolutionStruct
+from .config import (INCREMENT_CB, BCStruct, GridSolverStruct, LoadStepStruct, NumericsStruct, PhaseStruct,
+                     RestartStruct, SolutionStruct)
 
 LIB_PATH = Path(__file__).resolve().parent / 'libdamask_b200.so'
 
@@ -20,7 +21,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_last_error', 'dmk_get_launches', 'dmk_timer_start', 'dmk_timer_stop', 'dmk_phase_schmid',
            'dmk_phase_interaction', 'dmk_field_mean_noalloc', 'dmk_restart_write', 'dmk_restart_read',
            'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems', 'dmk_vti_open', 'dmk_vti_geometry',
-           'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close']
+           'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
+           'dmk_grid_run_ctx']
 
 _lib = None
 
@@ -61,6 +63,10 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_vti_read_int': (C.c_int, [vp, C.c_char_p, C.POINTER(C.c_int64), C.c_int64]),
         'dmk_vti_read_real': (C.c_int, [vp, C.c_char_p, dp, C.c_int64]),
         'dmk_vti_close': (None, [vp]),
+        'dmk_grid_run': (C.c_int, [C.POINTER(GridSolverStruct), C.POINTER(LoadStepStruct), C.c_int, C.c_int, C.c_int,
+                                   C.c_int, INCREMENT_CB, C.c_void_p]),
+        'dmk_grid_run_ctx': (C.c_int, [vp, C.POINTER(LoadStepStruct), C.c_int, C.c_int, C.c_int, C.c_int,
+                                       INCREMENT_CB, C.c_void_p]),
         'dmk_get_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_set_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_field_size': (C.c_int, [vp, C.c_int]),

@@ -62,10 +62,47 @@ class RestartStruct(C.Structure):
                 ('F_tau_lastinc', C.POINTER(C.c_double))]
 
 
+class LoadStepStruct(C.Structure):
+    """dmk_loadstep (include/damask_b200.h)."""
+    _fields_ = [('deformation', BCStruct), ('stress', BCStruct), ('q_rot', C.c_double * 4), ('t', C.c_double),
+                ('N', C.c_int), ('r', C.c_double), ('f_out', C.c_int), ('f_restart', C.c_int),
+                ('estimate_rate', C.c_int)]
+
+
+class IncrementInfoStruct(C.Structure):
+    """dmk_increment_info (include/damask_b200.h)."""
+    _fields_ = [('inc', C.c_int), ('t', C.c_double), ('cutback_level', C.c_int), ('converged', C.c_int),
+                ('iterations', C.c_int), ('residual_evals', C.c_int), ('load_step', C.c_int),
+                ('step_inc', C.c_int), ('P_av', C.c_double * 9)]
+
+
 class SolutionStruct(C.Structure):
     _fields_ = [('iterationsNeeded', C.c_int), ('converged', C.c_int), ('stagConverged', C.c_int),
                 ('residualEvals', C.c_int), ('err_div', C.c_double), ('err_BC', C.c_double),
                 ('P_av', C.c_double * 9)]
+
+
+INCREMENT_CB = C.CFUNCTYPE(C.c_int, C.POINTER(IncrementInfoStruct), C.c_void_p)
+FORWARD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
+                         C.POINTER(BCStruct), C.POINTER(BCStruct), C.POINTER(C.c_double))
+SOLUTION_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(SolutionStruct))
+CTX_FN = C.CFUNCTYPE(C.c_int, C.c_void_p)
+
+
+class GridSolverStruct(C.Structure):
+    """dmk_grid_solver: the five plugin procedures as function pointers."""
+    _fields_ = [('ctx', C.c_void_p), ('forward', FORWARD_FN), ('solution', SOLUTION_FN),
+                ('update_coords', CTX_FN), ('materialpoint_forward', CTX_FN)]
+
+
+def loadstep_structs(loadcases) -> C.Array:
+    arr = (LoadStepStruct * len(loadcases))()
+    for s, lc in zip(arr, loadcases):
+        s.deformation, s.stress = lc.deformation_bc(), lc.stress_bc()
+        s.q_rot[:] = [float(x) for x in lc.q_rot]
+        s.t, s.N, s.r = float(lc.t), int(lc.N), float(lc.r)
+        s.f_out, s.f_restart, s.estimate_rate = int(lc.f_out), int(lc.f_restart), int(bool(lc.estimate_rate))
+    return arr
 
 
 LATTICES = {'cF': 0, 'cI': 1}

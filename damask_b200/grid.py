@@ -415,6 +415,43 @@ def run_load_cases(solver, loadcases: list[LoadCase], N_cutback_max: int = 3, ma
     return stats
 
 
+def run_load_cases_native(solver, loadcases: list[LoadCase], N_cutback_max: int = 3,
+                          max_increments: int | None = None, on_increment=None,
+                          restart_inc: int = 0) -> list[IncrementStats]:
+    """run_load_cases through the library's C++ increment loop (dmk_grid_run): for a
+    SpectralBasic the loop calls the context directly (no interpreter between the procedures);
+    any other solver offers ``native_solver()``, a dmk_grid_solver table of its procedures."""
+    from .config import INCREMENT_CB, loadstep_structs
+    lib = _lib.load()
+    steps = loadstep_structs(loadcases)
+    stats: list[IncrementStats] = []
+    clock = [time.perf_counter()]
+
+    def cb(info_p, _user):
+        i = info_p.contents
+        now = time.perf_counter()
+        rec = IncrementStats(i.inc, i.t, i.cutback_level, bool(i.converged), i.iterations, i.residual_evals,
+                             now - clock[0], np.array(i.P_av[:]).reshape(3, 3, order='F'))
+        clock[0] = now
+        stats.append(rec)
+        if on_increment is not None:
+            on_increment(rec)
+        return 0
+
+    cfn = INCREMENT_CB(cb)
+    nmax = int(max_increments or 0)
+    if isinstance(solver, SpectralBasic):
+        # (SpectralBasic.total_counters / total_ms are kept by its Python solution() only)
+        rc = lib.dmk_grid_run_ctx(solver.ctx, steps, len(loadcases), N_cutback_max, restart_inc, nmax, cfn, None)
+    else:
+        table = solver.native_solver()
+        rc = lib.dmk_grid_run(C.byref(table), steps, len(loadcases), N_cutback_max, restart_inc, nmax, cfn, None)
+    if rc == -7:
+        raise NotConverged(lib.dmk_last_error().decode())
+    _lib.check(rc)
+    return stats
+
+
 def read_sta(path) -> list[tuple]:
     """Rows of a .sta file: (increment, time, cutback level, converged, iterations, staggered)."""
     rows = []

@@ -46,6 +46,7 @@ extern "C" {
 #define DMK_ERR_ARG (-4)
 #define DMK_ERR_STATE (-5)
 #define DMK_STATUS_TIMEOUT (-6)
+#define DMK_ERR_NOT_CONVERGED (-7)   /* the driver's IO_error 950: no convergence after the cutbacks */
 
 /* precision of the spectral part (FFT, Gamma, field update) */
 #define DMK_PRECISION_FP64 0
@@ -266,6 +267,44 @@ int dmk_vti_label(const dmk_vti* vti, int index, char* out, int cap, int* compon
 int dmk_vti_read_int(const dmk_vti* vti, const char* label, int64_t* out, int64_t n);
 int dmk_vti_read_real(const dmk_vti* vti, const char* label, double* out, int64_t n);
 void dmk_vti_close(dmk_vti* vti);
+
+/* The grid driver's increment loop (DAMASK_grid.f90:288-460) for the mechanical field: time steps
+   t * math_geometricFraction(r, inc, N), the global cutback (time step halved up to N_cutback_max
+   times, then DMK_ERR_NOT_CONVERGED as IO_error 950), the guess flag, restart skipping
+   (increments <= restart_inc only advance t), and per (sub)increment the calls forward,
+   materialpoint_forward (not after a cutback), solution and, when converged, updateCoords.  The
+   plugin is a table of the five procedures (DAMASK_grid.f90:110-119), so the same loop drives this
+   library's context (dmk_grid_run_ctx) or any other implementation. */
+typedef struct {
+  dmk_bc deformation, stress;   /* tBCmech of the load step */
+  double q_rot[4];              /* load-case rotation R as a quaternion */
+  double t;                     /* duration */
+  int N;                        /* increments */
+  double r;                     /* geometric ratio of the increments (1: equal) */
+  int f_out, f_restart;         /* output and restart frequency (for the callback's use) */
+  int estimate_rate;            /* guess the rate of the first increment from the last one */
+} dmk_loadstep;
+typedef struct {
+  int inc;                      /* total increment counter */
+  double t;                     /* time at the end of the (sub)increment */
+  int cutback_level, converged, iterations, residual_evals;
+  int load_step, step_inc;      /* 0-based load step, 1-based increment within it */
+  double P_av[9];
+} dmk_increment_info;
+/* called after every converged (sub)increment; a nonzero return stops the run (returns 0) */
+typedef int (*dmk_increment_cb)(const dmk_increment_info* info, void* user);
+typedef struct {
+  void* ctx;
+  int (*forward)(void* ctx, int cutBack, int guess, double dt, double dt_old, double t_remaining,
+                 const dmk_bc* deformation, const dmk_bc* stress, const double q_rot[4]);
+  int (*solution)(void* ctx, dmk_solution_state* out);
+  int (*update_coords)(void* ctx);
+  int (*materialpoint_forward)(void* ctx);
+} dmk_grid_solver;
+int dmk_grid_run(const dmk_grid_solver* solver, const dmk_loadstep* steps, int n_steps, int N_cutback_max,
+                 int restart_inc, int max_increments /* <= 0: all */, dmk_increment_cb cb, void* user);
+int dmk_grid_run_ctx(dmk_ctx* ctx, const dmk_loadstep* steps, int n_steps, int N_cutback_max, int restart_inc,
+                     int max_increments, dmk_increment_cb cb, void* user);
 
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);

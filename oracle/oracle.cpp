@@ -1574,7 +1574,7 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
 }
 
 // grid_mechanical_spectral_basic_updateCoords, grid_mech_spectral_basic.f90:361-372
-void orc_update_coords(orc_ctx* c) { update_coords(c); }
+int orc_update_coords(orc_ctx* c) { update_coords(c); return 0; }
 
 void orc_get_coords(orc_ctx* c, double* ip, double* nodes) {
   if (ip) std::memcpy(ip, c->xp.data(), sizeof(double) * c->xp.size());
@@ -1582,9 +1582,10 @@ void orc_get_coords(orc_ctx* c, double* ip, double* nodes) {
 }
 
 // materialpoint_forward -> mechanical_forward, phase_mechanical.f90:987-1002
-void orc_materialpoint_forward(orc_ctx* c) {
+int orc_materialpoint_forward(orc_ctx* c) {
   c->Fi0 = c->Fi; c->Fp0 = c->Fp; c->F0 = c->F; c->Li0 = c->Li; c->Lp0 = c->Lp; c->S0 = c->S;
   c->state0 = c->state;
+  return 0;
 }
 
 int orc_constitutive_response(orc_ctx* c, const double* F, double dt, double* P, double P_av[9],

@@ -89,10 +89,10 @@ int  orc_mech_init(orc_ctx*);
 int  orc_mech_forward(orc_ctx*, int cutBack, int guess, double dt, double dt_old, double t_remaining,
                       const orc_bc* deformation, const orc_bc* stress, const double q_rot[4]);
 int  orc_mech_solution(orc_ctx*, orc_solution* out);
-void orc_materialpoint_forward(orc_ctx*);
+int  orc_materialpoint_forward(orc_ctx*);
 /* utilities_updateCoords (spectral_utilities.f90:857-968) on the solver F; coordinates
    (3 per cell centre / per node, x fastest), undeformed before the first update */
-void orc_update_coords(orc_ctx*);
+int  orc_update_coords(orc_ctx*);
 void orc_get_coords(orc_ctx*, double* ip, double* nodes);
 
 /* operator-level entry points */

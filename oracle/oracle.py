@@ -45,8 +45,8 @@ def load() -> C.CDLL:
         'orc_mech_forward': (C.c_int, [vp, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                                        C.POINTER(BCStruct), C.POINTER(BCStruct), dp]),
         'orc_mech_solution': (C.c_int, [vp, C.POINTER(SolutionStruct)]),
-        'orc_materialpoint_forward': (None, [vp]),
-        'orc_update_coords': (None, [vp]),
+        'orc_materialpoint_forward': (C.c_int, [vp]),
+        'orc_update_coords': (C.c_int, [vp]),
         'orc_get_coords': (None, [vp, dp, dp]),
         'orc_constitutive_response': (C.c_int, [vp, dp, C.c_double, dp, dp, dp, dp, C.POINTER(C.c_int)]),
         'orc_update_gamma': (None, [vp, dp]),
@@ -116,6 +116,18 @@ class OracleSpectralBasic:
 
     def update_coords(self) -> None:
         self.lib.orc_update_coords(self.ctx)
+
+    def native_solver(self):
+        """The oracle's procedures as a dmk_grid_solver table (its orc_bc and orc_solution have the
+        layouts of dmk_bc and dmk_solution_state)."""
+        from damask_b200.config import CTX_FN, FORWARD_FN, SOLUTION_FN, GridSolverStruct
+        t = GridSolverStruct()
+        t.ctx = self.ctx
+        t.forward = C.cast(self.lib.orc_mech_forward, FORWARD_FN)
+        t.solution = C.cast(self.lib.orc_mech_solution, SOLUTION_FN)
+        t.update_coords = C.cast(self.lib.orc_update_coords, CTX_FN)
+        t.materialpoint_forward = C.cast(self.lib.orc_materialpoint_forward, CTX_FN)
+        return t
 
     def get_coords(self) -> tuple[np.ndarray, np.ndarray]:
         ip = np.empty((self.N, 3))
