@@ -12,7 +12,7 @@ import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
 
-from .grid import SpectralBasic, run_load_cases
+from .grid import SpectralBasic, run_load_cases, run_load_cases_native
 
 
 class BatchRunner:
@@ -22,12 +22,13 @@ class BatchRunner:
     at most ``threads`` RVEs hold device memory at a time."""
 
     def __init__(self, jobs, threads: int = 16, precision: str = 'fp64', max_increments: int | None = None,
-                 solver_class=SpectralBasic):
+                 solver_class=SpectralBasic, native: bool = True):
         self.jobs = list(jobs)
         self.threads = max(1, int(threads))
         self.precision = precision
         self.max_increments = max_increments
         self.solver_class = solver_class
+        self.native = native              # the C++ increment loop: one library call per RVE
         self.results = [None] * len(self.jobs)
         self.updates = [0] * len(self.jobs)
         self._lock = threading.Lock()
@@ -36,8 +37,10 @@ class BatchRunner:
         rve, phase, lcs, num = self.jobs[k]
         s = self.solver_class(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=self.precision)
         try:
-            stats = run_load_cases(s, lcs, max_increments=self.max_increments)
-            total = int(s.total_counters[0])
+            run = run_load_cases_native if self.native else run_load_cases
+            stats = run(s, lcs, max_increments=self.max_increments)
+            # material-point updates of the converged solutions (cut-back attempts not counted)
+            total = sum(r.residual_evals for r in stats) * s.N
             if on_finish is not None:
                 on_finish(k, s)
         finally:
