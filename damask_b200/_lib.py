@@ -22,7 +22,7 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_phase_interaction', 'dmk_field_mean_noalloc', 'dmk_restart_write', 'dmk_restart_read',
            'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems', 'dmk_vti_open', 'dmk_vti_geometry',
            'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
-           'dmk_grid_run_ctx']
+           'dmk_grid_run_ctx', 'dmk_fp64_peak']
 
 _lib = None
 
@@ -67,6 +67,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
                                    C.c_int, INCREMENT_CB, C.c_void_p]),
         'dmk_grid_run_ctx': (C.c_int, [vp, C.POINTER(LoadStepStruct), C.c_int, C.c_int, C.c_int, C.c_int,
                                        INCREMENT_CB, C.c_void_p]),
+        'dmk_fp64_peak': (C.c_int, [C.c_int, dp]),
         'dmk_get_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_set_field': (C.c_int, [vp, C.c_int, dp]),
         'dmk_field_size': (C.c_int, [vp, C.c_int]),

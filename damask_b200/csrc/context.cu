@@ -1531,6 +1531,43 @@ int dmk_timer_stop(dmk_ctx* c, double* ms) {
   return 0;
 }
 
+int dmk_fp64_peak(int device, double* tflops) {
+  if (!tflops) return fail(DMK_ERR_ARG, "null argument");
+  CK(cudaSetDevice(device));
+  int nsm = 0;
+  CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+  const int blocks = nsm * 8, iters = 1 << 16;
+  double* sink = nullptr;
+  cudaStream_t s = nullptr;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  auto release = [&]() {
+    if (sink) cudaFree(sink);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (s) cudaStreamDestroy(s);
+  };
+  if (cudaMalloc(&sink, sizeof(double) * blocks) != cudaSuccess || cudaStreamCreate(&s) != cudaSuccess ||
+      cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    release();
+    return fail(DMK_ERR_CUDA, "fp64 probe: allocation failed");
+  }
+  float best = 1e30f;
+  cudaError_t e = launch_fp64_probe(sink, blocks, iters, s);           // warm-up
+  for (int r = 0; r < 3 && e == cudaSuccess; ++r) {
+    e = cudaEventRecord(e0, s);
+    if (e == cudaSuccess) e = launch_fp64_probe(sink, blocks, iters, s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e == cudaSuccess && ms < best) best = ms;
+  }
+  release();
+  if (e != cudaSuccess) return fail(DMK_ERR_CUDA, std::string("fp64 probe: ") + cudaGetErrorString(e));
+  *tflops = 2.0 * 8.0 * double(iters) * blocks * 256.0 / (double(best) * 1e-3) / 1e12;
+  return 0;
+}
+
 int dmk_get_timings(dmk_ctx* c, double out[3]) {
   if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
   for (int k = 0; k < 3; ++k) out[k] = c->last_ms[k];

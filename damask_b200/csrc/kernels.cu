@@ -810,3 +810,28 @@ cudaError_t launch_coords(const double* u, const double* favg, const int n[3], c
 }
 
 }  // namespace dmk
+
+namespace dmk {
+
+// FP64 fused multiply-add throughput of the device (the denominator of the constitutive update's
+// FP64 roofline): 8 independent FMA chains per thread in registers, `iters` rounds; the result
+// goes to `sink` so that nothing is eliminated.
+__global__ void __launch_bounds__(256) fp64_probe_kernel(double* sink, int iters, double a, double b) {
+  double x[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) x[k] = threadIdx.x * 1e-3 + k;
+  for (int i = 0; i < iters; ++i)
+#pragma unroll
+    for (int k = 0; k < 8; ++k) x[k] = fma(x[k], a, b);
+  double s = 0.0;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) s += x[k];
+  if (s == 1.2345) sink[blockIdx.x] = s;      // practically never true: keeps the chains live
+}
+
+cudaError_t launch_fp64_probe(double* sink, int blocks, int iters, cudaStream_t s) {
+  fp64_probe_kernel<<<blocks, 256, 0, s>>>(sink, iters, 0.999999, 1e-9);
+  return cudaGetLastError();
+}
+
+}  // namespace dmk

@@ -67,6 +67,7 @@ cudaError_t launch_to_float(const double* a, float* b, int64_t n, int nsm, cudaS
 cudaError_t launch_to_double(const float* a, double* b, int64_t n, int nsm, cudaStream_t s);
 
 cudaError_t launch_reduce9(const double* partials, int nparts, double* out9, cudaStream_t s);
+cudaError_t launch_fp64_probe(double* sink, int blocks, int iters, cudaStream_t s);
 
 // spectral polarization scheme (polarization.cu)
 struct PolConst {

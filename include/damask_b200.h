@@ -306,6 +306,11 @@ int dmk_grid_run(const dmk_grid_solver* solver, const dmk_loadstep* steps, int n
 int dmk_grid_run_ctx(dmk_ctx* ctx, const dmk_loadstep* steps, int n_steps, int N_cutback_max, int restart_inc,
                      int max_increments, dmk_increment_cb cb, void* user);
 
+/* Measured FP64 fused-multiply-add throughput of a device in TFLOP/s (8 independent register FMA
+   chains per thread, 8 blocks of 256 threads per SM, best of 3 launches of about 10 ms); the
+   denominator of the constitutive update's FP64 roofline. */
+int dmk_fp64_peak(int device, double* tflops);
+
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 /* Device timer on the context's stream: CUDA events recorded at start and stop;

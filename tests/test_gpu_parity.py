@@ -266,3 +266,12 @@ def test_displacements_of_the_converged_field(gpu, oracle_lib):
     u_o, _ = displacements(cells, size, ip_o, nodes_o)
     assert np.allclose(u_p, u_o, rtol=1e-5, atol=1e-8)
     assert rel(ip, ip_o) < 1e-12 and rel(nodes, nodes_o) < 1e-12
+
+
+def test_fp64_peak_probe(gpu):
+    """The FP64 FMA probe behind the bench's FP64 roofline gives a plausible B200 figure."""
+    import ctypes as C
+    from damask_b200 import _lib
+    out = C.c_double()
+    _lib.check(_lib.load().dmk_fp64_peak(0, C.byref(out)))
+    assert 10.0 < out.value < 80.0
