@@ -1,12 +1,15 @@
 /*
  * damask_b200 — C-ABI of the B200 (sm_100a) implementation of DAMASK's grid
  * mechanical hot path: the basic spectral (FFT) fixed-point scheme with the
- * Gamma-operator convolution, driving the per-voxel phenopowerlaw/Hooke
- * constitutive update (FPI state integration, Lp Newton-Raphson, dP/dF).
+ * Gamma-operator convolution (and the spectral polarization scheme), driving the
+ * per-voxel phenopowerlaw/Hooke constitutive update (FPI state integration, Lp
+ * Newton-Raphson, dP/dF); coordinates, the grid geometry reader and the driver's
+ * increment loop.
  *
  * The entry points mirror the Fortran procedures the reference selects through
- * procedure pointers in src/grid/DAMASK_grid.f90:110-119,171-206, so a
- * Fortran host can bind them with ISO_C_BINDING.
+ * procedure pointers in src/grid/DAMASK_grid.f90:110-119,171-206, so a Fortran
+ * host can bind them with ISO_C_BINDING: one bind(C) interface per function,
+ * structs as bind(C) derived types, contexts as type(C_PTR).
  *
  * Conventions
  *  - Plain C types only; all arrays are host pointers owned by the caller and
