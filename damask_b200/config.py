@@ -298,7 +298,7 @@ class Numerics:
         if self.N_iter_min > self.N_iter_max or self.N_iter_min < 1: bad.append('N_iter_min')
         if self.N_iter_Lp_max < 1: bad.append('N_iter_Lp_max')
         if self.N_iter_state_max < 1: bad.append('N_iter_state_max')
-        if self.derivative != 'continuous': bad.append('derivative')
+        if self.derivative not in ('continuous', 'central_difference'): bad.append('derivative')
         if not 1 <= self.anderson_m <= 32: bad.append('anderson_m')
         if self.solver not in SOLVERS: bad.append('solver')
         if self.solver == 'spectral_polarization':
@@ -318,7 +318,7 @@ class Numerics:
         s.eps_abs_P, s.eps_rel_P = self.eps_abs_P, self.eps_rel_P
         s.update_gamma = int(bool(self.update_gamma))
         s.divergence_correction = {'none': 0, 'size': 1, 'grid+size': 2, 'size+grid': 2}[self.divergence_correction]
-        s.derivative = 0
+        s.derivative = {'continuous': 0, 'central_difference': 1}[self.derivative]
         s.r_cutback_min, s.r_cutback, s.r_increase = self.r_cutback_min, self.r_cutback, self.r_increase
         s.eps_rel_state, s.N_iter_state_max = self.eps_rel_state, int(self.N_iter_state_max)
         s.N_iter_Lp_max, s.r_linesearch_Lp = int(self.N_iter_Lp_max), self.r_linesearch_Lp

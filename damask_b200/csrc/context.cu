@@ -689,7 +689,8 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
     CKF(cufftExecZ2D(c->plan_bwd, spec, rtau));
     CKL(launch_pol_tau(c->Fsol, rtau, N, beta, c->Feval, c->stream));
     CKF(cufftExecD2Z(c->plan_fwd, c->Fsol, spec));                      // curl of F
-    CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->curl_partials, c->stream));
+    CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->gc.derivative,
+                    c->curl_partials, c->stream));
     CK(cudaEventRecord(c->ev[3], c->stream));
     int st = 0;                                                          // constitutive at F - r_F_tau / beta
     if (int e = evaluate_constitutive(c, c->dt, nullptr, 0, &st, c->Feval)) return e;
@@ -829,7 +830,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   for (int i = 0; i < 3; ++i)
     if (cells[i] < 1 || !(geomSize[i] > 0.0)) return fail(DMK_ERR_ARG, "cells and geomSize must be positive");
   if (precision != DMK_PRECISION_FP64 && precision != DMK_PRECISION_MIXED) return fail(DMK_ERR_ARG, "unknown precision");
-  if (num->derivative != 0) return fail(DMK_ERR_CONFIG, "only the continuous spectral derivative is on this path");
+  if (num->derivative != 0 && num->derivative != 1)
+    return fail(DMK_ERR_CONFIG, "spectral derivative must be continuous (0) or central_difference (1)");
   if (num->N_iter_max < 1 || num->N_iter_min < 1 || num->N_iter_min > num->N_iter_max)
     return fail(DMK_ERR_CONFIG, "invalid N_iter_min/N_iter_max");
   if (num->N_iter_Lp_max < 1 || num->N_iter_state_max < 1 || num->f_update_jacobi_Lp < 1 || !(num->r_cutback > 0.0) ||
@@ -887,6 +889,7 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   double sgs[3];
   scaled_geom(cells, geomSize, num->divergence_correction, sgs);
   for (int i = 0; i < 3; ++i) c->gc.rescale[i] = geomSize[i] / sgs[i];
+  c->gc.derivative = num->derivative;
 
   switch (c->NS) {
     case 12: c->pc12 = new PhaseConst<12>(); fill_phase_const<12>(c->hp, *c->pc12); break;
@@ -1279,7 +1282,8 @@ int dmk_mech_update_coords(dmk_ctx* c) {
   const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
   const double step[3] = {c->geom[0] / c->cells[0], c->geom[1] / c->cells[1], c->geom[2] / c->cells[2]};
   CKF(cufftExecD2Z(c->plan_fwd, c->Fsol, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
-  CKL(launch_coords_spec(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->wgt, c->favg, c->stream));
+  CKL(launch_coords_spec(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->wgt, c->favg, c->gc.derivative,
+                         c->stream));
   CKF(cufftExecZ2D(c->plan_vec_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), c->scratch));
   CKL(launch_coords(c->scratch, c->favg, c->cells, step, c->wgt, c->xp, c->xn, c->stream));
   c->launches += 2;   // each launcher above issues two kernels
@@ -1422,7 +1426,8 @@ int dmk_curl_rms(dmk_ctx* c, const double* F, double* out) {
   if (int rc = h2d_planes(c, F, c->r, 9)) return rc;
   CKF(cufftExecD2Z(c->plan_fwd, c->r, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
   const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
-  CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->div_partials, c->stream));
+  CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->gc.derivative,
+                    c->div_partials, c->stream));
   const int nb = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
   std::vector<double> h(nb);
   CK(cudaMemcpyAsync(h.data(), c->div_partials, sizeof(double) * nb, cudaMemcpyDeviceToHost, c->stream));

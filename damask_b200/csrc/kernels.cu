@@ -171,11 +171,10 @@ gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2,
     const int kz = int(rest / n1);
     const int sy = ky > n1 / 2 ? ky - n1 : ky;
     const int sz = kz > n2 / 2 ? kz - n2 : kz;
-    const double TAU = 6.283185307179586;
     double a[3];
-    a[0] = (n0 % 2 == 0 && kx == n0 / 2) ? 0.0 : TAU * double(kx) / L0;
-    a[1] = (n1 % 2 == 0 && ky == n1 / 2) ? 0.0 : TAU * double(sy) / L1;
-    a[2] = (n2 % 2 == 0 && kz == n2 / 2) ? 0.0 : TAU * double(sz) / L2;
+    a[0] = freq_derivative(kx, n0, L0, gc.derivative, true);
+    a[1] = freq_derivative(sy, n1, L1, gc.derivative, true);
+    a[2] = freq_derivative(sz, n2, L2, gc.derivative, true);
     double pr[9], pi[9];
 #pragma unroll
     for (int c = 0; c < 9; ++c) {
@@ -676,7 +675,7 @@ namespace dmk {
 // planes 0..2 of the spectrum; k = 0 gives 0 and the average F = Re F_hat(0) wgt.
 __global__ void __launch_bounds__(SPEC_THREADS)
 coords_spec_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
-                   double wgt, double* __restrict__ favg) {
+                   double wgt, double* __restrict__ favg, int derivative) {
   const int red0 = n0 / 2 + 1;
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (idx >= plane) return;
@@ -684,9 +683,9 @@ coords_spec_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n
   const int64_t rest = idx / red0;
   const int ky = int(rest % n1);
   const int kz = int(rest / n1);
-  const double TAU = 6.283185307179586;
-  const double a[3] = {TAU * double(kx) / L0, TAU * double(ky > n1 / 2 ? ky - n1 : ky) / L1,
-                       TAU * double(kz > n2 / 2 ? kz - n2 : kz) / L2};
+  const double a[3] = {freq_derivative(kx, n0, L0, derivative, false),
+                       freq_derivative(ky > n1 / 2 ? ky - n1 : ky, n1, L1, derivative, false),
+                       freq_derivative(kz > n2 / 2 ? kz - n2 : kz, n2, L2, derivative, false)};
   double2 F[9];
 #pragma unroll
   for (int c = 0; c < 9; ++c) F[c] = S[c * plane + idx];
@@ -787,11 +786,11 @@ __global__ void coords_node_kernel(const double* __restrict__ u, const double* _
 }
 
 cudaError_t launch_coords_spec(double* spec, int n0, int n1, int n2, const double L[3], double wgt, double* favg,
-                               cudaStream_t s) {
+                               int derivative, cudaStream_t s) {
   const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
   double2* S = reinterpret_cast<double2*>(spec);
   coords_spec_kernel<<<unsigned((plane + SPEC_THREADS - 1) / SPEC_THREADS), SPEC_THREADS, 0, s>>>(
-      S, plane, n0, n1, n2, L[0], L[1], L[2], wgt, favg);
+      S, plane, n0, n1, n2, L[0], L[1], L[2], wgt, favg, derivative);
   const int64_t yz = int64_t(n1) * n2;
   const dim3 grid(unsigned((yz + SPEC_THREADS - 1) / SPEC_THREADS), (n0 % 2 == 0 && n0 > 1) ? 2u : 1u);
   coords_hermitian_kernel<<<grid, SPEC_THREADS, 0, s>>>(S, plane, n0, n1, n2);

@@ -29,7 +29,20 @@ struct SolverScalars {
 struct GammaConst {
   double Cref[81];       // C_ref = C / wgt, column-major 3x3x3x3
   double rescale[3];     // geomSize / scaledGeomSize
+  int derivative;        // 0 continuous, 1 central difference
 };
+
+// Imaginary part a of the spectral derivative xi = i a for signed frequency k of an edge of n
+// cells and length L (utilities_getFreqDerivative, spectral_utilities.f90:808-850): continuous
+// 2 pi k / L, central difference sin(2 pi k / n) / (2 L / n).  first_order: the first-derivative
+// frequencies xi1st, whose Nyquist component is zero on even edges for the continuous
+// derivative (:322-332).
+__device__ __forceinline__ double freq_derivative(int k, int n, double L, int derivative, bool first_order) {
+  const double TAU = 6.283185307179586;
+  if (derivative == 1) return sin(TAU * double(k) / double(n)) / (2.0 * L / double(n));
+  if (first_order && n % 2 == 0 && k == n / 2) return 0.0;
+  return TAU * double(k) / L;
+}
 
 struct Numerics2 {
   int N_iter_min, N_iter_max, cells0;
@@ -81,7 +94,7 @@ cudaError_t launch_pol_tau(const double* F, double* G, int64_t N, double beta, d
 cudaError_t launch_pol_rF(const double* F, const double* Ftau, const double* P, const double* dPdF, const double* rtau,
                           int64_t N, const PolConst& pc, double* rF, cudaStream_t s);
 cudaError_t launch_curl(const double* spec, int n0, int n1, int n2, const double L[3], const double rg[3],
-                        double* partials, cudaStream_t s);
+                        int derivative, double* partials, cudaStream_t s);
 cudaError_t launch_pol_forward_tau(const double* F, double* Ftau, double* Flast, double* Fdot, int64_t N, int cutBack,
                                    int guess, double dt, double dt_old, const double* avRate, const PolConst& pc,
                                    cudaStream_t s);
@@ -90,7 +103,7 @@ cudaError_t launch_sub(double* X, const double* r, int64_t n, int nsm, cudaStrea
 // utilities_updateCoords (kernels.cu): u_hat from the spectrum of F (planes 0..2, Hermitian), then
 // cell-centre and node coordinates from the C2R output u (null: undeformed coordinates)
 cudaError_t launch_coords_spec(double* spec, int n0, int n1, int n2, const double L[3], double wgt, double* favg,
-                               cudaStream_t s);
+                               int derivative, cudaStream_t s);
 cudaError_t launch_coords(const double* u, const double* favg, const int n[3], const double step[3], double wgt,
                           double* xp, double* xn, cudaStream_t s);
 

@@ -131,7 +131,7 @@ pol_rF_kernel(const double* __restrict__ F, const double* __restrict__ Ftau, con
 // as the reference's scalar assignment to the whole array does.
 __global__ void __launch_bounds__(SPEC_THREADS)
 curl_kernel(const double2* __restrict__ S, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
-            double rg0, double rg1, double rg2, double* __restrict__ partials) {
+            double rg0, double rg1, double rg2, int derivative, double* __restrict__ partials) {
   __shared__ double red[SPEC_THREADS / 32];
   const int red0 = n0 / 2 + 1;
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -143,12 +143,11 @@ curl_kernel(const double2* __restrict__ S, int64_t plane, int n0, int n1, int n2
     const int kz = int(rest / n1);
     const int sy = ky > n1 / 2 ? ky - n1 : ky;
     const int sz = kz > n2 / 2 ? kz - n2 : kz;
-    const double TAU = 6.283185307179586;
-    // xi1st * rescaledGeom = i w (continuous derivative, Nyquist zeroed on even edges)
+    // xi1st * rescaledGeom = i w
     double w[3];
-    w[0] = ((n0 % 2 == 0 && kx == n0 / 2) ? 0.0 : TAU * double(kx) / L0) * rg0;
-    w[1] = ((n1 % 2 == 0 && ky == n1 / 2) ? 0.0 : TAU * double(sy) / L1) * rg1;
-    w[2] = ((n2 % 2 == 0 && kz == n2 / 2) ? 0.0 : TAU * double(sz) / L2) * rg2;
+    w[0] = freq_derivative(kx, n0, L0, derivative, true) * rg0;
+    w[1] = freq_derivative(sy, n1, L1, derivative, true) * rg1;
+    w[2] = freq_derivative(sz, n2, L2, derivative, true) * rg2;
     // (x + i y) (i w) = -y w + i x w
     auto term = [&](int c1, int d1, int c2, int d2, double& re, double& im) {
       const double2 a = S[c1 * plane + idx], b = S[c2 * plane + idx];
@@ -256,10 +255,11 @@ cudaError_t launch_pol_rF(const double* F, const double* Ftau, const double* P, 
   return cudaGetLastError();
 }
 cudaError_t launch_curl(const double* spec, int n0, int n1, int n2, const double L[3], const double rg[3],
-                        double* partials, cudaStream_t s) {
+                        int derivative, double* partials, cudaStream_t s) {
   const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
   curl_kernel<<<unsigned(gamma_div_blocks(n0, n1, n2)), SPEC_THREADS, 0, s>>>(
-      reinterpret_cast<const double2*>(spec), plane, n0, n1, n2, L[0], L[1], L[2], rg[0], rg[1], rg[2], partials);
+      reinterpret_cast<const double2*>(spec), plane, n0, n1, n2, L[0], L[1], L[2], rg[0], rg[1], rg[2], derivative,
+      partials);
   return cudaGetLastError();
 }
 cudaError_t launch_pol_forward_tau(const double* F, double* Ftau, double* Flast, double* Fdot, int64_t N, int cutBack,

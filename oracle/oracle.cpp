@@ -909,6 +909,14 @@ int constitutive_response(orc_ctx* c, double dt, bool rotate) {
 // ---------------------------------------------------------------- spectral
 inline long fidx(const orc_ctx* c, int x, int y, int z) { return (long(z) * c->cells[1] + y) * c->red + x; }
 
+// utilities_getFreqDerivative, spectral_utilities.f90:808-850: imaginary part of the derivative of
+// frequency k along d (continuous 2 pi k / L; central difference sin(2 pi k / n) / (2 L / n))
+double freq_derivative(const orc_ctx* c, int k, int d) {
+  if (c->num.derivative == 1)
+    return std::sin(TAU * double(k) / double(c->cells[d])) / (2.0 * c->geomSize[d] / double(c->cells[d]));
+  return TAU * double(k) / c->geomSize[d];
+}
+
 void spectral_init(orc_ctx* c) {
   const int* n = c->cells;
   c->red = n[0] / 2 + 1;
@@ -926,14 +934,15 @@ void spectral_init(orc_ctx* c) {
   } else {
     for (int i = 0; i < 3; ++i) c->scaledGeomSize[i] = g[i];
   }
-  // xi1st (continuous), spectral_utilities.f90:315-333 and :808-850
+  // xi1st, spectral_utilities.f90:315-333 and :808-850 (imaginary part; continuous: Nyquist
+  // zeroed on even edges, central difference: as xi2nd)
   c->xi.assign(size_t(c->red) * n[1] * n[2] * 3, 0.0);
   for (int z = 0; z < n[2]; ++z) for (int y = 0; y < n[1]; ++y) for (int x = 0; x < c->red; ++x) {
     int ks[3] = {x, y > n[1] / 2 ? y - n[1] : y, z > n[2] / 2 ? z - n[2] : z};
     int idx[3] = {x, y, z};
     for (int d = 0; d < 3; ++d) {
-      double v = TAU * double(ks[d]) / g[d];
-      if (n[d] % 2 == 0 && idx[d] == n[d] / 2) v = 0.0;
+      double v = freq_derivative(c, ks[d], d);
+      if (c->num.derivative == 0 && n[d] % 2 == 0 && idx[d] == n[d] / 2) v = 0.0;
       c->xi[fidx(c, x, y, z) * 3 + d] = v;
     }
   }
@@ -1072,7 +1081,7 @@ void update_coords(orc_ctx* c) {
     if (x == 0 && y == 0 && z == 0) { for (int l = 0; l < 3; ++l) half[l * H + f] = 0.0; continue; }
     int ks[3] = {x, y > n1 / 2 ? y - n1 : y, z > n2 / 2 ? z - n2 : z};
     cd xi2[3];
-    for (int d = 0; d < 3; ++d) xi2[d] = cd(0.0, TAU * double(ks[d]) / g[d]);   // no Nyquist zeroing
+    for (int d = 0; d < 3; ++d) xi2[d] = cd(0.0, freq_derivative(c, ks[d], d));   // no Nyquist zeroing
     cd den = 0.0;
     for (int d = 0; d < 3; ++d) den += std::conj(-xi2[d]) * xi2[d];
     for (int l = 0; l < 3; ++l) {

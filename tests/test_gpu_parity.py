@@ -275,3 +275,25 @@ def test_fp64_peak_probe(gpu):
     out = C.c_double()
     _lib.check(_lib.load().dmk_fp64_peak(0, C.byref(out)))
     assert 10.0 < out.value < 80.0
+
+
+@pytest.mark.parametrize('option', ['update_gamma', 'divergence_correction_none', 'divergence_correction_size',
+                                    'central_difference'])
+def test_numerics_options(gpu, oracle_lib, option):
+    """update_gamma (Gamma re-based on C_minMaxAvg every solution, spectral_utilities.f90:356-395)
+    and the divergence_correction modes (scaledGeomSize, :181-197) on a non-cubic RVE."""
+    num = workloads.numerics_default()
+    if option == 'update_gamma':
+        num.update_gamma = True
+    elif option == 'central_difference':
+        num.derivative = 'central_difference'      # utilities_getFreqDerivative, :808-850
+    else:
+        num.divergence_correction = option.split('_')[-1]
+    g, o = pair(oracle_lib, (8, 6, 10), 6, seed=5, num=num, size=(1.0e-3, 0.75e-3, 1.25e-3))
+    sg, so = run_both(g, o, 3)
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    for a, b in zip(sg, so):
+        assert rel(a.P_av, b.P_av) < TOL
+    for name in ('P', 'F', 'xi_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    g.close()

@@ -43,14 +43,22 @@ def test_divergence_rms_matches_reference_numpy(golden, oracle_lib):
     assert rel(o.divergence_rms(P), golden['div_rms']) < 1e-12
 
 
-def test_divergence_of_constant_field_vanishes(oracle_lib):
-    o = small_oracle(oracle_lib, cells=(5, 4, 6), init=False)
+def numerics_with(derivative):
+    n = workloads.numerics_default()
+    n.derivative = derivative
+    return n
+
+
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference'])
+def test_divergence_of_constant_field_vanishes(oracle_lib, derivative):
+    o = small_oracle(oracle_lib, cells=(5, 4, 6), init=False, num=numerics_with(derivative))
     P = np.tile(np.random.default_rng(3).normal(size=9) * 1e8, (o.N, 1))
     assert o.divergence_rms(P) < 5e-14 * 1e8
 
 
-def test_gamma_convolution_of_constant_field_is_aim(oracle_lib):
-    o = small_oracle(oracle_lib, cells=(4, 6, 5))
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference'])
+def test_gamma_convolution_of_constant_field_is_aim(oracle_lib, derivative):
+    o = small_oracle(oracle_lib, cells=(4, 6, 5), num=numerics_with(derivative))
     field = np.tile(np.random.default_rng(4).normal(size=9), (o.N, 1))
     aim = np.random.default_rng(5).normal(size=9)
     out = o.gamma_convolution(field, aim)
@@ -202,3 +210,23 @@ def test_coordinates_start_undeformed_and_follow_uniform_F(oracle_lib):
     up, un = displacements(cells, size, ip, nodes)
     assert rel(up, ip0 @ (Fu - np.eye(3)).T) < 1e-12
     assert rel(un, n0 @ (Fu - np.eye(3)).T) < 1e-12
+
+
+def test_central_difference_divergence_matches_finite_differences(oracle_lib):
+    """With derivative: central_difference the reference's frequencies are
+    i sin(2 pi k / n) / (2 L / n) (spectral_utilities.f90:808-850), half the symbol of the usual
+    central difference, so the spectral divergence is sum_j (P(x + h_j) - P(x - h_j)) / (4 h_j);
+    with divergence_correction 'size' no rescaling applies (:181-197), and the RMS follows
+    Parseval (:650-691)."""
+    cells, size = (6, 5, 7), (1.0e-3, 0.8e-3, 1.4e-3)
+    num = numerics_with('central_difference')
+    num.divergence_correction = 'size'
+    o = oracle_lib.OracleSpectralBasic(cells, size, np.zeros(int(np.prod(cells))), np.array([[1.0, 0, 0, 0]]),
+                                       workloads.fcc_al(), num, init=False, threads=1)
+    P = np.random.default_rng(9).normal(size=cells + (3, 3))
+    h = np.asarray(size) / np.asarray(cells)
+    div = sum((np.roll(P[..., :, j], -1, axis=j) - np.roll(P[..., :, j], 1, axis=j)) / (4 * h[j]) for j in range(3))
+    voxels = np.transpose(P, (0, 1, 2, 4, 3)).reshape(cells + (9,)).reshape(-1, 9, order='F')
+    rms = np.sqrt(np.mean(np.sum(div ** 2, axis=-1)))
+    assert abs(o.divergence_rms(voxels) - rms) < 1e-12 * rms
+    o.close()
