@@ -181,12 +181,14 @@ def load_peaks() -> dict:
     return {'hbm_gbs': 6650.0, 'source': 'fallback'}
 
 
-def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, local: int, cells=None) -> dict:
+def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, local: int, cells=None,
+            solver_name: str = 'spectral_basic') -> dict:
     from damask_b200 import workloads
     from damask_b200.grid import IncrementDriver, SpectralBasic
 
     import torch
     rve, phase, lcs, num = workloads.make(WORKLOAD, cells)
+    num.solver = solver_name
     free0 = torch.cuda.mem_get_info(local)[0]
     solver = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision,
                            device=local)
@@ -320,6 +322,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--precision', choices=['both', 'mixed', 'fp64'], default='both',
                     help='run one precision only (profiling); the bench line needs both')
+    ap.add_argument('--solver', choices=['spectral_basic', 'spectral_polarization'], default='spectral_basic',
+                    help='grid solver (the bench line is defined for spectral_basic)')
     ap.add_argument('--batch', type=int, default=0,
                     help='measure the batched workload instead: this many independent RVEs (512 in the '
                          'workload definition), one JSON line of its own')
@@ -350,7 +354,7 @@ def main():
     res = {}
     precs = ('mixed', 'fp64') if args.precision == 'both' else (args.precision,)
     for prec in precs:
-        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells)
+        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver)
     mx = res.get('mixed', res.get('fp64'))
     fp = res.get('fp64', mx)
     ms_max = allreduce_max(mx['ms'], world)
@@ -386,7 +390,8 @@ def main():
         'config': {'workload': f'{WORKLOAD}: 256^3 grid, 2000 Voronoi grains (seed 3), bcc N_sl [12,12], '
                                'tension dot_F_xx 1e-3/s, 100 increments to 10 %' if cells is None else
                                f'{WORKLOAD} at {cells}',
-                   'solver': 'basic spectral, Anderson fixed point (m=8)', 'precision': 'mixed',
+                   'solver': f"{args.solver.replace('spectral_', '')} spectral, Anderson fixed point (m=8)",
+                   'precision': 'mixed',
                    'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
                    'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
         'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
