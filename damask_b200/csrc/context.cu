@@ -236,11 +236,11 @@ int run_constitutive(dmk_ctx* c, const Fields& f, double dt, int apply) {
   }
   return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
 }
-cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o) {
+cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o, bool with_sums = true) {
   switch (c->NS) {
-    case 12: return launch_dPdF<12>(*c->pc12, f, dt, o, 0, c->N, c->stream);
-    case 18: return launch_dPdF<18>(*c->pc18, f, dt, o, 0, c->N, c->stream);
-    case 24: return launch_dPdF<24>(*c->pc24, f, dt, o, 0, c->N, c->stream);
+    case 12: return launch_dPdF<12>(*c->pc12, f, dt, o, 0, c->N, c->stream, with_sums);
+    case 18: return launch_dPdF<18>(*c->pc18, f, dt, o, 0, c->N, c->stream, with_sums);
+    case 24: return launch_dPdF<24>(*c->pc24, f, dt, o, 0, c->N, c->stream, with_sums);
   }
   return cudaErrorInvalidValue;
 }
@@ -472,12 +472,18 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
 // dP/dF of every voxel from the stored state: C_volAvg and C_minMaxAvg (grid_utilities.f90:171-202)
 int ensure_scratch(dmk_ctx* c, int K);
 
-int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev) {
+// planes_ready: the dPdF planes and norms of the current state are in place (evaluate_tangent_planes),
+// only their reductions remain
+int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev, bool planes_ready = false) {
   Fields f = make_fields(c, nullptr);
   TangentOut o = c->tan;
   o.per_voxel = per_voxel_dev;
-  CKL(run_dPdF(c, f, dt, o));
-  ++c->launches;                                           // tangent and its column sums
+  if (planes_ready) {
+    CKL(launch_tangent_sums(o, 0, c->N, c->N, c->stream));
+  } else {
+    CKL(run_dPdF(c, f, dt, o));
+    ++c->launches;                                         // tangent and its column sums
+  }
   if (per_voxel_dev) CKL(launch_from_planes(c->tan.planes, per_voxel_dev, c->N, 81, c->stream));
   CKL(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
   c->launches += 2;   // reduce, finalize and first-index kernels
@@ -533,6 +539,13 @@ bool inv_sym3333_host(const double* A, double* out) {
 int set_polarization_scale(dmk_ctx* c) {
   std::memcpy(c->polc.C, c->C_minMaxAvg, sizeof c->polc.C);
   if (!inv_sym3333_host(c->C_minMaxAvg, c->polc.S)) return fail(DMK_ERR_STATE, "matrix inversion error (S_scale)");
+  return 0;
+}
+
+// dP/dF planes (and norms) of every voxel from the stored state, without the reductions
+int evaluate_tangent_planes(dmk_ctx* c, double dt) {
+  Fields f = make_fields(c, nullptr);
+  CKL(run_dPdF(c, f, dt, c->tan, false));
   return 0;
 }
 
@@ -699,7 +712,9 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
     c->last_ms[1] += ms;
     CKL(launch_aim(c->sc, c->partials, nblocks_const(c), c->wgt, 0, c->stream));
     CK(cudaEventRecord(c->ev[0], c->stream));
-    if (int e = evaluate_tangent(c, c->dt, nullptr)) return e;
+    // the per-voxel tangent enters r_F; C_volAvg / C_minMaxAvg of the last residual are reduced
+    // from its planes after the solve (nothing reads them before)
+    if (int e = evaluate_tangent_planes(c, c->dt)) return e;
     CK(cudaEventRecord(c->ev[1], c->stream));
     CKF(cufftExecD2Z(c->plan_fwd, c->P, spec));                         // divergence of P
     CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, 0, 1,
@@ -796,6 +811,7 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
     }
     if (int rc = residual()) return rc;
   }
+  if (int rc = evaluate_tangent(c, c->dt, nullptr, true)) return rc;   // reductions of the last planes
   out->converged = reason > 0;
   out->iterationsNeeded = totalIter;
   out->stagConverged = 1;

@@ -341,18 +341,26 @@ int dPdF_blocks(int64_t count) { return int(std::max<int64_t>(1, std::min<int64_
 
 template <int NS>
 cudaError_t launch_dPdF(const PhaseConst<NS>& pc, const Fields& f, double dt, const TangentOut& o, int64_t first,
-                        int64_t count, cudaStream_t s) {
+                        int64_t count, cudaStream_t s, bool with_sums) {
   const size_t smem = size_t(TAN_SLOTS) * TAN_THREADS * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(dPdF_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   const int nb = int((count + TAN_THREADS - 1) / TAN_THREADS);
   dPdF_kernel<NS><<<nb, TAN_THREADS, smem, s>>>(pc, f, dt, o, first, count);
-  tangent_sum_kernel<<<dPdF_blocks(count), TSUM_THREADS, 0, s>>>(o.planes, o.norms, first, count, f.N, o);
+  if (with_sums) tangent_sum_kernel<<<dPdF_blocks(count), TSUM_THREADS, 0, s>>>(o.planes, o.norms, first, count, f.N, o);
   return cudaGetLastError();
 }
-template cudaError_t launch_dPdF<12>(const PhaseConst<12>&, const Fields&, double, const TangentOut&, int64_t, int64_t, cudaStream_t);
-template cudaError_t launch_dPdF<18>(const PhaseConst<18>&, const Fields&, double, const TangentOut&, int64_t, int64_t, cudaStream_t);
-template cudaError_t launch_dPdF<24>(const PhaseConst<24>&, const Fields&, double, const TangentOut&, int64_t, int64_t, cudaStream_t);
+
+cudaError_t launch_tangent_sums(const TangentOut& o, int64_t first, int64_t count, int64_t N, cudaStream_t s) {
+  tangent_sum_kernel<<<dPdF_blocks(count), TSUM_THREADS, 0, s>>>(o.planes, o.norms, first, count, N, o);
+  return cudaGetLastError();
+}
+template cudaError_t launch_dPdF<12>(const PhaseConst<12>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
+                                     cudaStream_t, bool);
+template cudaError_t launch_dPdF<18>(const PhaseConst<18>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
+                                     cudaStream_t, bool);
+template cudaError_t launch_dPdF<24>(const PhaseConst<24>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
+                                     cudaStream_t, bool);
 
 // Sums the per-block partials (C_volAvg) and finds the extreme Frobenius norms.
 // dPdF_max / dPdF_min (grid_utilities.f90:171-197) are the voxels of maximal /

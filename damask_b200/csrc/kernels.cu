@@ -368,13 +368,21 @@ forward_kernel(double* __restrict__ Fsol, double* __restrict__ Flast, double* __
 #pragma unroll
     for (int k = 0; k < 9; ++k) partials[int64_t(blockIdx.x) * 9 + k] = s[k];
 }
-// reduce partials once (so that the shift kernel does not re-read them per block)
-__global__ void reduce_partials9_kernel(const double* partials, int nparts, double* out) {
-  const int k = threadIdx.x;
-  if (k >= 9) return;
-  double s = 0.0;
-  for (int b = 0; b < nparts; ++b) s += partials[int64_t(b) * 9 + k];
-  out[k] = s;
+// reduce partials once (so that the shift kernel does not re-read them per block): one block of
+// REDUCE_THREADS, thread t sums the partials t, t + REDUCE_THREADS, ... (a fixed order), then a
+// block reduction
+constexpr int REDUCE_THREADS = 256;
+__global__ void __launch_bounds__(REDUCE_THREADS) reduce_partials9_kernel(const double* partials, int nparts,
+                                                                          double* out) {
+  __shared__ double red[9 * (REDUCE_THREADS / 32)];
+  double v[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+  for (int b = threadIdx.x; b < nparts; b += REDUCE_THREADS)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) v[k] += partials[int64_t(b) * 9 + k];
+  block_reduce_sum<9>(v, red);
+  if (threadIdx.x == 0)
+#pragma unroll
+    for (int k = 0; k < 9; ++k) out[k] = v[k];
 }
 __global__ void shift2_kernel(double* __restrict__ Fsol, int64_t N, const double* __restrict__ sums, double wgt,
                               const double* __restrict__ aim) {
@@ -384,7 +392,7 @@ __global__ void shift2_kernel(double* __restrict__ Fsol, int64_t N, const double
   for (int k = 0; k < 9; ++k) Fsol[k * N + v] -= sums[k] * wgt - aim[k];
 }
 cudaError_t launch_reduce9(const double* partials, int nparts, double* out9, cudaStream_t s) {
-  reduce_partials9_kernel<<<1, 32, 0, s>>>(partials, nparts, out9);
+  reduce_partials9_kernel<<<1, REDUCE_THREADS, 0, s>>>(partials, nparts, out9);
   return cudaGetLastError();
 }
 // stage 2: F -= (<F> * wgt - aim)
@@ -393,7 +401,7 @@ cudaError_t launch_forward(double* Fsol, double* Flast, double* Fdot, int64_t N,
                            const double* aim, cudaStream_t s) {
   const int nb = int((N + CONST_THREADS - 1) / CONST_THREADS);
   forward_kernel<<<nb, CONST_THREADS, 0, s>>>(Fsol, Flast, Fdot, N, cutBack, guess, dt, dt_old, avRate, partials);
-  reduce_partials9_kernel<<<1, 32, 0, s>>>(partials, nb, sums);
+  reduce_partials9_kernel<<<1, REDUCE_THREADS, 0, s>>>(partials, nb, sums);
   shift2_kernel<<<int((N + 255) / 256), 256, 0, s>>>(Fsol, N, sums, wgt, aim);
   return cudaGetLastError();
 }

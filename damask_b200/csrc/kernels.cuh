@@ -127,7 +127,9 @@ struct TangentOut {
 int tangent_reduce_doubles();
 template <int NS>
 cudaError_t launch_dPdF(const PhaseConst<NS>& pc, const Fields& f, double dt, const TangentOut& o, int64_t first,
-                        int64_t count, cudaStream_t s);
+                        int64_t count, cudaStream_t s, bool with_sums = true);
+// column sums and norms of the dPdF planes (the second stage of launch_dPdF)
+cudaError_t launch_tangent_sums(const TangentOut& o, int64_t first, int64_t count, int64_t N, cudaStream_t s);
 int dPdF_blocks(int64_t count);
 template <int NS>
 cudaError_t launch_tangent_pick(const PhaseConst<NS>& pc, const Fields& f, double dt, const long long* idx, double* out,
