@@ -297,3 +297,16 @@ def test_numerics_options(gpu, oracle_lib, option):
     for name in ('P', 'F', 'xi_sl'):
         assert rel(g.get_field(name), o.get_field(name)) < TOL, name
     g.close()
+
+
+@pytest.mark.parametrize('cells', [(64, 32, 64), (64, 64, 48)])
+def test_two_and_three_voxel_chunks(gpu, oracle_lib, cells):
+    """Contexts of 2^17 and 3 * 2^16 voxels split their constitutive passes into two and three
+    chunks on their own streams; results as the oracle's."""
+    g, o = pair(oracle_lib, cells, 30, seed=6)
+    sg, so = run_both(g, o, 1)
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    assert rel(sg[0].P_av, so[0].P_av) < TOL
+    for name in ('P', 'xi_sl', 'gamma_sl'):
+        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    g.close()
