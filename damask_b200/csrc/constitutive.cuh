@@ -474,7 +474,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         const double* L1 = dot_gen(w, c.it + 1, NST, N) + v;
         double* L2 = dot_gen(w, c.it, NST, N) + v;
         double d01 = 0.0, d12 = 0.0, d22 = 0.0;
-#pragma unroll 12
+#pragma unroll 24
         for (int i = 0; i < NST; ++i) {
           const double d = xs[i * PASS_THREADS];
           const double l1 = L1[i * N];                                 // dotState_last(:,1)
