@@ -1,14 +1,16 @@
-"""Host side of the grid mechanical solver: the plugin object and the increment loop.
+"""Host side of the grid mechanical solver: the plugin objects and the increment loop.
 
 ``SpectralBasic`` mirrors the five procedures DAMASK's grid driver selects for the
 ``spectral_basic`` solver (``src/grid/DAMASK_grid.f90:110-119,171-206``):
 ``init`` (constructor), ``forward``, ``solution``, ``update_coords`` and the
-materialpoint forward that follows a converged increment.  All compute runs in
-``libdamask_b200.so`` on the GPU; this module only marshals host arrays.
+materialpoint forward that follows a converged increment; ``SpectralPolarization`` the
+same for ``spectral_polarization``.  All compute runs in ``libdamask_b200.so`` on the
+GPU; this module only marshals host arrays.
 
 ``run_load_cases`` restates the driver's increment loop with its global cutback
 (``DAMASK_grid.f90:288-460``) for any object with that interface, so the same
-host logic drives the CUDA path and, in tests, the CPU oracle.
+host logic drives the CUDA path and, in tests, the CPU oracle;
+``run_load_cases_native`` runs the library's C++ version of that loop.
 """
 from __future__ import annotations
 
