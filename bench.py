@@ -395,6 +395,7 @@ def main():
                    'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
                    'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
         'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
+        's_per_increment': {'mixed': ms_max / args.steps * 1e-3, 'fp64': fp_ms / args.steps * 1e-3},
         'mixed_over_fp64': value / fp_value,
         'mixed_vs_fp64_P_av_rel_err_max': max(rel) if rel else None,
         'roofline': {'bound': 'hbm', 'kernel': 'constitutive update (begin + stress/control pass kernels), one '
