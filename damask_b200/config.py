@@ -107,6 +107,8 @@ def loadstep_structs(loadcases) -> C.Array:
 
 LATTICES = {'cF': 0, 'cI': 1}
 SOLVERS = {'spectral_basic': 0, 'spectral_polarization': 1}
+# solver.grid.FFT.derivative (spectral_utilities.f90:198-209)
+DERIVATIVES = {'continuous': 0, 'central_difference': 1, 'FWBW_difference': 2}
 BC_TYPES = {'L': 1, 'dot_F': 2, 'F_dot': 2, 'F': 3, 'P': 4, 'dot_P': 5, 'P_dot': 5}
 
 
@@ -298,7 +300,7 @@ class Numerics:
         if self.N_iter_min > self.N_iter_max or self.N_iter_min < 1: bad.append('N_iter_min')
         if self.N_iter_Lp_max < 1: bad.append('N_iter_Lp_max')
         if self.N_iter_state_max < 1: bad.append('N_iter_state_max')
-        if self.derivative not in ('continuous', 'central_difference'): bad.append('derivative')
+        if self.derivative not in DERIVATIVES: bad.append('derivative')
         if not 1 <= self.anderson_m <= 32: bad.append('anderson_m')
         if self.solver not in SOLVERS: bad.append('solver')
         if self.solver == 'spectral_polarization':
@@ -318,7 +320,7 @@ class Numerics:
         s.eps_abs_P, s.eps_rel_P = self.eps_abs_P, self.eps_rel_P
         s.update_gamma = int(bool(self.update_gamma))
         s.divergence_correction = {'none': 0, 'size': 1, 'grid+size': 2, 'size+grid': 2}[self.divergence_correction]
-        s.derivative = {'continuous': 0, 'central_difference': 1}[self.derivative]
+        s.derivative = DERIVATIVES[self.derivative]
         s.r_cutback_min, s.r_cutback, s.r_increase = self.r_cutback_min, self.r_cutback, self.r_increase
         s.eps_rel_state, s.N_iter_state_max = self.eps_rel_state, int(self.N_iter_state_max)
         s.N_iter_Lp_max, s.r_linesearch_Lp = int(self.N_iter_Lp_max), self.r_linesearch_Lp

@@ -846,8 +846,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   for (int i = 0; i < 3; ++i)
     if (cells[i] < 1 || !(geomSize[i] > 0.0)) return fail(DMK_ERR_ARG, "cells and geomSize must be positive");
   if (precision != DMK_PRECISION_FP64 && precision != DMK_PRECISION_MIXED) return fail(DMK_ERR_ARG, "unknown precision");
-  if (num->derivative != 0 && num->derivative != 1)
-    return fail(DMK_ERR_CONFIG, "spectral derivative must be continuous (0) or central_difference (1)");
+  if (num->derivative < 0 || num->derivative > 2)
+    return fail(DMK_ERR_CONFIG, "spectral derivative must be continuous (0), central_difference (1) or FWBW_difference (2)");
   if (num->N_iter_max < 1 || num->N_iter_min < 1 || num->N_iter_min > num->N_iter_max)
     return fail(DMK_ERR_CONFIG, "invalid N_iter_min/N_iter_max");
   if (num->N_iter_Lp_max < 1 || num->N_iter_state_max < 1 || num->f_update_jacobi_Lp < 1 || !(num->r_cutback > 0.0) ||

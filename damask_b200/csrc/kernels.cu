@@ -285,13 +285,192 @@ gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2,
   }
 }
 
+// Gamma and divergence with the complex FWBW frequencies (spectral_utilities.f90:356-395,
+// :436-501, :650-691).  With K(l,m) = sum_jn C_ref(l,j,m,n) conj(xi_j) xi_n the reference's
+// A = C_ref : (conj(-xi) (x) xi) is -K, and Gamma_hat : P_hat = K^-1 (P_hat conj(xi)) (x) xi; the
+// reference inverts K through its 6x6 real embedding, here K^-1 = adj(K) / det(K) in complex
+// arithmetic.  Points with |det Re K| <= 1e-16 are zero; k = 0 receives the aim.  The divergence
+// term is |P_hat conj(-xi) rescale|^2 with the same plane weights as gamma_div_kernel.
+template <typename Real>
+__global__ void __launch_bounds__(SPEC_THREADS)
+gamma_div_fwbw_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                      const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
+                      double* __restrict__ div_partials, int do_gamma, int do_div) {
+  __shared__ double red[SPEC_THREADS / 32];
+  using C2 = typename std::conditional<sizeof(Real) == 8, double2, float2>::type;
+  C2* S = reinterpret_cast<C2*>(spec);
+  const int red0 = n0 / 2 + 1;
+  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  double dsum = 0.0;
+  if (idx < plane) {
+    const int kx = int(idx % red0);
+    const int64_t rest = idx / red0;
+    const int ky = int(rest % n1);
+    const int kz = int(rest / n1);
+    const int ks[3] = {kx, ky > n1 / 2 ? ky - n1 : ky, kz > n2 / 2 ? kz - n2 : kz};
+    const int nn[3] = {n0, n1, n2};
+    const double LL[3] = {L0, L1, L2};
+    double xr[3], xm[3];
+    freq_fwbw(ks, nn, LL, xr, xm);
+    double pr[9], pi[9];
+#pragma unroll
+    for (int c = 0; c < 9; ++c) {
+      const C2 z = S[c * plane + idx];
+      pr[c] = double(z.x);
+      pi[c] = double(z.y);
+    }
+    if (do_div) {
+      double s = 0.0;
+#pragma unroll
+      for (int l = 0; l < 3; ++l) {
+        double vr = 0.0, vi = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+          // conj(-xi) rescale = (-xr + i xm) g
+          const double wr = -xr[m] * gc.rescale[m], wi = xm[m] * gc.rescale[m];
+          vr += pr[l + 3 * m] * wr - pi[l + 3 * m] * wi;
+          vi += pr[l + 3 * m] * wi + pi[l + 3 * m] * wr;
+        }
+        s += vr * vr + vi * vi;
+      }
+      const double weight = ((kx >= 1 && kx < red0 - 1) || red0 == 1) ? 2.0 : 1.0;
+      dsum = weight * s;
+    }
+    if (do_gamma) {
+      double rr[9], ri[9];
+      if (kx == 0 && ky == 0 && kz == 0) {
+#pragma unroll
+        for (int c = 0; c < 9; ++c) { rr[c] = sc->aim_rot[c]; ri[c] = 0.0; }
+      } else {
+        // d(j,n) = conj(xi_j) xi_n; K(l,m) = sum_jn Cref(l,j,m,n) d(j,n)
+        double dr[9], di[9];
+#pragma unroll
+        for (int n = 0; n < 3; ++n)
+#pragma unroll
+          for (int j = 0; j < 3; ++j) {
+            dr[j + 3 * n] = xr[j] * xr[n] + xm[j] * xm[n];
+            di[j + 3 * n] = xr[j] * xm[n] - xm[j] * xr[n];
+          }
+        double Kr[9], Ki[9];
+#pragma unroll
+        for (int m = 0; m < 3; ++m)
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            double sr = 0.0, si = 0.0;
+#pragma unroll
+            for (int n = 0; n < 3; ++n)
+#pragma unroll
+              for (int j = 0; j < 3; ++j) {
+                const double cc = gc.Cref[l + 3 * j + 9 * m + 27 * n];
+                sr = fma(cc, dr[j + 3 * n], sr);
+                si = fma(cc, di[j + 3 * n], si);
+              }
+            Kr[l + 3 * m] = sr;
+            Ki[l + 3 * m] = si;
+          }
+        if (fabs(det33(Kr)) > 1.0e-16) {
+          // complex cofactors: adj(l,m) = cof(m,l)
+          auto cm = [](double ar, double ai, double br, double bi, double& r, double& i) {
+            r = ar * br - ai * bi;
+            i = ar * bi + ai * br;
+          };
+          // K[a] K[d] - K[b] K[c] for column-major K[r + 3 c] = m_rc
+          auto det2 = [&](int a, int d, int b, int c, double& r, double& i) {
+            double r1, i1, r2, i2;
+            cm(Kr[a], Ki[a], Kr[d], Ki[d], r1, i1);
+            cm(Kr[b], Ki[b], Kr[c], Ki[c], r2, i2);
+            r = r1 - r2;
+            i = i1 - i2;
+          };
+          // adjugate, column-major A[l + 3 m] = adj(l, m)
+          double Ar[9], Ai[9];
+          det2(4, 8, 7, 5, Ar[0], Ai[0]);        // m11 m22 - m12 m21
+          det2(7, 2, 1, 8, Ar[1], Ai[1]);        // m12 m20 - m10 m22
+          det2(1, 5, 4, 2, Ar[2], Ai[2]);        // m10 m21 - m11 m20
+          det2(6, 5, 3, 8, Ar[3], Ai[3]);        // m02 m21 - m01 m22
+          det2(0, 8, 6, 2, Ar[4], Ai[4]);        // m00 m22 - m02 m20
+          det2(3, 2, 0, 5, Ar[5], Ai[5]);        // m01 m20 - m00 m21
+          det2(3, 7, 6, 4, Ar[6], Ai[6]);        // m01 m12 - m02 m11
+          det2(6, 1, 0, 7, Ar[7], Ai[7]);        // m02 m10 - m00 m12
+          det2(0, 4, 3, 1, Ar[8], Ai[8]);        // m00 m11 - m01 m10
+          // det = sum_m K(0,m) adj(m,0)
+          double detr = 0.0, deti = 0.0;
+#pragma unroll
+          for (int m = 0; m < 3; ++m) {
+            double r, i;
+            cm(Kr[3 * m], Ki[3 * m], Ar[m], Ai[m], r, i);
+            detr += r;
+            deti += i;
+          }
+          const double id2 = 1.0 / (detr * detr + deti * deti);
+          const double idr = detr * id2, idi = -deti * id2;    // 1 / det
+          // v = P_hat conj(xi); u = adj v / det
+          double vr[3], vi[3];
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            vr[l] = 0.0;
+            vi[l] = 0.0;
+#pragma unroll
+            for (int o = 0; o < 3; ++o) {
+              vr[l] += pr[l + 3 * o] * xr[o] + pi[l + 3 * o] * xm[o];
+              vi[l] += pi[l + 3 * o] * xr[o] - pr[l + 3 * o] * xm[o];
+            }
+          }
+          double ur[3], ui[3];
+#pragma unroll
+          for (int l = 0; l < 3; ++l) {
+            double sr = 0.0, si = 0.0;
+#pragma unroll
+            for (int n = 0; n < 3; ++n) {
+              double r, i;
+              cm(Ar[l + 3 * n], Ai[l + 3 * n], vr[n], vi[n], r, i);
+              sr += r;
+              si += i;
+            }
+            cm(sr, si, idr, idi, ur[l], ui[l]);
+          }
+#pragma unroll
+          for (int m = 0; m < 3; ++m)
+#pragma unroll
+            for (int l = 0; l < 3; ++l) cm(ur[l], ui[l], xr[m], xm[m], rr[l + 3 * m], ri[l + 3 * m]);
+        } else {
+#pragma unroll
+          for (int c = 0; c < 9; ++c) { rr[c] = 0.0; ri[c] = 0.0; }
+        }
+      }
+#pragma unroll
+      for (int c = 0; c < 9; ++c) {
+        C2 z;
+        z.x = Real(rr[c]);
+        z.y = Real(ri[c]);
+        S[c * plane + idx] = z;
+      }
+    }
+  }
+  if (do_div) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dsum += __shfl_down_sync(0xffffffffu, dsum, o);
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = dsum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      double s = 0.0;
+      for (int w = 0; w < SPEC_THREADS / 32; ++w) s += red[w];
+      div_partials[blockIdx.x] = s;
+    }
+  }
+}
+
 template <typename Real>
 cudaError_t launch_gamma_div(Real* spec, int n0, int n1, int n2, const double L[3], const GammaConst& gc,
                              const SolverScalars* sc, double* div_partials, int do_gamma, int do_div, cudaStream_t s) {
   const int64_t plane = int64_t(n0 / 2 + 1) * n1 * n2;
   const int nb = int((plane + SPEC_THREADS - 1) / SPEC_THREADS);
-  gamma_div_kernel<Real><<<nb, SPEC_THREADS, 0, s>>>(spec, plane, n0, n1, n2, L[0], L[1], L[2], gc, sc, div_partials,
-                                                     do_gamma, do_div);
+  if (gc.derivative == 2)
+    gamma_div_fwbw_kernel<Real><<<nb, SPEC_THREADS, 0, s>>>(spec, plane, n0, n1, n2, L[0], L[1], L[2], gc, sc,
+                                                            div_partials, do_gamma, do_div);
+  else
+    gamma_div_kernel<Real><<<nb, SPEC_THREADS, 0, s>>>(spec, plane, n0, n1, n2, L[0], L[1], L[2], gc, sc,
+                                                       div_partials, do_gamma, do_div);
   return cudaGetLastError();
 }
 template cudaError_t launch_gamma_div<double>(double*, int, int, int, const double*, const GammaConst&, const SolverScalars*,
@@ -680,7 +859,8 @@ namespace dmk {
 // utilities_updateCoords (spectral_utilities.f90:857-968).  Fourier part: with the
 // second-derivative frequencies xi = i a, a = 2 pi k / L (Nyquist kept, :315-333),
 // u_hat = F_hat xi / (conj(-xi) . xi) = -i (F_hat a) / |a|^2 per stored point, written to
-// planes 0..2 of the spectrum; k = 0 gives 0 and the average F = Re F_hat(0) wgt.
+// planes 0..2 of the spectrum; k = 0 gives 0 and the average F = Re F_hat(0) wgt.  With the
+// complex FWBW frequencies the same quotient is formed in complex arithmetic.
 __global__ void __launch_bounds__(SPEC_THREADS)
 coords_spec_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
                    double wgt, double* __restrict__ favg, int derivative) {
@@ -702,6 +882,26 @@ coords_spec_kernel(double2* __restrict__ S, int64_t plane, int n0, int n1, int n
     for (int c = 0; c < 9; ++c) favg[c] = F[c].x * wgt;
 #pragma unroll
     for (int l = 0; l < 3; ++l) S[l * plane] = make_double2(0.0, 0.0);
+    return;
+  }
+  if (derivative == 2) {
+    // complex xi2nd = xr + i xm: u_hat = F_hat xi / (-|xi|^2)
+    const int ks[3] = {kx, ky > n1 / 2 ? ky - n1 : ky, kz > n2 / 2 ? kz - n2 : kz};
+    const int nn[3] = {n0, n1, n2};
+    const double LL[3] = {L0, L1, L2};
+    double xr[3], xm[3];
+    freq_fwbw(ks, nn, LL, xr, xm);
+    const double den = -(xr[0] * xr[0] + xm[0] * xm[0] + xr[1] * xr[1] + xm[1] * xm[1] + xr[2] * xr[2] + xm[2] * xm[2]);
+#pragma unroll
+    for (int l = 0; l < 3; ++l) {
+      double sr = 0.0, si = 0.0;
+#pragma unroll
+      for (int m = 0; m < 3; ++m) {
+        sr += F[l + 3 * m].x * xr[m] - F[l + 3 * m].y * xm[m];
+        si += F[l + 3 * m].x * xm[m] + F[l + 3 * m].y * xr[m];
+      }
+      S[l * plane + idx] = make_double2(sr / den, si / den);
+    }
     return;
   }
   const double a2 = a[0] * a[0] + a[1] * a[1] + a[2] * a[2];

@@ -29,7 +29,7 @@ struct SolverScalars {
 struct GammaConst {
   double Cref[81];       // C_ref = C / wgt, column-major 3x3x3x3
   double rescale[3];     // geomSize / scaledGeomSize
-  int derivative;        // 0 continuous, 1 central difference
+  int derivative;        // 0 continuous, 1 central difference, 2 FWBW difference
 };
 
 // Imaginary part a of the spectral derivative xi = i a for signed frequency k of an edge of n
@@ -42,6 +42,33 @@ __device__ __forceinline__ double freq_derivative(int k, int n, double L, int de
   if (derivative == 1) return sin(TAU * double(k) / double(n)) / (2.0 * L / double(n));
   if (first_order && n % 2 == 0 && k == n / 2) return 0.0;
   return TAU * double(k) / L;
+}
+
+// FWBW_difference (utilities_getFreqDerivative, spectral_utilities.f90:823-849): the complex
+// frequencies xi_d = (e^{i t_d} - 1) prod_{e != d} (e^{i t_e} + 1) / (4 L_d / n_d), t_e = 2 pi k_e / n_e,
+// for the signed indices k; the factors multiply in the order e = 1, 2, 3.  xi1st = xi2nd here.
+// In real space xi_d is the forward difference along d averaged over the four edges of the
+// staggered cell, so xi(-k) = conj(xi(k)) and the operators built on it keep spectra Hermitian.
+__device__ __forceinline__ void freq_fwbw(const int k[3], const int n[3], const double L[3], double xr[3],
+                                          double xim[3]) {
+  const double TAU = 6.283185307179586;
+  double c[3], s[3];
+#pragma unroll
+  for (int e = 0; e < 3; ++e) sincos(TAU * double(k[e]) / double(n[e]), &s[e], &c[e]);
+#pragma unroll
+  for (int d = 0; d < 3; ++d) {
+    double pr = 1.0, pi = 0.0;
+#pragma unroll
+    for (int e = 0; e < 3; ++e) {
+      const double fr = c[e] + (e == d ? -1.0 : 1.0), fi = s[e];
+      const double t = pr * fr - pi * fi;
+      pi = pr * fi + pi * fr;
+      pr = t;
+    }
+    const double h4 = 4.0 * L[d] / double(n[d]);
+    xr[d] = pr / h4;
+    xim[d] = pi / h4;
+  }
 }
 
 struct Numerics2 {

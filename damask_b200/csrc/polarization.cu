@@ -143,16 +143,30 @@ curl_kernel(const double2* __restrict__ S, int64_t plane, int n0, int n1, int n2
     const int kz = int(rest / n1);
     const int sy = ky > n1 / 2 ? ky - n1 : ky;
     const int sz = kz > n2 / 2 ? kz - n2 : kz;
-    // xi1st * rescaledGeom = i w
-    double w[3];
-    w[0] = freq_derivative(kx, n0, L0, derivative, true) * rg0;
-    w[1] = freq_derivative(sy, n1, L1, derivative, true) * rg1;
-    w[2] = freq_derivative(sz, n2, L2, derivative, true) * rg2;
-    // (x + i y) (i w) = -y w + i x w
+    // xi1st * rescaledGeom = wr + i wi (continuous and central difference: wr = 0)
+    double wr[3] = {0.0, 0.0, 0.0}, wi[3];
+    if (derivative == 2) {
+      const int ks[3] = {kx, sy, sz};
+      const int nn[3] = {n0, n1, n2};
+      const double LL[3] = {L0, L1, L2};
+      freq_fwbw(ks, nn, LL, wr, wi);
+      wr[0] *= rg0; wr[1] *= rg1; wr[2] *= rg2;
+      wi[0] *= rg0; wi[1] *= rg1; wi[2] *= rg2;
+    } else {
+      wi[0] = freq_derivative(kx, n0, L0, derivative, true) * rg0;
+      wi[1] = freq_derivative(sy, n1, L1, derivative, true) * rg1;
+      wi[2] = freq_derivative(sz, n2, L2, derivative, true) * rg2;
+    }
+    // a w[d1] - b w[d2]; with wr = 0: (x + i y) (i w) = -y w + i x w
     auto term = [&](int c1, int d1, int c2, int d2, double& re, double& im) {
       const double2 a = S[c1 * plane + idx], b = S[c2 * plane + idx];
-      re = -a.y * w[d1] + b.y * w[d2];
-      im = a.x * w[d1] - b.x * w[d2];
+      if (derivative == 2) {
+        re = (a.x * wr[d1] - a.y * wi[d1]) - (b.x * wr[d2] - b.y * wi[d2]);
+        im = (a.x * wi[d1] + a.y * wr[d1]) - (b.x * wi[d2] + b.y * wr[d2]);
+      } else {
+        re = -a.y * wi[d1] + b.y * wi[d2];
+        im = a.x * wi[d1] - b.x * wi[d2];
+      }
     };
     if (kx >= 1 && kx < red0 - 1) {
       double s = 0.0;

@@ -78,7 +78,7 @@ typedef struct {
   double eps_abs_div, eps_rel_div, eps_abs_P, eps_rel_P;
   int update_gamma;
   int divergence_correction;   /* 0 none, 1 size, 2 grid+size */
-  int derivative;              /* 0 continuous, 1 central_difference (utilities_getFreqDerivative) */
+  int derivative;              /* 0 continuous, 1 central_difference, 2 FWBW_difference (utilities_getFreqDerivative) */
   double r_cutback_min, r_cutback, r_increase, eps_rel_state;
   int N_iter_state_max;
   int N_iter_Lp_max;

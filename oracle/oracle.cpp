@@ -467,7 +467,7 @@ struct orc_ctx {
   // spectral
   int red;                        // cells1/2+1
   double scaledGeomSize[3];
-  std::vector<double> xi;         // 3 per Fourier point (imaginary part of xi1st), index ((z*n1+y)*red+x)
+  std::vector<cd> xi;             // xi1st, 3 per Fourier point, index ((z*n1+y)*red+x)
   T4 C_ref;
   std::vector<cd> work;           // full complex workspace, 9 components
   std::vector<double> xp, xn;     // discretization_IPcoords / _NodeCoords, 3 per point
@@ -909,12 +909,22 @@ int constitutive_response(orc_ctx* c, double dt, bool rotate) {
 // ---------------------------------------------------------------- spectral
 inline long fidx(const orc_ctx* c, int x, int y, int z) { return (long(z) * c->cells[1] + y) * c->red + x; }
 
-// utilities_getFreqDerivative, spectral_utilities.f90:808-850: imaginary part of the derivative of
-// frequency k along d (continuous 2 pi k / L; central difference sin(2 pi k / n) / (2 L / n))
-double freq_derivative(const orc_ctx* c, int k, int d) {
+// utilities_getFreqDerivative, spectral_utilities.f90:808-850: component d of the derivative
+// frequency of the signed index triple ks.  continuous: i 2 pi k_d / L_d; central difference:
+// i sin(2 pi k_d / n_d) / (2 L_d / n_d); FWBW difference: (e^{i t_d} - 1) times (e^{i t_e} + 1)
+// for the other two directions e, over 4 L_d / n_d, with t = 2 pi k / n (factors in the order 1, 2, 3).
+cd freq_derivative(const orc_ctx* c, const int ks[3], int d) {
   if (c->num.derivative == 1)
-    return std::sin(TAU * double(k) / double(c->cells[d])) / (2.0 * c->geomSize[d] / double(c->cells[d]));
-  return TAU * double(k) / c->geomSize[d];
+    return cd(0.0, std::sin(TAU * double(ks[d]) / double(c->cells[d])) / (2.0 * c->geomSize[d] / double(c->cells[d])));
+  if (c->num.derivative == 2) {
+    cd p(1.0, 0.0);
+    for (int e = 0; e < 3; ++e) {
+      const double t = TAU * double(ks[e]) / double(c->cells[e]);
+      p = p * cd(std::cos(t) + (e == d ? -1.0 : 1.0), std::sin(t));
+    }
+    return p / (4.0 * c->geomSize[d] / double(c->cells[d]));
+  }
+  return cd(0.0, TAU * double(ks[d]) / c->geomSize[d]);
 }
 
 void spectral_init(orc_ctx* c) {
@@ -934,14 +944,14 @@ void spectral_init(orc_ctx* c) {
   } else {
     for (int i = 0; i < 3; ++i) c->scaledGeomSize[i] = g[i];
   }
-  // xi1st, spectral_utilities.f90:315-333 and :808-850 (imaginary part; continuous: Nyquist
-  // zeroed on even edges, central difference: as xi2nd)
-  c->xi.assign(size_t(c->red) * n[1] * n[2] * 3, 0.0);
+  // xi1st, spectral_utilities.f90:315-333 and :808-850 (continuous: Nyquist zeroed on even
+  // edges; the difference schemes: as xi2nd)
+  c->xi.assign(size_t(c->red) * n[1] * n[2] * 3, cd(0.0, 0.0));
   for (int z = 0; z < n[2]; ++z) for (int y = 0; y < n[1]; ++y) for (int x = 0; x < c->red; ++x) {
     int ks[3] = {x, y > n[1] / 2 ? y - n[1] : y, z > n[2] / 2 ? z - n[2] : z};
     int idx[3] = {x, y, z};
     for (int d = 0; d < 3; ++d) {
-      double v = freq_derivative(c, ks[d], d);
+      cd v = freq_derivative(c, ks, d);
       if (c->num.derivative == 0 && n[d] % 2 == 0 && idx[d] == n[d] / 2) v = 0.0;
       c->xi[fidx(c, x, y, z) * 3 + d] = v;
     }
@@ -973,9 +983,9 @@ double divergence_rms(orc_ctx* c) {
   const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
   const double rg[3] = {c->geomSize[0] / c->scaledGeomSize[0], c->geomSize[1] / c->scaledGeomSize[1], c->geomSize[2] / c->scaledGeomSize[2]};
   auto term = [&](int x, int y, int z) {
-    const double* xv = &c->xi[fidx(c, x, y, z) * 3];
+    const cd* xv = &c->xi[fidx(c, x, y, z) * 3];
     cd w[3];
-    for (int m = 0; m < 3; ++m) w[m] = std::conj(-cd(0.0, xv[m])) * cd(rg[m], 0.0);
+    for (int m = 0; m < 3; ++m) w[m] = std::conj(-xv[m]) * cd(rg[m], 0.0);
     double sr = 0.0, si = 0.0;
     cd v[3];
     for (int l = 0; l < 3; ++l) { cd s = 0.0; for (int m = 0; m < 3; ++m) s += spec(c, l + 3 * m, x, y, z) * w[m]; v[l] = s; }
@@ -1024,9 +1034,9 @@ void gamma_convolution(orc_ctx* c, M3* field, const M3& aim) {
     if (x == 0 && y == 0 && z == 0) {
       for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) R[i][j] = cd(aim.a[i][j], 0.0);
     } else {
-      const double* xv = &c->xi[f * 3];
+      const cd* xv = &c->xi[f * 3];
       cd xd[3][3];
-      for (int l = 0; l < 3; ++l) for (int m = 0; m < 3; ++m) xd[l][m] = std::conj(-cd(0.0, xv[l])) * cd(0.0, xv[m]);
+      for (int l = 0; l < 3; ++l) for (int m = 0; m < 3; ++m) xd[l][m] = std::conj(-xv[l]) * xv[m];
       cd t[3][3];
       for (int l = 0; l < 3; ++l) for (int m = 0; m < 3; ++m) {
         cd s = 0.0;
@@ -1081,7 +1091,7 @@ void update_coords(orc_ctx* c) {
     if (x == 0 && y == 0 && z == 0) { for (int l = 0; l < 3; ++l) half[l * H + f] = 0.0; continue; }
     int ks[3] = {x, y > n1 / 2 ? y - n1 : y, z > n2 / 2 ? z - n2 : z};
     cd xi2[3];
-    for (int d = 0; d < 3; ++d) xi2[d] = cd(0.0, freq_derivative(c, ks[d], d));   // no Nyquist zeroing
+    for (int d = 0; d < 3; ++d) xi2[d] = freq_derivative(c, ks, d);   // no Nyquist zeroing
     cd den = 0.0;
     for (int d = 0; d < 3; ++d) den += std::conj(-xi2[d]) * xi2[d];
     for (int l = 0; l < 3; ++l) {
@@ -1188,7 +1198,7 @@ double curl_rms(orc_ctx* c) {
   const int n0 = c->cells[0], n1 = c->cells[1], n2 = c->cells[2];
   const double rg[3] = {c->geomSize[0] / c->scaledGeomSize[0], c->geomSize[1] / c->scaledGeomSize[1],
                         c->geomSize[2] / c->scaledGeomSize[2]};
-  auto xi = [&](int x, int y, int z, int d) { return cd(0.0, c->xi[fidx(c, x, y, z) * 3 + d]) * cd(rg[d], 0.0); };
+  auto xi = [&](int x, int y, int z, int d) { return c->xi[fidx(c, x, y, z) * 3 + d] * cd(rg[d], 0.0); };
   auto T = [&](int l, int m, int x, int y, int z) { return spec(c, l + 3 * m, x, y, z); };
   double res = 0.0;
   for (int y = 0; y < n1; ++y) for (int z = 0; z < n2; ++z) {

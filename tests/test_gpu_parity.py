@@ -278,15 +278,15 @@ def test_fp64_peak_probe(gpu):
 
 
 @pytest.mark.parametrize('option', ['update_gamma', 'divergence_correction_none', 'divergence_correction_size',
-                                    'central_difference'])
+                                    'central_difference', 'FWBW_difference'])
 def test_numerics_options(gpu, oracle_lib, option):
     """update_gamma (Gamma re-based on C_minMaxAvg every solution, spectral_utilities.f90:356-395)
     and the divergence_correction modes (scaledGeomSize, :181-197) on a non-cubic RVE."""
     num = workloads.numerics_default()
     if option == 'update_gamma':
         num.update_gamma = True
-    elif option == 'central_difference':
-        num.derivative = 'central_difference'      # utilities_getFreqDerivative, :808-850
+    elif option in ('central_difference', 'FWBW_difference'):
+        num.derivative = option                    # utilities_getFreqDerivative, :808-850
     else:
         num.divergence_correction = option.split('_')[-1]
     g, o = pair(oracle_lib, (8, 6, 10), 6, seed=5, num=num, size=(1.0e-3, 0.75e-3, 1.25e-3))
@@ -296,6 +296,32 @@ def test_numerics_options(gpu, oracle_lib, option):
         assert rel(a.P_av, b.P_av) < TOL
     for name in ('P', 'F', 'xi_sl'):
         assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+    g.close()
+
+
+@pytest.mark.parametrize('cells', [(5, 6, 7), (6, 4, 8), (1, 6, 5), (5, 7, 3)])
+def test_fwbw_spectral_operators(gpu, oracle_lib, cells):
+    """The complex FWBW frequencies (spectral_utilities.f90:823-849) in every spectral operator:
+    divergence RMS, Gamma convolution (complex inverse of the acoustic tensor), curl RMS and, on
+    grids without a Nyquist index (even edges give near-zero |xi|^2 at points other than k = 0),
+    the coordinate update."""
+    num = workloads.numerics_default()
+    num.derivative = 'FWBW_difference'
+    size = (1.0e-3, 0.8e-3, 1.2e-3)
+    g, o = pair(oracle_lib, cells, 3, num=num, size=size)
+    rng = np.random.default_rng(21)
+    P = rng.normal(size=(g.N, 9)) * 1e8
+    aim = rng.normal(size=9)
+    assert rel(g.divergence_rms(P), o.divergence_rms(P)) < 1e-12
+    assert rel(g.gamma_convolution(P, aim), o.gamma_convolution(P, aim)) < 1e-12
+    F = np.tile(np.eye(3).reshape(-1), (g.N, 1)) + 0.05 * rng.normal(size=(g.N, 9))
+    assert rel(g.curl_rms(F), o.curl_rms(F)) < 1e-12
+    if all(n % 2 == 1 for n in cells):
+        for s in (g, o):
+            s.set_field('F_solver', F)
+            s.update_coords()
+        for a, b in zip(g.get_coords(), o.get_coords()):
+            assert rel(a, b) < 1e-12
     g.close()
 
 

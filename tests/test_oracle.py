@@ -49,14 +49,14 @@ def numerics_with(derivative):
     return n
 
 
-@pytest.mark.parametrize('derivative', ['continuous', 'central_difference'])
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference', 'FWBW_difference'])
 def test_divergence_of_constant_field_vanishes(oracle_lib, derivative):
     o = small_oracle(oracle_lib, cells=(5, 4, 6), init=False, num=numerics_with(derivative))
     P = np.tile(np.random.default_rng(3).normal(size=9) * 1e8, (o.N, 1))
     assert o.divergence_rms(P) < 5e-14 * 1e8
 
 
-@pytest.mark.parametrize('derivative', ['continuous', 'central_difference'])
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference', 'FWBW_difference'])
 def test_gamma_convolution_of_constant_field_is_aim(oracle_lib, derivative):
     o = small_oracle(oracle_lib, cells=(4, 6, 5), num=numerics_with(derivative))
     field = np.tile(np.random.default_rng(4).normal(size=9), (o.N, 1))
@@ -229,4 +229,56 @@ def test_central_difference_divergence_matches_finite_differences(oracle_lib):
     voxels = np.transpose(P, (0, 1, 2, 4, 3)).reshape(cells + (9,)).reshape(-1, 9, order='F')
     rms = np.sqrt(np.mean(np.sum(div ** 2, axis=-1)))
     assert abs(o.divergence_rms(voxels) - rms) < 1e-12 * rms
+    o.close()
+
+
+@pytest.mark.parametrize('cells', [(6, 5, 7), (4, 6, 8)])
+def test_fwbw_divergence_matches_staggered_differences(oracle_lib, cells):
+    """With derivative: FWBW_difference the frequencies are (e^{i t_d} - 1) prod_{e != d} (e^{i t_e} + 1)
+    / (4 L_d / n_d) (spectral_utilities.f90:823-849).  conj(-xi) multiplies the spectrum by the
+    backward difference along d and the sum of the two neighbours along the other directions,
+    so the divergence is the edge-averaged difference sum_j B_j A_e A_f P(:, j) / (4 h_j) on the
+    staggered grid (B x = x(n - 1) - x(n), A x = x(n - 1) + x(n)), and its RMS follows Parseval."""
+    size = (1.0e-3, 0.8e-3, 1.4e-3)
+    num = numerics_with('FWBW_difference')
+    num.divergence_correction = 'size'
+    o = oracle_lib.OracleSpectralBasic(cells, size, np.zeros(int(np.prod(cells))), np.array([[1.0, 0, 0, 0]]),
+                                       workloads.fcc_al(), num, init=False, threads=1)
+    P = np.random.default_rng(11).normal(size=cells + (3, 3))
+    h = np.asarray(size) / np.asarray(cells)
+
+    def back(x, ax):
+        return np.roll(x, 1, axis=ax) - x
+
+    def both(x, ax):
+        return np.roll(x, 1, axis=ax) + x
+
+    div = 0.0
+    for j in range(3):
+        d = back(P[..., :, j], j)
+        for e in range(3):
+            if e != j:
+                d = both(d, e)
+        div = div + d / (4 * h[j])
+    voxels = np.transpose(P, (0, 1, 2, 4, 3)).reshape(cells + (9,)).reshape(-1, 9, order='F')
+    rms = np.sqrt(np.mean(np.sum(div ** 2, axis=-1)))
+    assert abs(o.divergence_rms(voxels) - rms) < 1e-12 * rms
+    o.close()
+
+
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference', 'FWBW_difference'])
+@pytest.mark.parametrize('cells', [(5, 6, 7), (6, 4, 8)])
+def test_gamma_c_gamma_is_gamma(oracle_lib, derivative, cells):
+    """Gamma_hat C_ref Gamma_hat = Gamma_hat point by point for any wave vector (the acoustic
+    tensor K = C_ref : conj(xi) (x) xi cancels against its inverse), so convolving C : Gamma(tau)
+    again reproduces Gamma(tau); with the complex FWBW frequencies this exercises the complex
+    inverse of spectral_utilities.f90:356-395."""
+    o = small_oracle(oracle_lib, cells=cells, num=numerics_with(derivative))
+    C = o.aims()['C_minMaxAvg'].reshape(3, 3, 3, 3, order='F')
+    tau = np.random.default_rng(12).normal(size=(o.N, 9)) * 1e8
+    g1 = o.gamma_convolution(tau, np.zeros(9))
+    H = g1.reshape(-1, 3, 3).transpose(0, 2, 1)                   # [v, i, j]
+    tau2 = np.einsum('ijkl,vkl->vij', C, H).transpose(0, 2, 1).reshape(-1, 9)
+    g2 = o.gamma_convolution(tau2, np.zeros(9))
+    assert rel(g2, g1) < 1e-11
     o.close()

@@ -98,12 +98,13 @@ def test_polarization_numerics_validation():
 
 
 # ------------------------------------------------------------------------------- GPU
-def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres'):
+def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres', derivative='continuous'):
     from damask_b200.grid import SpectralPolarization
     rve = synthetic.voronoi_rve(cells, workloads.SIZE_1MM, grains, seed)
     phase = phase or workloads.fcc_al()
     num = workloads.numerics_default()
     num.solver = 'spectral_polarization'
+    num.derivative = derivative
     if snes == 'nrichardson':
         num.PETSc_options = '-snes_type nrichardson'
     g = SpectralPolarization(rve.cells, rve.size, rve.material, rve.quaternions, phase, num)
@@ -112,13 +113,16 @@ def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres'):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson'])
+@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'fcc9_fwbw'])
 def test_polarization_parity(gpu, oracle_lib, case):
     if case == 'fcc16_anderson':
         g, o = gpu_pair(oracle_lib, (16, 16, 16), 20)
         n = 3
     elif case == 'fcc8_richardson':
         g, o = gpu_pair(oracle_lib, (8, 8, 8), 6, snes='nrichardson')
+        n = 3
+    elif case == 'fcc9_fwbw':
+        g, o = gpu_pair(oracle_lib, (9, 7, 5), 6, seed=2, derivative='FWBW_difference')
         n = 3
     else:
         g, o = gpu_pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_24())
