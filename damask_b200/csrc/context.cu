@@ -699,8 +699,9 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
     CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, 1, 0,
                                 c->stream));
     ++c->launches;
-    CKF(cufftExecZ2D(c->plan_bwd, spec, rtau));
-    CKL(launch_pol_tau(c->Fsol, rtau, N, beta, c->Feval, c->stream));
+    // the transform writes to Feval: rtau = r + 9N is only 8-byte aligned for odd N, which cuFFT rejects
+    CKF(cufftExecZ2D(c->plan_bwd, spec, c->Feval));
+    CKL(launch_pol_tau(c->Fsol, c->Feval, rtau, N, beta, c->Feval, c->stream));
     CKF(cufftExecD2Z(c->plan_fwd, c->Fsol, spec));                      // curl of F
     CKL(launch_curl(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc.rescale, c->gc.derivative,
                     c->curl_partials, c->stream));

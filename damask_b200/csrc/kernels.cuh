@@ -117,7 +117,8 @@ struct PolConst {
 };
 cudaError_t launch_pol_pre(const double* F, const double* Ftau, int64_t N, const PolConst& pc, double* out,
                            cudaStream_t s);
-cudaError_t launch_pol_tau(const double* F, double* G, int64_t N, double beta, double* Feval, cudaStream_t s);
+cudaError_t launch_pol_tau(const double* F, const double* G, double* rtau, int64_t N, double beta, double* Feval,
+                           cudaStream_t s);
 cudaError_t launch_pol_rF(const double* F, const double* Ftau, const double* P, const double* dPdF, const double* rtau,
                           int64_t N, const PolConst& pc, double* rF, cudaStream_t s);
 cudaError_t launch_curl(const double* spec, int n0, int n1, int n2, const double L[3], const double rg[3],

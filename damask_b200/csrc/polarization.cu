@@ -66,15 +66,16 @@ __global__ void pol_pre_kernel(const double* __restrict__ F, const double* __res
   for (int k = 0; k < 9; ++k) out[k * N + v] = pc.beta * t1[k] - pc.alpha * t2[k];
 }
 
-// r_F_tau = beta F - Gamma(...) (in place on the convolution result G) and the deformation
-// gradient of the constitutive evaluation, F - r_F_tau / beta (:591, :596-604)
-__global__ void pol_tau_kernel(const double* __restrict__ F, double* __restrict__ G, int64_t N, double beta,
-                               double* __restrict__ Feval) {
+// r_F_tau = beta F - Gamma(...) from the convolution result G and the deformation gradient of
+// the constitutive evaluation, F - r_F_tau / beta (:591, :596-604).  G may be Feval itself (each
+// element is read before it is overwritten by the same thread).
+__global__ void pol_tau_kernel(const double* __restrict__ F, const double* G, double* __restrict__ rtau, int64_t N,
+                               double beta, double* Feval) {
   const int64_t i = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   if (i >= 9 * N) return;
   const double f = F[i];
   const double r = beta * f - G[i];
-  G[i] = r;
+  rtau[i] = r;
   Feval[i] = f - r / beta;
 }
 
@@ -259,8 +260,9 @@ cudaError_t launch_pol_pre(const double* F, const double* Ftau, int64_t N, const
   pol_pre_kernel<<<unsigned((N + 127) / 128), 128, 0, s>>>(F, Ftau, N, pc, out);
   return cudaGetLastError();
 }
-cudaError_t launch_pol_tau(const double* F, double* G, int64_t N, double beta, double* Feval, cudaStream_t s) {
-  pol_tau_kernel<<<unsigned((9 * N + 255) / 256), 256, 0, s>>>(F, G, N, beta, Feval);
+cudaError_t launch_pol_tau(const double* F, const double* G, double* rtau, int64_t N, double beta, double* Feval,
+                           cudaStream_t s) {
+  pol_tau_kernel<<<unsigned((9 * N + 255) / 256), 256, 0, s>>>(F, G, rtau, N, beta, Feval);
   return cudaGetLastError();
 }
 cudaError_t launch_pol_rF(const double* F, const double* Ftau, const double* P, const double* dPdF, const double* rtau,
