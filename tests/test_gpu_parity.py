@@ -111,10 +111,13 @@ def test_solver_parity(gpu, oracle_lib, case):
     g.close()
 
 
-def test_mixed_precision_within_1e5(gpu, oracle_lib):
-    """FP32 FFT/Gamma/field update with the FP64 correction sweep: <P> within 1e-5 of FP64."""
+@pytest.mark.parametrize('derivative', ['continuous', 'FWBW_difference'])
+def test_mixed_precision_within_1e5(gpu, oracle_lib, derivative):
+    """FP32 FFT/Gamma/field update with the FP64 correction sweep: <P> within 1e-5 of FP64 (the
+    FP32 instantiations of both Gamma kernels)."""
     rve = synthetic.voronoi_rve((16, 16, 16), workloads.SIZE_1MM, 12, 3)
     ph, num = workloads.bcc_24(), workloads.numerics_default()
+    num.derivative = derivative
     res = {}
     for prec in ('fp64', 'mixed'):
         s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, ph, num, precision=prec)

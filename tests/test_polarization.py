@@ -98,13 +98,15 @@ def test_polarization_numerics_validation():
 
 
 # ------------------------------------------------------------------------------- GPU
-def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres', derivative='continuous'):
+def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres', derivative='continuous',
+             update_gamma=False):
     from damask_b200.grid import SpectralPolarization
     rve = synthetic.voronoi_rve(cells, workloads.SIZE_1MM, grains, seed)
     phase = phase or workloads.fcc_al()
     num = workloads.numerics_default()
     num.solver = 'spectral_polarization'
     num.derivative = derivative
+    num.update_gamma = update_gamma
     if snes == 'nrichardson':
         num.PETSc_options = '-snes_type nrichardson'
     g = SpectralPolarization(rve.cells, rve.size, rve.material, rve.quaternions, phase, num)
@@ -113,7 +115,8 @@ def gpu_pair(oracle_lib, cells, grains, seed=0, phase=None, snes='ngmres', deriv
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'fcc9_fwbw'])
+@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'fcc9_fwbw', 'fcc8_central',
+                                  'fcc8_update_gamma'])
 def test_polarization_parity(gpu, oracle_lib, case):
     if case == 'fcc16_anderson':
         g, o = gpu_pair(oracle_lib, (16, 16, 16), 20)
@@ -123,6 +126,13 @@ def test_polarization_parity(gpu, oracle_lib, case):
         n = 3
     elif case == 'fcc9_fwbw':
         g, o = gpu_pair(oracle_lib, (9, 7, 5), 6, seed=2, derivative='FWBW_difference')
+        n = 3
+    elif case == 'fcc8_central':
+        g, o = gpu_pair(oracle_lib, (8, 6, 10), 6, seed=4, derivative='central_difference')
+        n = 3
+    elif case == 'fcc8_update_gamma':
+        # Gamma and the polarization scales re-based on C_minMaxAvg every solution (:291-295)
+        g, o = gpu_pair(oracle_lib, (8, 8, 8), 6, seed=5, update_gamma=True)
         n = 3
     else:
         g, o = gpu_pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_24())
@@ -137,8 +147,11 @@ def test_polarization_parity(gpu, oracle_lib, case):
     for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'F_tau', 'F_tau_lastinc'):
         assert rel(g.get_field(name), o.get_field(name)) < TOL, name
     assert rel(g.aims()['C_volAvg'], o.aims()['C_volAvg']) < TOL
-    for a, b in zip(g.get_coords(), o.get_coords()):
-        assert rel(a, b) < TOL
+    # the difference schemes' |xi|^2 is ~1e-32 at Nyquist points of even grids (sin(pi) rounds to
+    # 1.2e-16), where utilities_updateCoords divides by it: coordinates there are rounding noise
+    if g.numerics.derivative == 'continuous' or all(n % 2 == 1 for n in g.cells):
+        for a, b in zip(g.get_coords(), o.get_coords()):
+            assert rel(a, b) < TOL
     g.close()
 
 
