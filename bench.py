@@ -182,12 +182,12 @@ def load_peaks() -> dict:
 
 
 def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, local: int, cells=None,
-            solver_name: str = 'spectral_basic') -> dict:
+            solver_name: str = 'spectral_basic', workload: str = WORKLOAD) -> dict:
     from damask_b200 import workloads
     from damask_b200.grid import IncrementDriver, SpectralBasic
 
     import torch
-    rve, phase, lcs, num = workloads.make(WORKLOAD, cells)
+    rve, phase, lcs, num = workloads.make(workload, cells)
     num.solver = solver_name
     free0 = torch.cuda.mem_get_info(local)[0]
     solver = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision,
@@ -245,7 +245,7 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     return out
 
 
-def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None) -> dict:
+def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None, workload: str = WORKLOAD) -> dict:
     """The CPU restatement on the same material and load, on a 48^3 cut of the
     workload's statistics (13 grains, seed 3), first increments; ~10-30 s of work."""
     from damask_b200 import workloads
@@ -256,7 +256,7 @@ def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None) -> d
     threads = threads or os.cpu_count() or 1
     cells = (48, 48, 48)
     rve = voronoi_rve(cells, workloads.SIZE_1MM, 13, 3)
-    phase = workloads.bcc_24()
+    phase = workloads.PHASES[workloads.WORKLOADS[workload][3]]()
     lcs = workloads.tension_x(100.0, 100)
     o = OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, workloads.numerics_default(),
                             threads=threads)
@@ -271,7 +271,8 @@ def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None) -> d
     dt = time.perf_counter() - t0
     o.close()
     return {'value': upd / dt, 'seconds': dt, 'cores': threads, 'updates': upd,
-            'sample': f'oracle (C++ FP64, OpenMP) on a 48^3 RVE, 13 grains, same bcc-24 material and tension load, '
+            'sample': f'oracle (C++ FP64, OpenMP) on a 48^3 RVE, 13 grains, same {phase.n_slip}-system material and '
+                      f'tension load, '
                       f'increments {warmup + 1}..{warmup + steps}'}
 
 
@@ -328,6 +329,8 @@ def main():
                     help='measure the batched workload instead: this many independent RVEs (512 in the '
                          'workload definition), one JSON line of its own')
     ap.add_argument('--batch-threads', type=int, default=48)
+    ap.add_argument('--workload', choices=['grid256_bcc24_2000g', 'grid256_bcc48_2000g'], default=WORKLOAD,
+                    help='the headline bcc N_sl [12,12] RVE, or the same RVE with all three cI families (48 systems)')
     args = ap.parse_args()
     if args.batch:
         return run_batch(args)
@@ -338,13 +341,13 @@ def main():
     if args.impl == 'reference':
         if rank != 0:
             return
-        s = cpu_sample(steps=max(1, args.steps), warmup=0)
+        s = cpu_sample(steps=max(1, args.steps), warmup=0, workload=args.workload)
         line = {'metric': METRIC, 'value': s['value'], 'unit': 'updates/s', 'n_gpus': args.gpus, 'steps': args.steps,
                 'warmup': 0, 'ms_per_step': 1e3 * s['seconds'] / max(1, args.steps), 'higher_is_better': True,
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
                 'impl': 'reference',
-                'config': {'workload': 'bcc-24 phenopowerlaw RVE, tension 1e-3/s (48^3 bounded sample of the '
-                                       '256^3/2000-grain workload)', 'solver': 'Anderson fixed point'},
+                'config': {'workload': f'{args.workload}: bcc phenopowerlaw RVE, tension 1e-3/s (48^3 bounded '
+                                       'sample of the 256^3/2000-grain workload)', 'solver': 'Anderson fixed point'},
                 'cpu_baseline': {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port',
                                  'sample': s['sample']},
                 'e2e': {'value': s['value'], 'unit': 'updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
@@ -354,7 +357,7 @@ def main():
     res = {}
     precs = ('mixed', 'fp64') if args.precision == 'both' else (args.precision,)
     for prec in precs:
-        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver)
+        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver, args.workload)
     mx = res.get('mixed', res.get('fp64'))
     fp = res.get('fp64', mx)
     ms_max = allreduce_max(mx['ms'], world)
@@ -381,15 +384,16 @@ def main():
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        s = cpu_sample()
+        s = cpu_sample(workload=args.workload)
         cpu = {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port', 'sample': s['sample']}
     line = {
         'metric': METRIC, 'value': value, 'unit': 'updates/s', 'n_gpus': world, 'steps': args.steps,
         'warmup': warmup, 'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64 constitutive, f32 spectral (mixed)', 'data': 'synthetic',
-        'config': {'workload': f'{WORKLOAD}: 256^3 grid, 2000 Voronoi grains (seed 3), bcc N_sl [12,12], '
+        'config': {'workload': f'{args.workload}: 256^3 grid, 2000 Voronoi grains (seed 3), bcc N_sl '
+                               f'{"[12,12,24]" if "bcc48" in args.workload else "[12,12]"}, '
                                'tension dot_F_xx 1e-3/s, 100 increments to 10 %' if cells is None else
-                               f'{WORKLOAD} at {cells}',
+                               f'{args.workload} at {cells}',
                    'solver': f"{args.solver.replace('spectral_', '')} spectral, Anderson fixed point (m=8)",
                    'precision': 'mixed',
                    'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
@@ -402,7 +406,8 @@ def main():
                                                'evaluation of all voxels',
                      'achieved': achieved_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
                      'frac': achieved_gbs / peaks['hbm_gbs'], 'peak_source': peaks['source'],
-                     'traffic': TRAFFIC_BYTES_PER_UPDATE * mx['N'], 'traffic_source': 'ncu at 64^3, scaled by voxels',
+                     'traffic': TRAFFIC_BYTES_PER_UPDATE * mx['N'] if args.workload == WORKLOAD else None,
+                     'traffic_source': 'ncu at 64^3 (bcc N_sl [12,12]), scaled by voxels',
                      'bytes_per_update': bpu, 'avg_launch_ms': avg_launch_ms,
                      'fp64': {'achieved': fp64_tflops, 'peak': fp64_peak, 'unit': 'TFLOP/s',
                               'frac': fp64_tflops / fp64_peak, 'peak_source': fp64_source,

@@ -283,6 +283,7 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
 DMK_INSTANTIATE(12)
 DMK_INSTANTIATE(18)
 DMK_INSTANTIATE(24)
+DMK_INSTANTIATE(48)
 #undef DMK_INSTANTIATE
 
 }  // namespace dmk

@@ -151,7 +151,8 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
     hooke_S<NS>(pc, Fe, s6);
     // Lp_c = sum_s dot_gamma_s P_s and the weights of its derivative
     double Lc[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    unsigned neg = 0u;
+    static_assert(NS <= 64, "one sense bit per slip system");
+    SenseMask<NS> neg = 0u;
 #pragma unroll 2
     for (int s = 0; s < NS; ++s) {
       const SysConst& c = sc[s];
@@ -178,7 +179,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       }
       if (!(fabs(g) > TINY10)) dg = 0.0;
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
-      if (!(g > 0.0)) neg |= 1u << s;
+      if (!(g > 0.0)) neg |= SenseMask<NS>(1) << s;
       sw[s * PASS_THREADS] = dt * dg;
       sg[s * PASS_THREADS] = fabs(g);
       double2 P[5];
@@ -313,7 +314,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
 // read with uniform addresses (broadcast) in the control kernels.
 template <int NS>
 __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double* hs) {
-  for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.h[i / NS][i % NS];
+  for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.hmat[i];
 }
 
 // Slots of the stress kernel (stride PASS_THREADS): 1/xi [0, NS), Newton weights

@@ -68,6 +68,8 @@ struct dmk_ctx {
   PhaseConst<12>* pc12 = nullptr;
   PhaseConst<18>* pc18 = nullptr;
   PhaseConst<24>* pc24 = nullptr;
+  PhaseConst<48>* pc48 = nullptr;
+  double* hmat = nullptr;        // slip-slip hardening matrix (NS x NS), read by the pass kernels
   Numerics nm;
   Numerics2 nm2;
   GammaConst gc;
@@ -233,6 +235,7 @@ int run_constitutive(dmk_ctx* c, const Fields& f, double dt, int apply) {
     case 12: return constitutive_passes<12>(c, *c->pc12, f, dt, apply);
     case 18: return constitutive_passes<18>(c, *c->pc18, f, dt, apply);
     case 24: return constitutive_passes<24>(c, *c->pc24, f, dt, apply);
+    case 48: return constitutive_passes<48>(c, *c->pc48, f, dt, apply);
   }
   return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
 }
@@ -241,6 +244,7 @@ cudaError_t run_dPdF(dmk_ctx* c, const Fields& f, double dt, const TangentOut& o
     case 12: return launch_dPdF<12>(*c->pc12, f, dt, o, 0, c->N, c->stream, with_sums);
     case 18: return launch_dPdF<18>(*c->pc18, f, dt, o, 0, c->N, c->stream, with_sums);
     case 24: return launch_dPdF<24>(*c->pc24, f, dt, o, 0, c->N, c->stream, with_sums);
+    case 48: return launch_dPdF<48>(*c->pc48, f, dt, o, 0, c->N, c->stream, with_sums);
   }
   return cudaErrorInvalidValue;
 }
@@ -249,6 +253,7 @@ cudaError_t run_pick(dmk_ctx* c, const Fields& f, double dt) {
     case 12: return launch_tangent_pick<12>(*c->pc12, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
     case 18: return launch_tangent_pick<18>(*c->pc18, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
     case 24: return launch_tangent_pick<24>(*c->pc24, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
+    case 48: return launch_tangent_pick<48>(*c->pc48, f, dt, c->tan_idx, c->tan_out, c->tan.planes, c->stream);
   }
   return cudaErrorInvalidValue;
 }
@@ -256,7 +261,8 @@ cudaError_t run_pick(dmk_ctx* c, const Fields& f, double dt) {
 int nblocks_const(const dmk_ctx* c) { return int((c->N + CONST_THREADS - 1) / CONST_THREADS); }
 
 template <int NS>
-void fill_phase_const(const HostPhase& hp, PhaseConst<NS>& pc) {
+void fill_phase_const(const HostPhase& hp, const double* hmat, PhaseConst<NS>& pc) {
+  pc.hmat = hmat;
   std::memcpy(pc.C66, hp.C66, sizeof pc.C66);
   std::memcpy(pc.C, hp.C, sizeof pc.C);
   for (int s = 0; s < NS; ++s) {
@@ -292,7 +298,6 @@ void fill_phase_const(const HostPhase& hp, PhaseConst<NS>& pc) {
     pc.ixiinf[s] = 1.0 / hp.xiinf[s];
     pc.n_int[s] = (hp.n[s] == std::floor(hp.n[s]) && hp.n[s] >= 1.0 && hp.n[s] <= 64.0) ? int(hp.n[s]) : -1;
     pc.a_int[s] = (hp.a[s] == std::floor(hp.a[s]) && hp.a[s] >= 0.0 && hp.a[s] <= 64.0) ? int(hp.a[s]) : -1;
-    for (int k = 0; k < NS; ++k) pc.h[s][k] = hp.h[s * NS + k];
   }
   pc.atol_xi = hp.atol_xi;
   pc.atol_gamma = hp.atol_gamma;
@@ -863,9 +868,9 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   int rc = build_host_phase(*phase, c->hp, g_err);
   if (rc) { delete c; return DMK_ERR_CONFIG; }
   c->NS = c->hp.Ns;
-  if (c->NS != 12 && c->NS != 18 && c->NS != 24) {
+  if (c->NS != 12 && c->NS != 18 && c->NS != 24 && c->NS != 48) {
     delete c;
-    return fail(DMK_ERR_CONFIG, "number of active slip systems must be 12, 18 or 24 on this path");
+    return fail(DMK_ERR_CONFIG, "number of active slip systems must be 12, 18, 24 or 48 on this path");
   }
   c->device = device;
   c->precision = precision;
@@ -908,10 +913,14 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   for (int i = 0; i < 3; ++i) c->gc.rescale[i] = geomSize[i] / sgs[i];
   c->gc.derivative = num->derivative;
 
+  if ((rc = dalloc(&c->hmat, size_t(c->NS) * c->NS))) return bail(rc);
+  if (cudaMemcpy(c->hmat, c->hp.h.data(), sizeof(double) * c->NS * c->NS, cudaMemcpyHostToDevice) != cudaSuccess)
+    return bail(fail(DMK_ERR_CUDA, "copy of the hardening matrix failed"));
   switch (c->NS) {
-    case 12: c->pc12 = new PhaseConst<12>(); fill_phase_const<12>(c->hp, *c->pc12); break;
-    case 18: c->pc18 = new PhaseConst<18>(); fill_phase_const<18>(c->hp, *c->pc18); break;
-    case 24: c->pc24 = new PhaseConst<24>(); fill_phase_const<24>(c->hp, *c->pc24); break;
+    case 12: c->pc12 = new PhaseConst<12>(); fill_phase_const<12>(c->hp, c->hmat, *c->pc12); break;
+    case 18: c->pc18 = new PhaseConst<18>(); fill_phase_const<18>(c->hp, c->hmat, *c->pc18); break;
+    case 24: c->pc24 = new PhaseConst<24>(); fill_phase_const<24>(c->hp, c->hmat, *c->pc24); break;
+    case 48: c->pc48 = new PhaseConst<48>(); fill_phase_const<48>(c->hp, c->hmat, *c->pc48); break;
   }
 
   const int NST = 2 * c->NS;
@@ -1632,6 +1641,8 @@ void dmk_destroy(dmk_ctx* c) {
   delete c->pc12;
   delete c->pc18;
   delete c->pc24;
+  delete c->pc48;
+  if (c->hmat) cudaFree(c->hmat);
   delete c;
 }
 

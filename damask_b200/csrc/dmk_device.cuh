@@ -6,6 +6,7 @@
 // 3x3 tensors use the Fortran component order c = i + 3*j; the symmetric stress
 // S uses six planes (11, 22, 33, 23, 13, 12).
 #pragma once
+#include <type_traits>
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -25,7 +26,7 @@ struct PhaseConst {
   double PnS[2][NS][9];    // P_nS (pos/neg sense), column-major
   double dn[NS][6];        // slip direction d and plane normal n (unit): P = d (x) n
   double dg0[NS], n[NS], a[NS], h0f[NS], xiinf[NS], ixiinf[NS];
-  double h[NS][NS];        // slip-slip hardening matrix, row = reacting system
+  const double* hmat;      // slip-slip hardening matrix (NS x NS, row = reacting system) in device memory
   int n_int[NS];           // stress exponent as integer if integral, else -1
   int a_int[NS];           // hardening exponent as integer if integral, else -1
   double atol_xi, atol_gamma;
@@ -166,6 +167,10 @@ __device__ __forceinline__ double powr(double x, double e, int ei) { return ei >
 
 // Per slip system constants of the Newton loop, staged in shared memory once per
 // block; pairs hold the positive and negative sense so that one 16-byte load serves both.
+// one bit per slip system (the sense of its resolved shear): 32 bits up to 32 systems, else 64
+template <int NS>
+using SenseMask = typename std::conditional<(NS > 32), unsigned long long, unsigned>::type;
+
 struct SysConst {
   double2 p6[6];     // (p6[0][s][t], p6[1][s][t]): tau = S : P_nS
   double2 q6[6];     // (q6[0][s][t], q6[1][s][t]): Q = C : P_nS

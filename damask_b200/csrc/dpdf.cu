@@ -32,9 +32,13 @@ constexpr int TAN_THREADS = 64;
 //   [0, 54)    K (9x6, row q = k + 3 l)
 //   [54, 90)   L (6x6) while it is built, then a1, a2, a3, d (3x3 each)
 //   [90, 99)   Fp0^-1
-//   [99, 123)  dgamma (NS <= 24) while K is built, then Fe and Fp^-1 (3x3 each)
-//   [123, 132) F
-constexpr int TAN_SLOTS = 132;
+//   [99, 99 + G)      dgamma (NS entries) while K is built, then Fe and Fp^-1 (3x3 each);
+//                     G = max(NS, 24)
+//   [99 + G, 108 + G) F
+template <int NS>
+__host__ __device__ constexpr int tan_dg_slots() { return NS > 24 ? NS : 24; }
+template <int NS>
+__host__ __device__ constexpr int tan_slots() { return 108 + tan_dg_slots<NS>(); }
 
 // sym6(C : sym(Y)) for a 3x3 Y (column-major), through the Mandel stiffness; (11 22 33 23 13 12)
 template <int NS>
@@ -60,7 +64,7 @@ __device__ double tangent_voxel(const PhaseConst<NS>& pc, const Fields& f, int64
   double* const sL = xs + 54 * T;              // later: a1, a2, a3, d
   double* const sFp0i = xs + 90 * T;
   double* const sdg = xs + 99 * T;             // later: Fe, Fp^-1
-  double* const sF = xs + 123 * T;
+  double* const sF = xs + (99 + tan_dg_slots<NS>()) * T;
   double s6[6];
   {
     double F[9], invFp[9], Fe[9], Fp[9], Fp0[9], invFp0[9];
@@ -75,7 +79,8 @@ __device__ double tangent_voxel(const PhaseConst<NS>& pc, const Fields& f, int64
 #pragma unroll
     for (int k = 0; k < 9; ++k) sFp0i[k * T] = invFp0[k];
     // kinetics (phenopowerlaw.f90:303-350): dgamma_s and the sense of each system
-    unsigned neg = 0u;
+    static_assert(NS <= 64, "one sense bit per slip system");
+    SenseMask<NS> neg = 0u;
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
       const double tp = dot6(s6, pc.p6[0][s]), tn = dot6(s6, pc.p6[1][s]);
@@ -83,7 +88,7 @@ __device__ double tangent_voxel(const PhaseConst<NS>& pc, const Fields& f, int64
       const double tmax = pos ? tp : tn;
       const double g = (pos ? pc.dg0[s] : -pc.dg0[s]) * powr(tmax / f.state[s * N + v], pc.n[s], pc.n_int[s]);
       sdg[s * T] = fabs(g) > TINY10 ? g * pc.n[s] / tmax : 0.0;
-      if (!(g > 0.0)) neg |= 1u << s;
+      if (!(g > 0.0)) neg |= SenseMask<NS>(1) << s;
     }
     // K = dLp/dS on symmetric dS, column by column: K_c = sum_s dgamma_s p_s[c] P_s; and
     // L_c = e_c + dt sym6(C : sym(B K_c)) with B = Fe^T A, A = F Fp0^-1
@@ -335,6 +340,8 @@ template cudaError_t launch_tangent_pick<18>(const PhaseConst<18>&, const Fields
                                              const double*, cudaStream_t);
 template cudaError_t launch_tangent_pick<24>(const PhaseConst<24>&, const Fields&, double, const long long*, double*,
                                              const double*, cudaStream_t);
+template cudaError_t launch_tangent_pick<48>(const PhaseConst<48>&, const Fields&, double, const long long*, double*,
+                                             const double*, cudaStream_t);
 
 // number of per-block partials the tangent reduction produces for count voxels
 int dPdF_blocks(int64_t count) { return int(std::max<int64_t>(1, std::min<int64_t>(TSUM_BLOCKS, (count + 255) / 256))); }
@@ -342,7 +349,7 @@ int dPdF_blocks(int64_t count) { return int(std::max<int64_t>(1, std::min<int64_
 template <int NS>
 cudaError_t launch_dPdF(const PhaseConst<NS>& pc, const Fields& f, double dt, const TangentOut& o, int64_t first,
                         int64_t count, cudaStream_t s, bool with_sums) {
-  const size_t smem = size_t(TAN_SLOTS) * TAN_THREADS * sizeof(double);
+  const size_t smem = size_t(tan_slots<NS>()) * TAN_THREADS * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(dPdF_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem));
   if (e != cudaSuccess) return e;
   const int nb = int((count + TAN_THREADS - 1) / TAN_THREADS);
@@ -360,6 +367,8 @@ template cudaError_t launch_dPdF<12>(const PhaseConst<12>&, const Fields&, doubl
 template cudaError_t launch_dPdF<18>(const PhaseConst<18>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
                                      cudaStream_t, bool);
 template cudaError_t launch_dPdF<24>(const PhaseConst<24>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
+                                     cudaStream_t, bool);
+template cudaError_t launch_dPdF<48>(const PhaseConst<48>&, const Fields&, double, const TangentOut&, int64_t, int64_t,
                                      cudaStream_t, bool);
 
 // Sums the per-block partials (C_volAvg) and finds the extreme Frobenius norms.

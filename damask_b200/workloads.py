@@ -10,6 +10,9 @@ with the same keys as DAMASK's ``material.yaml`` / ``load.yaml``.
   C11/C12/C44 = 233.3/135.5/118.0 GPa, xi_0 95/97 MPa, xi_inf 222/412 MPa,
   h_0 1 GPa, n 20, a 2; the 24 interaction values start [1,1.4,1,1.4] and are
   padded with 1.4 (the reference needs one value per interaction type present).
+* ``bcc_48``: the same with the third cI family {123}<111> (N_sl [12,12,24], 48 systems), which
+  takes the {112} parameters (xi_0 97 MPa, xi_inf 412 MPa); 28 interaction values
+  [1,1.4,1,1.4] + 24 x 1.4, as the reference's phenopowerlaw_polygonal-ferrite.yaml.
 """
 from __future__ import annotations
 
@@ -42,6 +45,18 @@ def bcc_24() -> Phase:
                         'n_sl': [20, 20], 'xi_0_sl': [95.0e6, 97.0e6], 'xi_inf_sl': [222.0e6, 412.0e6]}}})
 
 
+def bcc_48() -> Phase:
+    h = [1, 1.4, 1, 1.4] + [1.4] * 24
+    return Phase.from_dict({
+        'lattice': 'cI',
+        'mechanical': {
+            'elastic': {'type': 'Hooke', 'C_11': 233.3e9, 'C_12': 135.5e9, 'C_44': 118.0e9},
+            'plastic': {'type': 'phenopowerlaw', 'N_sl': [12, 12, 24], 'a_sl': [2.0, 2.0, 2.0],
+                        'dot_gamma_0_sl': [0.001] * 3, 'h_0_sl-sl': [1.0e9] * 3, 'h_sl-sl': h,
+                        'n_sl': [20, 20, 20], 'xi_0_sl': [95.0e6, 97.0e6, 97.0e6],
+                        'xi_inf_sl': [222.0e6, 412.0e6, 412.0e6]}}})
+
+
 def tension_x(t: float, N: int, f_out: int = 1) -> list[LoadCase]:
     """Uniaxial tension dot_F_xx = 1e-3/s with P_yy = P_zz = 0 (examples/grid/tensionX.yaml)."""
     return parse_load({'loadstep': [{
@@ -64,14 +79,16 @@ WORKLOADS = {
     'grid64_fcc_200g': ((64, 64, 64), 200, 1, 'fcc_al', 100.0, 100),
     'grid32_fcc_50g': ((32, 32, 32), 50, 2, 'fcc_al', 50.0, 50),
     'grid256_bcc24_2000g': ((256, 256, 256), 2000, 3, 'bcc_24', 100.0, 100),
+    'grid256_bcc48_2000g': ((256, 256, 256), 2000, 3, 'bcc_48', 100.0, 100),
 }
+PHASES = {'fcc_al': lambda: fcc_al(), 'bcc_24': lambda: bcc_24(), 'bcc_48': lambda: bcc_48()}
 
 
 def make(name: str, cells=None) -> tuple[RVE, Phase, list[LoadCase], Numerics]:
     c, grains, seed, ph, t, N = WORKLOADS[name]
     cells = tuple(cells) if cells is not None else c
     rve = voronoi_rve(cells, SIZE_1MM, grains, seed)
-    phase = fcc_al() if ph == 'fcc_al' else bcc_24()
+    phase = PHASES[ph]()
     return rve, phase, tension_x(t, N), numerics_default()
 
 

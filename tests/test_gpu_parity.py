@@ -36,7 +36,8 @@ def test_init_sweep(gpu, oracle_lib):
     g.close()
 
 
-@pytest.mark.parametrize('phase', [workloads.fcc_al(), workloads.bcc_24()], ids=['fcc12', 'bcc24'])
+@pytest.mark.parametrize('phase', [workloads.fcc_al(), workloads.bcc_24(), workloads.bcc_48()],
+                         ids=['fcc12', 'bcc24', 'bcc48'])
 def test_constitutive_response_and_tangent(gpu, oracle_lib, phase):
     """utilities_constitutiveResponse and phase_mechanical_dPdF in the plastic range."""
     g, o = pair(oracle_lib, (6, 5, 4), 4, phase=phase)
@@ -86,7 +87,7 @@ def run_both(g, o, n):
     return sg, so
 
 
-@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson'])
+@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'bcc48_anderson'])
 def test_solver_parity(gpu, oracle_lib, case):
     """grid_mechanical_spectral_basic_{forward,solution} + materialpoint_forward over several
     increments of uniaxial tension: per-voxel fields within 1e-9, identical iteration counts."""
@@ -96,6 +97,9 @@ def test_solver_parity(gpu, oracle_lib, case):
     elif case == 'fcc8_richardson':
         num.PETSc_options = '-snes_type nrichardson'
         g, o, n = *pair(oracle_lib, (8, 8, 8), 6, num=num), 3
+    elif case == 'bcc48_anderson':
+        # all three cI families, N_sl [12,12,24]
+        g, o, n = *pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_48()), 2
     else:
         g, o, n = *pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_24()), 2
     sg, so = run_both(g, o, n)
