@@ -207,6 +207,11 @@ class Numerics:
     eps_rel_P: float = 1.0e-3
     update_gamma: bool = False
     divergence_correction: str = 'grid+size'
+    # solver.grid.FFT.memory_efficient / FFTW_plan_mode (spectral_utilities.f90:176, :210-223):
+    # accepted and validated; Gamma_hat is always evaluated on the fly (both settings give the same
+    # operator) and cuFFT has no planner modes
+    memory_efficient: bool = True
+    FFTW_plan_mode: str = 'FFTW_MEASURE'
     derivative: str = 'continuous'
     N_cutback_max: int = 3
     r_cutback_min: float = 1.0e-3
@@ -275,6 +280,10 @@ class Numerics:
             n.divergence_correction = fft['divergence_correction']
         if 'derivative' in fft:
             n.derivative = fft['derivative']
+        if 'memory_efficient' in fft:
+            n.memory_efficient = bool(fft['memory_efficient'])
+        if 'FFTW_plan_mode' in fft:
+            n.FFTW_plan_mode = str(fft['FFTW_plan_mode'])
         if 'N_cutback_max' in grid:
             n.N_cutback_max = int(grid['N_cutback_max'])
         for k in ('r_cutback_min', 'r_cutback', 'r_increase', 'eps_rel_state', 'N_iter_state_max'):
@@ -301,6 +310,10 @@ class Numerics:
         if self.N_iter_Lp_max < 1: bad.append('N_iter_Lp_max')
         if self.N_iter_state_max < 1: bad.append('N_iter_state_max')
         if self.derivative not in DERIVATIVES: bad.append('derivative')
+        if self.divergence_correction not in ('none', 'size', 'grid+size', 'size+grid'):
+            bad.append('divergence_correction')
+        if self.FFTW_plan_mode not in ('FFTW_ESTIMATE', 'FFTW_MEASURE', 'FFTW_PATIENT', 'FFTW_EXHAUSTIVE'):
+            bad.append('FFTW_plan_mode')
         if not 1 <= self.anderson_m <= 32: bad.append('anderson_m')
         if self.solver not in SOLVERS: bad.append('solver')
         if self.solver == 'spectral_polarization':

@@ -69,6 +69,13 @@ def test_numerics_from_yaml_and_validation():
         Numerics(N_iter_min=5, N_iter_max=2).to_struct()
     with pytest.raises(ValueError):
         Numerics(PETSc_options='-snes_type newtonls').to_struct()
+    # solver.grid.FFT keys (spectral_utilities.f90:176-223)
+    n = Numerics.from_dict({'solver': {'grid': {'FFT': {'memory_efficient': False, 'FFTW_plan_mode': 'FFTW_PATIENT',
+                                                        'derivative': 'FWBW_difference'}}}})
+    assert not n.memory_efficient and n.FFTW_plan_mode == 'FFTW_PATIENT' and n.to_struct().derivative == 2
+    for bad in ({'FFTW_plan_mode': 'FFTW_WISDOM_ONLY'}, {'divergence_correction': 'grid'}, {'derivative': 'FWBW'}):
+        with pytest.raises(ValueError, match=list(bad)[0]):
+            Numerics.from_dict({'solver': {'grid': {'FFT': bad}}}).to_struct()
 
 
 def test_phase_rejects_unsupported():
