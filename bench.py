@@ -182,13 +182,14 @@ def load_peaks() -> dict:
 
 
 def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, local: int, cells=None,
-            solver_name: str = 'spectral_basic', workload: str = WORKLOAD) -> dict:
+            solver_name: str = 'spectral_basic', workload: str = WORKLOAD, derivative: str = 'continuous') -> dict:
     from damask_b200 import workloads
     from damask_b200.grid import IncrementDriver, SpectralBasic
 
     import torch
     rve, phase, lcs, num = workloads.make(workload, cells)
     num.solver = solver_name
+    num.derivative = derivative
     free0 = torch.cuda.mem_get_info(local)[0]
     solver = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision,
                            device=local)
@@ -329,6 +330,8 @@ def main():
                     help='measure the batched workload instead: this many independent RVEs (512 in the '
                          'workload definition), one JSON line of its own')
     ap.add_argument('--batch-threads', type=int, default=48)
+    ap.add_argument('--derivative', choices=['continuous', 'central_difference', 'FWBW_difference'],
+                    default='continuous', help='solver.grid.FFT.derivative (testing and profiling only)')
     ap.add_argument('--workload', choices=['grid256_bcc24_2000g', 'grid256_bcc48_2000g'], default=WORKLOAD,
                     help='the headline bcc N_sl [12,12] RVE, or the same RVE with all three cI families (48 systems)')
     args = ap.parse_args()
@@ -357,7 +360,8 @@ def main():
     res = {}
     precs = ('mixed', 'fp64') if args.precision == 'both' else (args.precision,)
     for prec in precs:
-        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver, args.workload)
+        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver, args.workload,
+                            args.derivative)
     mx = res.get('mixed', res.get('fp64'))
     fp = res.get('fp64', mx)
     ms_max = allreduce_max(mx['ms'], world)
@@ -394,7 +398,8 @@ def main():
                                f'{"[12,12,24]" if "bcc48" in args.workload else "[12,12]"}, '
                                'tension dot_F_xx 1e-3/s, 100 increments to 10 %' if cells is None else
                                f'{args.workload} at {cells}',
-                   'solver': f"{args.solver.replace('spectral_', '')} spectral, Anderson fixed point (m=8)",
+                   'solver': f"{args.solver.replace('spectral_', '')} spectral, Anderson fixed point (m=8)"
+                             + ('' if args.derivative == 'continuous' else f', derivative {args.derivative}'),
                    'precision': 'mixed',
                    'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
                    'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
