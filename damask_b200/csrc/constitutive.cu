@@ -56,7 +56,7 @@ __device__ __forceinline__ void append_and_count(const Fields& f, const PassWork
 }  // namespace
 
 template <int NS>
-__global__ void __launch_bounds__(PASS_THREADS, 4)
+__global__ void __launch_bounds__(pass_threads<NS>(), 4)
 constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                           int apply_update, int use_dot0, int64_t v_begin, int64_t v_end) {
@@ -111,7 +111,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         for (int i = 0; i < NST; ++i) {
           const double d = w.dot0[i * N + v];
           bad |= isnan(d);
-          xs[i * PASS_THREADS] = d;
+          xs[i * pass_threads<NS>()] = d;
         }
       } else {
         double s0[6];
@@ -119,7 +119,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         for (int k = 0; k < 6; ++k) s0[k] = f.S0[k * N + v];
         bad = dot_state_slots<NS>(pc, hs, s0, f.state0, N, v, xs, nullptr);
 #pragma unroll 12
-        for (int i = 0; i < NST; ++i) w.dot0[i * N + v] = xs[i * PASS_THREADS];
+        for (int i = 0; i < NST; ++i) w.dot0[i * N + v] = xs[i * pass_threads<NS>()];
       }
       if (bad) {
         double s6[6];
@@ -141,7 +141,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         double* D0 = w.D + v;                               // dotState generation 0
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
-          const double d = xs[i * PASS_THREADS];
+          const double d = xs[i * pass_threads<NS>()];
           f.state[i * N + v] = fma(d, dts, f.state0[i * N + v]);
           D0[i * N] = d;
         }
@@ -158,7 +158,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
 
 // one state iteration of every listed voxel: integrateStress (integrateStateFPI:626-629)
 template <int NS>
-__global__ void __launch_bounds__(PASS_THREADS)
+__global__ void __launch_bounds__(pass_threads<NS>())
 constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                            const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                            const int* __restrict__ list_in, int64_t n_in) {
@@ -178,7 +178,7 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
 #pragma unroll
     for (int k = 0; k < 9; ++k) Lp[k] = f.Lp[k * N + v];
 #pragma unroll
-    for (int s = 0; s < NS; ++s) xs[s * PASS_THREADS] = 1.0 / f.state[s * N + v];
+    for (int s = 0; s < NS; ++s) xs[s * pass_threads<NS>()] = 1.0 / f.state[s * N + v];
     double S[6], Fp[9], P[9], Fe[9];
     const double* Fp0s = (w.sub[v] == 0.0 ? f.Fp0 : w.Fp0s) + v;   // subFp0 (see sub_start)
     const int st = integrate_stress<NS>(pc, sc, nm, w.Fs + v, Fp0s, N, xs, step * dt, Lp, S, Fp, P, Fe,
@@ -194,7 +194,7 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
 #pragma unroll
       for (int k = 0; k < 6; ++k) f.S[k * N + v] = S[k];
 #pragma unroll
-      for (int s = 0; s < NS; ++s) w.adg[s * N + v] = xs[(2 * NS + s) * PASS_THREADS];
+      for (int s = 0; s < NS; ++s) w.adg[s * N + v] = xs[(2 * NS + s) * pass_threads<NS>()];
     }
     w.ctl[v] = st == 0 ? PH_DOT1 : PH_CTRL;
     w.ctl[N + v] = st;
@@ -218,7 +218,7 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
 // state update and substep control of every listed voxel up to its next
 // integrateStress; the voxels that continue are appended to the next list
 template <int NS>
-__global__ void __launch_bounds__(PASS_THREADS, 4)
+__global__ void __launch_bounds__(pass_threads<NS>(), 4)
 constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                             const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                             const int* __restrict__ list_in, int64_t n_in) {
@@ -247,13 +247,13 @@ template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                       const PassWork& w, double dt, int apply_update, int use_dot0, int64_t v_begin,
                                       int64_t v_end, cudaStream_t s) {
-  const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
+  const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
   if (v_end <= v_begin) return cudaSuccess;
-  const int nb = int((v_end - v_begin + PASS_THREADS - 1) / PASS_THREADS);
-  constitutive_begin_kernel<NS><<<nb, PASS_THREADS, smem, s>>>(pc, nm, f, w, dt, apply_update, use_dot0, v_begin,
+  const int nb = int((v_end - v_begin + pass_threads<NS>() - 1) / pass_threads<NS>());
+  constitutive_begin_kernel<NS><<<nb, pass_threads<NS>(), smem, s>>>(pc, nm, f, w, dt, apply_update, use_dot0, v_begin,
                                                                 v_end);
   return cudaGetLastError();
 }
@@ -261,16 +261,16 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
-  const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * PASS_THREADS * sizeof(double);
-  const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * PASS_THREADS) * sizeof(double);
+  const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * pass_threads<NS>() * sizeof(double);
+  const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem_s));
   if (e == cudaSuccess)
     e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_c));
   if (e != cudaSuccess) return e;
-  const int nb = int((n_in + PASS_THREADS - 1) / PASS_THREADS);
-  constitutive_stress_kernel<NS><<<nb, PASS_THREADS, smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in);
-  constitutive_control_kernel<NS><<<nb, PASS_THREADS, smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  const int nb = int((n_in + pass_threads<NS>() - 1) / pass_threads<NS>());
+  constitutive_stress_kernel<NS><<<nb, pass_threads<NS>(), smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  constitutive_control_kernel<NS><<<nb, pass_threads<NS>(), smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in);
   return cudaGetLastError();
 }
 

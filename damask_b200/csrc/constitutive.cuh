@@ -108,7 +108,7 @@ __device__ __forceinline__ bool qr_solve(double* A, double* b) {
 // integrateStress, phase_mechanical.f90:379-584 (Fi = I, Li = 0).
 // F and Fp0 point at voxel v's planes (stride N); they are read at the start and again
 // for the final Fp / P so that no copy stays in registers through the Newton loop.
-// xs: this thread's shared-memory slots (stride PASS_THREADS): 1/xi (NS entries), the
+// xs: this thread's shared-memory slots (stride pass_threads<NS>()): 1/xi (NS entries), the
 // Newton weights dt*dgamma (NS), |dot_gamma| of the last residual evaluation (NS), then
 // A, the last accepted Lp guess and the Newton step (9 each).  Lp (in/out) is the warm
 // start and, on success, the result; S, Fp, P and Fe are written only on success.
@@ -116,11 +116,11 @@ template <int NS>
 __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __restrict__ sc, const Numerics& nm,
                                 const double* Fg, const double* Fp0g, int64_t N, double* xs, double dt, double* Lp,
                                 double* S, double* Fp, double* Pout, double* Feout, int& newton) {
-  double* const sw = xs + NS * PASS_THREADS;
-  double* const sg = xs + 2 * NS * PASS_THREADS;
-  double* const sA = xs + 3 * NS * PASS_THREADS;
-  double* const sLo = sA + 9 * PASS_THREADS;
-  double* const sdL = sLo + 9 * PASS_THREADS;
+  double* const sw = xs + NS * pass_threads<NS>();
+  double* const sg = xs + 2 * NS * pass_threads<NS>();
+  double* const sA = xs + 3 * NS * pass_threads<NS>();
+  double* const sLo = sA + 9 * pass_threads<NS>();
+  double* const sdL = sLo + 9 * pass_threads<NS>();
   {
     double F[9], Fp0[9], invFp0[9], A[9];
 #pragma unroll
@@ -128,12 +128,12 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
     if (inv33(Fp0, invFp0)) return 5;                     // STATUS_FAIL_PHASE_MECHANICAL_STRESS
     mm33(F, invFp0, A);
 #pragma unroll
-    for (int k = 0; k < 9; ++k) sA[k * PASS_THREADS] = A[k];
+    for (int k = 0; k < 9; ++k) sA[k * pass_threads<NS>()] = A[k];
   }
 
   double Lg[9], B[9], s6[6];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; sLo[k * PASS_THREADS] = Lp[k]; sdL[k * PASS_THREADS] = 0.0; }
+  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; sLo[k * pass_threads<NS>()] = Lp[k]; sdL[k * pass_threads<NS>()] = 0.0; }
   double step = 1.0, res_old = 1.7976931348623157e308;
   int jaco = 0;
   for (int it = 1;; ++it) {
@@ -145,7 +145,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
     {
       double A[9];
 #pragma unroll
-      for (int k = 0; k < 9; ++k) A[k] = sA[k * PASS_THREADS];
+      for (int k = 0; k < 9; ++k) A[k] = sA[k * pass_threads<NS>()];
       mm33(A, B, Fe);
     }
     hooke_S<NS>(pc, Fe, s6);
@@ -163,7 +163,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       const double tn = s6[0] * p[0].y + s6[1] * p[1].y + s6[2] * p[2].y + s6[3] * p[3].y + s6[4] * p[4].y + s6[5] * p[5].y;
       const bool pos = tp > tn;
       const double tmax = pos ? tp : tn;
-      const double ixs = xs[s * PASS_THREADS];
+      const double ixs = xs[s * pass_threads<NS>()];
       const double r = tmax * ixs;
       const double2 kin = c.kin;
       const int ni = c.n_int;
@@ -180,8 +180,8 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       if (!(fabs(g) > TINY10)) dg = 0.0;
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
       if (!(g > 0.0)) neg |= SenseMask<NS>(1) << s;
-      sw[s * PASS_THREADS] = dt * dg;
-      sg[s * PASS_THREADS] = fabs(g);
+      sw[s * pass_threads<NS>()] = dt * dg;
+      sg[s * pass_threads<NS>()] = fabs(g);
       double2 P[5];
 #pragma unroll
       for (int k = 0; k < 5; ++k) P[k] = c.P[k];
@@ -199,12 +199,12 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
     if (nR < res_old) {
       res_old = nR;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) sLo[k * PASS_THREADS] = Lg[k];
+      for (int k = 0; k < 9; ++k) sLo[k * pass_threads<NS>()] = Lg[k];
       step = 1.0;
     } else {
       step = nm.r_linesearch_Lp * step;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * PASS_THREADS], step, sLo[k * PASS_THREADS]);
+      for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * pass_threads<NS>()], step, sLo[k * pass_threads<NS>()]);
       continue;
     }
     if (jaco % nm.f_update_jacobi_Lp == 0) {
@@ -220,7 +220,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       {
         double A[9];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) A[k] = sA[k * PASS_THREADS];
+        for (int k = 0; k < 9; ++k) A[k] = sA[k * pass_threads<NS>()];
         mtm33(A, Fe, M);                                  // M = A^T Fe, M[p + 3q] = M(p,q)
       }
       double C6[36];
@@ -229,7 +229,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
 #pragma unroll 2
       for (int s = 0; s < NS; ++s) {
         const SysConst& c = sc[s];
-        const double ws = sw[s * PASS_THREADS];
+        const double ws = sw[s * pass_threads<NS>()];
         const bool ng = (neg >> s) & 1u;
         double q[6];
 #pragma unroll
@@ -272,7 +272,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
           const double2 qq = c.q6[t];
           cq = fma(ng ? qq.y : qq.x, y6[t], cq);
         }
-        cq *= sw[s * PASS_THREADS];
+        cq *= sw[s * pass_threads<NS>()];
         double2 P[5];
 #pragma unroll
         for (int k = 0; k < 5; ++k) P[k] = c.P[k];
@@ -281,10 +281,10 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
         for (int k = 0; k < 9; ++k) X[k] = fma(cq, Ps[k], X[k]);
       }
 #pragma unroll
-      for (int k = 0; k < 9; ++k) sdL[k * PASS_THREADS] = X[k];
+      for (int k = 0; k < 9; ++k) sdL[k * pass_threads<NS>()] = X[k];
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * PASS_THREADS], step, Lg[k]);
+    for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * pass_threads<NS>()], step, Lg[k]);
   }
   // Fp = (Fp0^-1 B)^-1 / det^(1/3); P = F Fp^-1 S Fp^-T; Fe = F Fp^-1  (:571-581)
   double F[9], invFpn[9], Fpn[9];
@@ -317,7 +317,7 @@ __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double
   for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.hmat[i];
 }
 
-// Slots of the stress kernel (stride PASS_THREADS): 1/xi [0, NS), Newton weights
+// Slots of the stress kernel (stride pass_threads<NS>()): 1/xi [0, NS), Newton weights
 // [NS, 2NS), |dot_gamma| [2NS, 3NS), Newton 3x3 scratch [3NS, 3NS + 27).
 template <int NS>
 __host__ __device__ constexpr int stress_slots() { return 3 * NS + 27; }
@@ -358,12 +358,12 @@ __device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double* __restri
     }
     const double d = pc.h0f[l] * left * hg;
     bad |= isnan(d);
-    xs[l * PASS_THREADS] = d;
+    xs[l * pass_threads<NS>()] = d;
   }
 #pragma unroll
   for (int s = 0; s < NS; ++s) {
     bad |= isnan(adg[s]);
-    xs[(NS + s) * PASS_THREADS] = adg[s];
+    xs[(NS + s) * pass_threads<NS>()] = adg[s];
   }
   return bad;
 }
@@ -461,7 +461,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         const double* st0 = sub_start(f, w, c.stepFrac).st0;
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
-          const double d = xs[i * PASS_THREADS];
+          const double d = xs[i * pass_threads<NS>()];
           f.state[i * N + v] = fma(d, dts, st0[i * N + v]);
           D0[i * N] = d;
         }
@@ -477,7 +477,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
         double d01 = 0.0, d12 = 0.0, d22 = 0.0;
 #pragma unroll 24
         for (int i = 0; i < NST; ++i) {
-          const double d = xs[i * PASS_THREADS];
+          const double d = xs[i * pass_threads<NS>()];
           const double l1 = L1[i * N];                                 // dotState_last(:,1)
           const double l2 = c.it > 1 ? L2[i * N] : 0.0;               // dotState_last(:,2)
           const double a = d - l1, b = l1 - l2;
@@ -491,7 +491,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) {
           const double l1 = L1[i * N];
-          const double d = xs[i * PASS_THREADS] * zeta + l1 * (1.0 - zeta);
+          const double d = xs[i * pass_threads<NS>()] * zeta + l1 * (1.0 - zeta);
           const double st = f.state[i * N + v];
           const double r = st - st0[i * N + v] - d * dts;
           const double stn = st - r;

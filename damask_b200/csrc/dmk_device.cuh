@@ -63,6 +63,10 @@ struct Fields {
 };
 
 constexpr int PASS_THREADS = 128;   // threads per block of the pass kernels
+// threads per block of the pass kernels for NS systems: 64 above 24 systems, where the per-thread
+// shared-memory slots of 128-thread blocks would leave one block per SM in the begin and control kernels
+template <int NS>
+__host__ __device__ constexpr int pass_threads() { return NS > 24 ? 64 : PASS_THREADS; }
 
 // Per-voxel iteration state of the pass scheme (planes of N entries each).
 struct PassWork {
