@@ -83,6 +83,36 @@ def test_curl_of_compatible_field_vanishes(oracle_lib):
     o.close()
 
 
+@pytest.mark.parametrize('cells', [(8, 6, 5), (5, 7, 3)])
+def test_curl_of_fwbw_gradient_vanishes(oracle_lib, cells):
+    """With derivative: FWBW_difference (spectral_utilities.f90:823-849) the compatible fields are
+    the staggered gradients G_ij = D_j A_e A_f u_i / (4 h_j) (D x = x(n + 1) - x(n) along j,
+    A x = x(n + 1) + x(n) along the two other directions): their spectra are u_hat (x) xi, whose
+    curl vanishes; the same field is not curl-free for the continuous frequencies."""
+    size = (1.0e-3, 2.0e-3, 1.5e-3)
+    rng = np.random.default_rng(6)
+    u = rng.normal(size=cells + (3,)) * 1e-6
+    h = np.asarray(size) / np.asarray(cells)
+    grad = np.zeros(cells + (3, 3))
+    for j in range(3):
+        d = np.roll(u, -1, axis=j) - u
+        for e in range(3):
+            if e != j:
+                d = np.roll(d, -1, axis=e) + d
+        grad[..., :, j] = d / (4 * h[j])
+    voxels = np.transpose(np.eye(3) + grad, (0, 1, 2, 4, 3)).reshape(cells + (9,)).reshape(-1, 9, order='F')
+    res = {}
+    for derivative in ('FWBW_difference', 'continuous'):
+        num = workloads.numerics_default()
+        num.derivative = derivative
+        o = oracle_lib.OracleSpectralBasic(cells, size, np.zeros(int(np.prod(cells))), np.array([[1.0, 0, 0, 0]]),
+                                           workloads.fcc_al(), num, init=False, threads=1)
+        res[derivative] = o.curl_rms(voxels)
+        o.close()
+    assert res['FWBW_difference'] < 1e-12 * np.abs(grad).max()
+    assert res['continuous'] > 1e-3 * np.abs(grad).max()
+
+
 def test_polarization_numerics_validation():
     num = config.Numerics()
     num.solver = 'spectral_polarization'
