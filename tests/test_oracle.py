@@ -282,3 +282,40 @@ def test_gamma_c_gamma_is_gamma(oracle_lib, derivative, cells):
     g2 = o.gamma_convolution(tau2, np.zeros(9))
     assert rel(g2, g1) < 1e-11
     o.close()
+
+
+def test_update_coords_inverts_gradients_of_purely_imaginary_frequencies(oracle_lib):
+    """utilities_updateCoords (spectral_utilities.f90:899-909) forms u_hat = F_hat xi / sum(conj(-xi) xi).
+    For a gradient F_hat = u_hat (x) xi that is u_hat sum(xi^2) / (-|xi|^2): u itself when xi is purely
+    imaginary (continuous, central difference), but not for the complex FWBW frequencies.  The
+    restatement keeps the reference's formula for all three (odd grid, so no Nyquist terms)."""
+    from damask_b200.grid import displacements
+    cells, size = (5, 7, 3), (1.0e-3, 2.0e-3, 1.5e-3)
+    rng = np.random.default_rng(6)
+    u = rng.normal(size=cells + (3,)) * 1e-6
+    u -= u.mean(axis=(0, 1, 2))
+    h = np.asarray(size) / np.asarray(cells)
+    k = [np.fft.fftfreq(n, d=s / n) * 2 * np.pi for n, s in zip(cells, size)]
+    uh, K = np.fft.fftn(u, axes=(0, 1, 2)), np.meshgrid(*k, indexing='ij')
+    spectral = np.stack([np.stack([np.real(np.fft.ifftn(1j * K[j] * uh[..., i], axes=(0, 1, 2))) for j in range(3)],
+                                  -1) for i in range(3)], -2)
+    staggered = np.zeros(cells + (3, 3))
+    for j in range(3):
+        d = np.roll(u, -1, axis=j) - u
+        for e in range(3):
+            if e != j:
+                d = np.roll(d, -1, axis=e) + d
+        staggered[..., :, j] = d / (4 * h[j])
+    err = {}
+    for derivative, grad in (('continuous', spectral), ('FWBW_difference', staggered)):
+        F = np.transpose(np.eye(3) + grad, (0, 1, 2, 4, 3)).reshape(cells + (9,)).reshape(-1, 9, order='F')
+        o = oracle_lib.OracleSpectralBasic(cells, size, np.zeros(int(np.prod(cells))), np.array([[1.0, 0, 0, 0]]),
+                                           workloads.fcc_al(), numerics_with(derivative), init=False, threads=1)
+        o.set_field('F_solver', F)
+        o.update_coords()
+        up, _ = displacements(cells, size, *o.get_coords())
+        o.close()
+        ref = u.transpose(2, 1, 0, 3).reshape(-1, 3)
+        err[derivative] = np.abs(up - ref).max() / np.abs(ref).max()
+    assert err['continuous'] < 1e-12
+    assert err['FWBW_difference'] > 0.1
