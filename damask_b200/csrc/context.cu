@@ -61,7 +61,8 @@ struct dmk_ctx {
   double geom[3];
   int64_t N = 0;
   double wgt = 0.0;
-  int NS = 0;
+  int NS = 0;                    // slip systems of the kernels (the compiled count)
+  int NSact = 0;                 // active slip systems of the phase (NS minus the inert padding)
   int precision = DMK_PRECISION_FP64;
   dmk_numerics num;
   HostPhase hp;
@@ -259,6 +260,38 @@ cudaError_t run_pick(dmk_ctx* c, const Fields& f, double dt) {
 }
 
 int nblocks_const(const dmk_ctx* c) { return int((c->N + CONST_THREADS - 1) / CONST_THREADS); }
+
+// Slip-system counts with compiled kernels are 12, 18, 24 and 48.  Any other count (the reference
+// takes any N_sl up to the family sizes) runs on the next larger one with inert systems appended:
+// zero Schmid matrices, dot_gamma_0 = 0, h_0 = 0 and zero interaction rows and columns, so they
+// never slip or harden and each term they add to a sum over systems is an exact zero.  Their
+// states (xi = 1, gamma = 0) stay on the device; field and restart accessors show the active ones.
+int padded_slip_count(int ns) {
+  for (int k : {12, 18, 24, 48})
+    if (ns <= k) return k;
+  return 0;
+}
+void pad_host_phase(HostPhase& hp, int np) {
+  const int ns = hp.Ns;
+  if (np == ns) return;
+  const std::array<double, 9> z9{};
+  const std::array<double, 6> z6{};
+  hp.P.resize(np, z9);
+  hp.Ppos.resize(np, z9);
+  hp.Pneg.resize(np, z9);
+  hp.dn.resize(np, z6);
+  hp.dg0.resize(np, 0.0);
+  hp.n.resize(np, 1.0);
+  hp.a.resize(np, 1.0);
+  hp.h0f.resize(np, 0.0);
+  hp.xiinf.resize(np, 1.0);
+  hp.xi0.resize(np, 1.0);
+  std::vector<double> h(size_t(np) * np, 0.0);
+  for (int s = 0; s < ns; ++s)
+    for (int k = 0; k < ns; ++k) h[size_t(s) * np + k] = hp.h[size_t(s) * ns + k];
+  hp.h.swap(h);
+  hp.Ns = np;
+}
 
 template <int NS>
 void fill_phase_const(const HostPhase& hp, const double* hmat, PhaseConst<NS>& pc) {
@@ -867,11 +900,13 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   dmk_ctx* c = new dmk_ctx();
   int rc = build_host_phase(*phase, c->hp, g_err);
   if (rc) { delete c; return DMK_ERR_CONFIG; }
-  c->NS = c->hp.Ns;
-  if (c->NS != 12 && c->NS != 18 && c->NS != 24 && c->NS != 48) {
+  c->NSact = c->hp.Ns;
+  if (c->NSact < 1 || padded_slip_count(c->NSact) == 0) {
     delete c;
-    return fail(DMK_ERR_CONFIG, "number of active slip systems must be 12, 18, 24 or 48 on this path");
+    return fail(DMK_ERR_CONFIG, "between 1 and 48 active slip systems on this path");
   }
+  pad_host_phase(c->hp, padded_slip_count(c->NSact));
+  c->NS = c->hp.Ns;
   c->device = device;
   c->precision = precision;
   c->num = *num;
@@ -1238,13 +1273,41 @@ int dmk_materialpoint_forward(dmk_ctx* c) {
   return 0;
 }
 
+// omega_plastic of the restart data: per voxel xi then gamma of the active systems (sizeState = 2 Ns)
+static int state_to_host(dmk_ctx* c, const double* dev_state, double* host) {
+  const int na = c->NSact;
+  if (na == c->NS) return d2h_planes(c, dev_state, host, 2 * na);
+  std::vector<double> xi(size_t(na) * c->N), ga(size_t(na) * c->N);
+  if (int rc = d2h_planes(c, dev_state, xi.data(), na)) return rc;
+  if (int rc = d2h_planes(c, dev_state + int64_t(c->NS) * c->N, ga.data(), na)) return rc;
+  for (int64_t v = 0; v < c->N; ++v)
+    for (int s = 0; s < na; ++s) {
+      host[v * 2 * na + s] = xi[v * na + s];
+      host[v * 2 * na + na + s] = ga[v * na + s];
+    }
+  return 0;
+}
+static int state_from_host(dmk_ctx* c, const double* host, double* dev_state) {
+  const int na = c->NSact;
+  if (na == c->NS) return h2d_planes(c, host, dev_state, 2 * na);
+  std::vector<double> xi(size_t(na) * c->N), ga(size_t(na) * c->N);
+  for (int64_t v = 0; v < c->N; ++v)
+    for (int s = 0; s < na; ++s) {
+      xi[v * na + s] = host[v * 2 * na + s];
+      ga[v * na + s] = host[v * 2 * na + na + s];
+    }
+  // pageable sources: each copy has left the host buffer when cudaMemcpyAsync returns
+  if (int rc = h2d_planes(c, xi.data(), dev_state, na)) return rc;
+  return h2d_planes(c, ga.data(), dev_state + int64_t(c->NS) * c->N, na);
+}
+
 int dmk_restart_write(dmk_ctx* c, dmk_restart* r) {
   if (!c || !r || !r->F || !r->F_lastinc || !r->F_phase || !r->F_p || !r->L_p || !r->omega_plastic)
     return fail(DMK_ERR_ARG, "null argument");
   int rc;
   if ((rc = d2h_planes(c, c->Fsol, r->F, 9)) || (rc = d2h_planes(c, c->Flast, r->F_lastinc, 9)) ||
       (rc = d2h_planes(c, c->F, r->F_phase, 9)) || (rc = d2h_planes(c, c->Fp, r->F_p, 9)) ||
-      (rc = d2h_planes(c, c->Lp, r->L_p, 9)) || (rc = d2h_planes(c, c->state, r->omega_plastic, 2 * c->NS)))
+      (rc = d2h_planes(c, c->Lp, r->L_p, 9)) || (rc = state_to_host(c, c->state, r->omega_plastic)))
     return rc;
   std::memcpy(r->P_aim, c->P_aim, sizeof r->P_aim);
   std::memcpy(r->F_aim, c->F_aim, sizeof r->F_aim);
@@ -1267,7 +1330,7 @@ int dmk_restart_read(dmk_ctx* c, const dmk_restart* r) {
   int rc;
   // mechanical_restartRead: the converged phase state; the current values follow at the sweep
   if ((rc = h2d_planes(c, r->F_phase, c->F0, 9)) || (rc = h2d_planes(c, r->F_p, c->Fp0, 9)) ||
-      (rc = h2d_planes(c, r->L_p, c->Lp0, 9)) || (rc = h2d_planes(c, r->omega_plastic, c->state0, 2 * c->NS)) ||
+      (rc = h2d_planes(c, r->L_p, c->Lp0, 9)) || (rc = state_from_host(c, r->omega_plastic, c->state0)) ||
       (rc = h2d_planes(c, r->F, c->Fsol, 9)) || (rc = h2d_planes(c, r->F_lastinc, c->Flast, 9)))
     return rc;
   if (c->solver == 1) {   // grid_mech_spectral_polarization.f90:236-245
@@ -1327,7 +1390,7 @@ int dmk_get_coords(dmk_ctx* c, double* ip, double* nodes) {
 
 int dmk_field_size(dmk_ctx* c, int field) {
   if (!c) return fail(DMK_ERR_ARG, "null argument");
-  if (field == DMK_FIELD_XI_SL || field == DMK_FIELD_GAMMA_SL) return c->NS;
+  if (field == DMK_FIELD_XI_SL || field == DMK_FIELD_GAMMA_SL) return c->NSact;
   if (field == DMK_FIELD_O) return 4;
   if (field >= 0 && field <= DMK_FIELD_F_SOLVER) return 9;
   if ((field == DMK_FIELD_F_TAU || field == DMK_FIELD_F_TAU_LASTINC) && c->solver == 1) return 9;
@@ -1351,8 +1414,8 @@ int dmk_get_field(dmk_ctx* c, int field, double* host) {
     case DMK_FIELD_F_TAU_LASTINC:
       if (c->solver != 1) break;
       return d2h_planes(c, c->Ftau_last, host, 9);
-    case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NS);
-    case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NS);
+    case DMK_FIELD_XI_SL: return d2h_planes(c, c->state, host, c->NSact);
+    case DMK_FIELD_GAMMA_SL: return d2h_planes(c, c->state + int64_t(c->NS) * N, host, c->NSact);
     case DMK_FIELD_S:
       if (int rc = ensure_scratch(c, 9)) return rc;
       CKL(launch_sym6_to9(c->S, c->scratch, N, c->stream));

@@ -61,7 +61,8 @@ extern "C" {
 typedef struct {
   int lattice;            /* 0 = cF, 1 = cI */
   int n_families;         /* entries used in the per-family arrays */
-  int N_sl[4];            /* active systems per family; their sum must be 12, 18, 24 or 48 */
+  int N_sl[4];            /* active systems per family, 1 to 48 in total: the kernels exist for 12, 18,
+                             24 and 48; other sums run on the next of these with inert systems */
   double C11, C12, C44;
   double dot_gamma_0[4], n[4], a[4], h_0[4], xi_0[4], xi_inf[4], c_1[4], c_2[4], f_sat[4];
   int n_h;                /* number of h_sl-sl interaction values */

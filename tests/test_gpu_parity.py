@@ -17,6 +17,25 @@ pytestmark = pytest.mark.gpu
 TOL = 1e-9
 
 
+def partial_families(lattice):
+    """Active slip-system sums without compiled kernels: cF N_sl [6] (run as 12) and cI
+    N_sl [12,12,12] (run as 48), padded with inert systems."""
+    from damask_b200.config import Phase
+    if lattice == 'cF':
+        d = {'lattice': 'cF', 'mechanical': {
+            'elastic': {'type': 'Hooke', 'C_11': 106.75e9, 'C_12': 60.41e9, 'C_44': 28.34e9},
+            'plastic': {'type': 'phenopowerlaw', 'N_sl': [6], 'a_sl': [2.25], 'dot_gamma_0_sl': [0.001],
+                        'h_0_sl-sl': [75e6], 'h_sl-sl': [1, 1, 1.4, 1.4, 1.4, 1.4, 1.4], 'n_sl': [20],
+                        'xi_0_sl': [31e6], 'xi_inf_sl': [63e6]}}}
+    else:
+        d = {'lattice': 'cI', 'mechanical': {
+            'elastic': {'type': 'Hooke', 'C_11': 233.3e9, 'C_12': 135.5e9, 'C_44': 118.0e9},
+            'plastic': {'type': 'phenopowerlaw', 'N_sl': [12, 12, 12], 'a_sl': [2.0] * 3,
+                        'dot_gamma_0_sl': [0.001] * 3, 'h_0_sl-sl': [1e9] * 3, 'h_sl-sl': [1, 1.4, 1, 1.4] + [1.4] * 24,
+                        'n_sl': [20] * 3, 'xi_0_sl': [95e6, 97e6, 97e6], 'xi_inf_sl': [222e6, 412e6, 412e6]}}}
+    return Phase.from_dict(d)
+
+
 def pair(oracle_lib, cells, grains, seed=0, phase=None, num=None, size=workloads.SIZE_1MM, precision='fp64'):
     rve = synthetic.voronoi_rve(cells, size, grains, seed)
     phase = phase or workloads.fcc_al()
@@ -36,8 +55,9 @@ def test_init_sweep(gpu, oracle_lib):
     g.close()
 
 
-@pytest.mark.parametrize('phase', [workloads.fcc_al(), workloads.bcc_24(), workloads.bcc_48()],
-                         ids=['fcc12', 'bcc24', 'bcc48'])
+@pytest.mark.parametrize('phase', [workloads.fcc_al(), workloads.bcc_24(), workloads.bcc_48(),
+                                   partial_families('cF'), partial_families('cI')],
+                         ids=['fcc12', 'bcc24', 'bcc48', 'fcc6_padded', 'bcc36_padded'])
 def test_constitutive_response_and_tangent(gpu, oracle_lib, phase):
     """utilities_constitutiveResponse and phase_mechanical_dPdF in the plastic range."""
     g, o = pair(oracle_lib, (6, 5, 4), 4, phase=phase)
@@ -87,7 +107,8 @@ def run_both(g, o, n):
     return sg, so
 
 
-@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'bcc48_anderson'])
+@pytest.mark.parametrize('case', ['fcc16_anderson', 'fcc8_richardson', 'bcc8_anderson', 'bcc48_anderson',
+                                  'bcc36_padded'])
 def test_solver_parity(gpu, oracle_lib, case):
     """grid_mechanical_spectral_basic_{forward,solution} + materialpoint_forward over several
     increments of uniaxial tension: per-voxel fields within 1e-9, identical iteration counts."""
@@ -97,6 +118,8 @@ def test_solver_parity(gpu, oracle_lib, case):
     elif case == 'fcc8_richardson':
         num.PETSc_options = '-snes_type nrichardson'
         g, o, n = *pair(oracle_lib, (8, 8, 8), 6, num=num), 3
+    elif case == 'bcc36_padded':
+        g, o, n = *pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=partial_families('cI')), 2
     elif case == 'bcc48_anderson':
         # all three cI families, N_sl [12,12,24]
         g, o, n = *pair(oracle_lib, (8, 8, 8), 10, seed=3, phase=workloads.bcc_48()), 2

@@ -52,3 +52,25 @@ def test_restart_rejects_mismatched_data(gpu):
     with pytest.raises(ValueError):
         g.restart_read(d)
     g.close()
+
+
+def test_restart_state_of_padded_phase(gpu):
+    """A phase whose active slip systems run on a larger compiled count (cF N_sl [6] on 12) writes
+    and reads omega_plastic with the active systems only (xi then gamma per voxel, sizeState = 2 Ns)."""
+    from test_gpu_parity import partial_families
+    rve = synthetic.voronoi_rve((6, 6, 6), workloads.SIZE_1MM, 4, 2)
+    ph = partial_families('cF')
+    args = (rve.cells, rve.size, rve.material, rve.quaternions, ph, workloads.numerics_default())
+    a = SpectralBasic(*args)
+    drv = IncrementDriver(a, workloads.tension_x(60.0, 60))
+    for _ in range(3):
+        drv.step()
+    d = a.restart_write()
+    xi, ga = a.get_field('xi_sl'), a.get_field('gamma_sl')
+    assert xi.shape == ga.shape == (a.N, 6) and np.abs(ga).max() > 0.0
+    assert np.array_equal(d['omega_plastic'][:, :6], xi) and np.array_equal(d['omega_plastic'][:, 6:], ga)
+    a.close()
+    b = SpectralBasic(*args)
+    b.restart_read(d)
+    assert np.array_equal(b.restart_write()['omega_plastic'], d['omega_plastic'])
+    b.close()
