@@ -68,7 +68,7 @@ def test_nonschmid_product_vs_oracle(oracle_lib):
 
 
 @pytest.mark.parametrize('ph', [workloads.fcc_al(), workloads.bcc_24(), phase('cF', [12, 6]),
-                                phase('cI', [12, 12, 24])])
+                                phase('cI', [12, 12, 24]), phase('cF', [6]), phase('cI', [12, 12, 12])])
 def test_interaction_product_vs_oracle(oracle_lib, ph):
     h = product_interaction(ph)
     assert np.array_equal(h, oracle_lib.interaction(ph))
