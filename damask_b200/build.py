@@ -9,6 +9,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
@@ -51,15 +52,19 @@ def build(verbose: bool = False, force: bool = False) -> Path:
     common = ARCH + ['-O3', '-lineinfo', '-std=c++17', '-Xcompiler', '-fPIC', '-Xcompiler', '-O3'] + _host_cxx()
     if verbose:
         common += ['-Xptxas', '-v']
-    objs = []
+    cmds, objs = [], []
     for src in SOURCES:
         obj = objdir / (Path(src).stem + '.o')
         cmd = [nvcc] + common + ['-c', str(CSRC / src), '-o', str(obj)]
         if src.endswith('.cpp'):
             cxx = '/usr/bin/g++' if Path('/usr/bin/g++').exists() else (shutil.which('g++') or 'g++')
             cmd = [cxx, '-O3', '-std=c++17', '-fPIC', '-c', str(CSRC / src), '-o', str(obj)]
-        subprocess.run(cmd, check=True)
+        cmds.append(cmd)
         objs.append(str(obj))
+    # the translation units are independent: compile them concurrently
+    with ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.run, cmd, check=True) for cmd in cmds]:
+            f.result()
     tmp = LIB.with_suffix('.so.tmp')
     subprocess.run([nvcc] + ARCH + _host_cxx() + ['-shared', '-o', str(tmp)] + objs + ['-lcufft', '-lcudart', '-lz'], check=True)
     os.replace(tmp, LIB)
