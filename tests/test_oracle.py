@@ -319,3 +319,18 @@ def test_update_coords_inverts_gradients_of_purely_imaginary_frequencies(oracle_
         err[derivative] = np.abs(up - ref).max() / np.abs(ref).max()
     assert err['continuous'] < 1e-12
     assert err['FWBW_difference'] > 0.1
+
+
+@pytest.mark.parametrize('derivative', ['continuous', 'central_difference', 'FWBW_difference'])
+@pytest.mark.parametrize('cells', [(5, 6, 7), (6, 4, 8)])
+def test_gamma_output_is_curl_free(oracle_lib, derivative, cells):
+    """Gamma_hat : tau_hat = (K^-1 tau_hat conj(xi)) (x) xi is a gradient for the same first-derivative
+    frequencies that utilities_curlRMS uses (spectral_utilities.f90:697-757), so its curl RMS vanishes
+    for each of the three derivatives, including the complex FWBW ones."""
+    o = small_oracle(oracle_lib, cells=cells, num=numerics_with(derivative))
+    tau = np.random.default_rng(13).normal(size=(o.N, 9)) * 1e8
+    g = o.gamma_convolution(tau, np.zeros(9))
+    F = g + np.eye(3).reshape(-1)
+    assert o.curl_rms(F) < 1e-12 * np.abs(g).max()
+    assert o.curl_rms(F + 1e-3 * np.abs(g).max() * np.random.default_rng(14).normal(size=F.shape)) > 1e-6 * np.abs(g).max()
+    o.close()
