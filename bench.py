@@ -45,10 +45,15 @@ def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> 
     return newton * (264 + 56 * ns) + steps * (567 + 135 * ns) + state * (455 + 86 * ns) + updates * (89 * ns)
 
 
-# DRAM bytes that the constitutive kernels move per material-point update, from the ncu
-# capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (64^3 cut of this
-# workload; the traffic grows with the number of voxels)
-TRAFFIC_BYTES_PER_UPDATE = 9428
+# DRAM bytes that the constitutive kernels move per material-point update, by slip-system count,
+# from the ncu capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (64^3 cut of
+# the workload; the traffic grows with the number of voxels)
+TRAFFIC_BYTES_PER_UPDATE = {24: 9428}
+
+# the 48-system RVE's window inside the default bench line (5.7 s per increment at 256^3)
+BCC48_WARMUP, BCC48_STEPS = 3, 3
+# timed increments of the CPU baseline leg (after the headline's warm-up window)
+CPU_STEPS = 3
 
 
 def bc_bytes() -> int:
@@ -197,48 +202,45 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     drv = IncrementDriver(solver, lcs)
     p_av = []
 
-    def one_step(e2e_buf=None):
+    def one_step():
         c0, t0 = solver.total_counters.copy(), solver.total_ms.copy()
         recs = drv.step()
         c = solver.total_counters - c0
         tm = solver.total_ms - t0
-        if e2e_buf is not None:
-            solver.get_field('P', out=e2e_buf)
         p_av.extend(r.P_av for r in recs)
         return recs, c, tm
 
     for _ in range(warmup):
         one_step()
-    # timed region: inputs resident in HBM, device time on the solver's stream
+    # timed region: inputs resident in HBM, device time on the solver's stream.  Each step is
+    # timed twice from the same increment: the increment itself (value) and, end to end through
+    # the public API, the increment plus the read-back of its stress field P into pinned host
+    # memory (e2e; the boundary conditions enter from host memory inside the increment).
+    pinned = torch.empty((solver.N, 9), dtype=torch.float64, pin_memory=True).numpy()
     barrier(world)
     clocks = ClockSampler(local)
     clocks.start()
     launches0 = solver.launches()
-    solver.timer_start()
     upd = newton = state = evals = 0
-    const_ms = 0.0
+    const_ms = ms = ms_e2e = 0.0
     for _ in range(steps):
+        solver.timer_start()
         recs, c, tm = one_step()
+        ms_step = solver.timer_stop()
+        solver.timer_start()
+        solver.get_field('P', out=pinned)
+        ms_copy = solver.timer_stop()
+        ms += ms_step
+        ms_e2e += ms_step + ms_copy
         upd += c[0]
         state += c[1]
         newton += c[2]
         evals += c[3]
         const_ms += tm[0]
-    ms = solver.timer_stop()
     launches = solver.launches() - launches0
     clk = clocks.stop()
     barrier(world)
-    # end to end through the public API: per step the BCs go in from host memory
-    # and the stress field P comes back into pinned host memory
-    pinned = torch.empty((solver.N, 9), dtype=torch.float64, pin_memory=True).numpy()
-    barrier(world)
-    solver.timer_start()
-    upd_e2e = 0
-    for _ in range(steps):
-        recs, c, _tm = one_step(e2e_buf=pinned)
-        upd_e2e += c[0]
-    ms_e2e = solver.timer_stop()
-    barrier(world)
+    upd_e2e = upd
     out = {'updates': upd, 'ms': ms, 'newton': newton, 'state': state, 'evals': evals, 'const_ms': const_ms,
            'launches': launches, 'clocks': clk, 'updates_e2e': upd_e2e, 'ms_e2e': ms_e2e, 'N': solver.N,
            'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8, 'device_gb': device_gb}
@@ -246,9 +248,10 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     return out
 
 
-def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None, workload: str = WORKLOAD) -> dict:
-    """The CPU restatement on the same material and load, on a 48^3 cut of the
-    workload's statistics (13 grains, seed 3), first increments; ~10-30 s of work."""
+def cpu_sample(steps: int = 5, warmup: int = 5, threads: int | None = None, workload: str = WORKLOAD) -> dict:
+    """The CPU restatement on the same material and load, on a 48^3 cut of the workload at its
+    grain density (13 grains, seed 3): `warmup` untimed increments, then `steps` timed ones
+    (the increment window of the GPU figures: after the same warm-up, the same load)."""
     from damask_b200 import workloads
     from damask_b200.grid import IncrementDriver
     from damask_b200.synthetic import voronoi_rve
@@ -272,9 +275,10 @@ def cpu_sample(steps: int = 2, warmup: int = 0, threads: int | None = None, work
     dt = time.perf_counter() - t0
     o.close()
     return {'value': upd / dt, 'seconds': dt, 'cores': threads, 'updates': upd,
-            'sample': f'oracle (C++ FP64, OpenMP) on a 48^3 RVE, 13 grains, same {phase.n_slip}-system material and '
-                      f'tension load, '
-                      f'increments {warmup + 1}..{warmup + steps}'}
+            'warmup': warmup, 'increments_timed': f'{warmup + 1}..{warmup + steps}',
+            'sample': f'oracle (C++ FP64, OpenMP, {threads} threads) on a 48^3 RVE, 13 grains, same '
+                      f'{phase.n_slip}-system material and tension load, increments {warmup + 1}..{warmup + steps} '
+                      f'after {warmup} untimed warm-up increments'}
 
 
 def _json_default(o):
@@ -314,6 +318,59 @@ def run_batch(args) -> None:
     print(json.dumps(line, default=_json_default), flush=True)
 
 
+def measure(workload, steps, warmup, world, rank, local, cells, solver, derivative, precision) -> dict:
+    """Both precisions of one workload over the same increment window; the figures of a bench line."""
+    res = {}
+    precs = ('mixed', 'fp64') if precision == 'both' else (precision,)
+    for prec in precs:
+        res[prec] = run_gpu(prec, steps, warmup, world, rank, local, cells, solver, workload, derivative)
+    mx = res.get('mixed', res.get('fp64'))
+    fp = res.get('fp64', mx)
+    ms_max = allreduce_max(mx['ms'], world)
+    value = allreduce_sum(mx['updates'], world) / (ms_max * 1e-3)
+    fp_ms = allreduce_max(fp['ms'], world)
+    fp_value = allreduce_sum(fp['updates'], world) / (fp_ms * 1e-3)
+    e2e_ms = allreduce_max(mx['ms_e2e'], world)
+    e2e_value = allreduce_sum(mx['updates_e2e'], world) / (e2e_ms * 1e-3)
+    # agreement of the volume-averaged stress of the mixed and FP64 runs, increment by increment
+    rel = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(mx['p_av'], fp['p_av'])]
+    peaks = load_peaks()
+    fp64_peak, fp64_source = measure_fp64_peak(local)
+    ns = mx['ns']
+    bpu = constitutive_bytes(ns)
+    avg_launch_ms = mx['const_ms'] / max(1, mx['evals'])
+    achieved_gbs = bpu * mx['N'] / (avg_launch_ms * 1e-3) / 1e9
+    flops = constitutive_flops(ns, mx['newton'], mx['state'], mx['updates'])
+    fp64_tflops = flops / (mx['const_ms'] * 1e-3) / 1e12
+    traffic = TRAFFIC_BYTES_PER_UPDATE.get(ns)
+    roofline = {
+        'bound': 'fp64',
+        'kernel': 'constitutive update (begin + stress/control pass kernels), one evaluation of all voxels',
+        'achieved': fp64_tflops, 'peak': fp64_peak, 'unit': 'TFLOP/s', 'frac': fp64_tflops / fp64_peak,
+        'peak_source': fp64_source, 'nominal_peak': FP64_NOMINAL_TFLOPS,
+        'flops_per_update': flops / max(1, mx['updates']),
+        'flop_source': 'static FP64 count of the kernels times the counted Newton / state iterations',
+        'traffic': traffic * mx['N'] if traffic else None,
+        'traffic_source': f'ncu DRAM bytes per update at 64^3 ({ns} systems), times the voxels of one evaluation',
+        'avg_launch_ms': avg_launch_ms,
+        'hbm': {'achieved': achieved_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved_gbs / peaks['hbm_gbs'],
+                'peak_source': peaks['source'], 'bytes_per_update': bpu},
+        'fp64': {'achieved': fp64_tflops, 'peak': fp64_peak, 'unit': 'TFLOP/s', 'frac': fp64_tflops / fp64_peak},
+    }
+    return {'mixed': mx, 'fp64_raw': fp, 'value': value, 'ms_per_step': ms_max / steps,
+            'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / steps},
+            's_per_increment': {'mixed': ms_max / steps * 1e-3, 'fp64': fp_ms / steps * 1e-3},
+            'mixed_over_fp64': value / fp_value, 'P_av_rel_err': max(rel) if rel else None,
+            'roofline': roofline,
+            'e2e': {'value': e2e_value, 'unit': 'updates/s', 'h2d_bytes_per_step': bc_bytes(),
+                    'd2h_bytes_per_step': mx['d2h_bytes'],
+                    'how': 'the same increments as value: each increment plus the read-back of its P field into '
+                           'pinned host memory through dmk_get_field'},
+            'iterations': {'newton_per_update': mx['newton'] / max(1, mx['updates']),
+                           'state_per_update': mx['state'] / max(1, mx['updates']),
+                           'residual_evals': mx['evals']}}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -322,6 +379,7 @@ def main():
     ap.add_argument('--impl', choices=['ours', 'reference'], default='ours')
     ap.add_argument('--cells', type=str, default=None, help='override grid (testing only)')
     ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-bcc48', action='store_true', help='leave out the 48-system key of the bench line')
     ap.add_argument('--precision', choices=['both', 'mixed', 'fp64'], default='both',
                     help='run one precision only (profiling); the bench line needs both')
     ap.add_argument('--solver', choices=['spectral_basic', 'spectral_polarization'], default='spectral_basic',
@@ -344,43 +402,29 @@ def main():
     if args.impl == 'reference':
         if rank != 0:
             return
-        s = cpu_sample(steps=max(1, args.steps), warmup=0, workload=args.workload)
+        # the same increment window as this implementation's timed region: W untimed warm-up
+        # increments, then K timed ones, on the bounded 48^3 sample
+        s = cpu_sample(steps=max(1, args.steps), warmup=warmup, workload=args.workload)
         line = {'metric': METRIC, 'value': s['value'], 'unit': 'updates/s', 'n_gpus': args.gpus, 'steps': args.steps,
-                'warmup': 0, 'ms_per_step': 1e3 * s['seconds'] / max(1, args.steps), 'higher_is_better': True,
+                'warmup': warmup, 'ms_per_step': 1e3 * s['seconds'] / max(1, args.steps), 'higher_is_better': True,
                 'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
-                'impl': 'reference',
+                'impl': 'reference', 'warmup_match': True,
                 'config': {'workload': f'{args.workload}: bcc phenopowerlaw RVE, tension 1e-3/s (48^3 bounded '
-                                       'sample of the 256^3/2000-grain workload)', 'solver': 'Anderson fixed point'},
+                                       'sample of the 256^3/2000-grain workload)', 'solver': 'Anderson fixed point',
+                           'increments_timed': s['increments_timed']},
                 'cpu_baseline': {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port',
                                  'sample': s['sample']},
                 'e2e': {'value': s['value'], 'unit': 'updates/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}}
         print(json.dumps(line, default=_json_default), flush=True)
         return
 
-    res = {}
-    precs = ('mixed', 'fp64') if args.precision == 'both' else (args.precision,)
-    for prec in precs:
-        res[prec] = run_gpu(prec, args.steps, warmup, world, rank, local, cells, args.solver, args.workload,
-                            args.derivative)
-    mx = res.get('mixed', res.get('fp64'))
-    fp = res.get('fp64', mx)
-    ms_max = allreduce_max(mx['ms'], world)
-    upd_tot = allreduce_sum(mx['updates'], world)
-    value = upd_tot / (ms_max * 1e-3)
-    fp_ms = allreduce_max(fp['ms'], world)
-    fp_value = allreduce_sum(fp['updates'], world) / (fp_ms * 1e-3)
-    e2e_ms = allreduce_max(mx['ms_e2e'], world)
-    e2e_value = allreduce_sum(mx['updates_e2e'], world) / (e2e_ms * 1e-3)
-    # agreement of the volume-averaged stress of the mixed and FP64 runs, increment by increment
-    rel = [float(np.abs(a - b).max() / np.abs(b).max()) for a, b in zip(mx['p_av'], fp['p_av'])]
-    peaks = load_peaks()
-    fp64_peak, fp64_source = measure_fp64_peak(local)
-    ns = mx['ns']
-    bpu = constitutive_bytes(ns)
-    avg_launch_ms = mx['const_ms'] / max(1, mx['evals'])
-    achieved_gbs = bpu * mx['N'] / (avg_launch_ms * 1e-3) / 1e9
-    flops = constitutive_flops(ns, mx['newton'], mx['state'], mx['updates'])
-    fp64_tflops = flops / (mx['const_ms'] * 1e-3) / 1e12
+    headline = measure(args.workload, args.steps, warmup, world, rank, local, cells, args.solver, args.derivative,
+                       args.precision)
+    # the 48-system RVE of the same grid (all three cI families), on a short window
+    b48 = None
+    if args.workload == WORKLOAD and cells is None and not args.no_bcc48 and args.precision == 'both':
+        b48 = measure('grid256_bcc48_2000g', BCC48_STEPS, BCC48_WARMUP, world, rank, local, None, args.solver,
+                      args.derivative, 'both')
     if world > 1:
         import torch.distributed as dist
         dist.destroy_process_group()
@@ -388,11 +432,12 @@ def main():
         return
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        s = cpu_sample(workload=args.workload)
+        s = cpu_sample(steps=CPU_STEPS, warmup=warmup, workload=args.workload)
         cpu = {'value': s['value'], 'unit': 'updates/s', 'cores': s['cores'], 'kind': 'port', 'sample': s['sample']}
+    mx = headline['mixed']
     line = {
-        'metric': METRIC, 'value': value, 'unit': 'updates/s', 'n_gpus': world, 'steps': args.steps,
-        'warmup': warmup, 'ms_per_step': ms_max / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'metric': METRIC, 'value': headline['value'], 'unit': 'updates/s', 'n_gpus': world, 'steps': args.steps,
+        'warmup': warmup, 'ms_per_step': headline['ms_per_step'], 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'f64 constitutive, f32 spectral (mixed)', 'data': 'synthetic',
         'config': {'workload': f'{args.workload}: 256^3 grid, 2000 Voronoi grains (seed 3), bcc N_sl '
                                f'{"[12,12,24]" if "bcc48" in args.workload else "[12,12]"}, '
@@ -401,31 +446,27 @@ def main():
                    'solver': f"{args.solver.replace('spectral_', '')} spectral, Anderson fixed point (m=8)"
                              + ('' if args.derivative == 'continuous' else f', derivative {args.derivative}'),
                    'precision': 'mixed',
-                   'parallelism': f'replicas x{world}', 'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
+                   'parallelism': f'replicas x{world}',
+                   'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
                    'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
-        'fp64': {'value': fp_value, 'unit': 'updates/s', 'ms_per_step': fp_ms / args.steps},
-        's_per_increment': {'mixed': ms_max / args.steps * 1e-3, 'fp64': fp_ms / args.steps * 1e-3},
-        'mixed_over_fp64': value / fp_value,
-        'mixed_vs_fp64_P_av_rel_err_max': max(rel) if rel else None,
-        'roofline': {'bound': 'hbm', 'kernel': 'constitutive update (begin + stress/control pass kernels), one '
-                                               'evaluation of all voxels',
-                     'achieved': achieved_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s',
-                     'frac': achieved_gbs / peaks['hbm_gbs'], 'peak_source': peaks['source'],
-                     'traffic': TRAFFIC_BYTES_PER_UPDATE * mx['N'] if args.workload == WORKLOAD else None,
-                     'traffic_source': 'ncu at 64^3 (bcc N_sl [12,12]), scaled by voxels',
-                     'bytes_per_update': bpu, 'avg_launch_ms': avg_launch_ms,
-                     'fp64': {'achieved': fp64_tflops, 'peak': fp64_peak, 'unit': 'TFLOP/s',
-                              'frac': fp64_tflops / fp64_peak, 'peak_source': fp64_source,
-                              'nominal': FP64_NOMINAL_TFLOPS}},
+        'fp64': headline['fp64'],
+        's_per_increment': headline['s_per_increment'],
+        'mixed_over_fp64': headline['mixed_over_fp64'],
+        'mixed_vs_fp64_P_av_rel_err_max': headline['P_av_rel_err'],
+        'roofline': headline['roofline'],
         'cpu_baseline': cpu,
-        'e2e': {'value': e2e_value, 'unit': 'updates/s', 'h2d_bytes_per_step': bc_bytes(),
-                'd2h_bytes_per_step': mx['d2h_bytes']},
+        'e2e': headline['e2e'],
         'gpu_launches': mx['launches'],
         'clocks': mx['clocks'],
-        'iterations': {'newton_per_update': mx['newton'] / max(1, mx['updates']),
-                       'state_per_update': mx['state'] / max(1, mx['updates']),
-                       'residual_evals': mx['evals']},
+        'iterations': headline['iterations'],
     }
+    if b48 is not None:
+        line['bcc48'] = {'workload': 'grid256_bcc48_2000g: the same RVE with N_sl [12,12,24] (48 systems)',
+                         'value': b48['value'], 'unit': 'updates/s', 'fp64': b48['fp64'],
+                         'mixed_over_fp64': b48['mixed_over_fp64'], 'P_av_rel_err': b48['P_av_rel_err'],
+                         'increments_timed': f'{BCC48_WARMUP + 1}..{BCC48_WARMUP + BCC48_STEPS}',
+                         's_per_increment': b48['s_per_increment'], 'roofline_fp64': b48['roofline']['fp64'],
+                         'clocks': b48['mixed']['clocks']}
     print(json.dumps(line, default=_json_default), flush=True)
 
 

@@ -13,7 +13,6 @@
 
 #include <cuda_runtime.h>
 
-#include <mutex>
 #include <string>
 
 namespace dmk {
@@ -30,9 +29,6 @@ constexpr int64_t NA_MAX_VOXELS = NA_VOXELS_PER_BLOCK * NA_MAX_BLOCKS;
 
 // 9 partial sums per block, then the 9 results: 147,465 doubles = 1.13 MiB per GPU
 static __device__ __align__(256) double g_mean_scratch[NA_MAX_BLOCKS * 9 + 9];
-
-std::mutex g_na_mutex;
-double* g_na_ptr[64] = {nullptr};      // device address of g_mean_scratch, per device ordinal
 
 __global__ void __launch_bounds__(NA_THREADS)
 na_partial_kernel(const double* __restrict__ f, int64_t n, double* __restrict__ part) {
@@ -69,25 +65,23 @@ __global__ void na_final_kernel(const double* __restrict__ part, int nblocks, do
   out[k] = t * scale;
 }
 
-// Set-up, once per device, with that device current: the device address of the array.
+// Set-up, with the calling thread's current device: the device address of the array on that
+// device.  It is looked up on every call (a table lookup once the library's device code is
+// loaded on the device) rather than cached, so it stays right after the host resets a device.
 int na_scratch(double** ptr) {
   int dev = -1;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= 64) {
+  if (e != cudaSuccess || dev < 0) {
     dmk::set_last_error(std::string("dmk_field_mean_noalloc: no current CUDA device: ") + cudaGetErrorString(e));
     return DMK_ERR_CUDA;
   }
-  std::lock_guard<std::mutex> lock(g_na_mutex);
-  if (!g_na_ptr[dev]) {
-    double* p = nullptr;
-    e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_mean_scratch);
-    if (e != cudaSuccess || !p) {
-      dmk::set_last_error(std::string("dmk_field_mean_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
-      return DMK_ERR_CUDA;
-    }
-    g_na_ptr[dev] = p;
+  double* p = nullptr;
+  e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_mean_scratch);
+  if (e != cudaSuccess || !p) {
+    dmk::set_last_error(std::string("dmk_field_mean_noalloc: cudaGetSymbolAddress failed: ") + cudaGetErrorString(e));
+    return DMK_ERR_CUDA;
   }
-  *ptr = g_na_ptr[dev];
+  *ptr = p;
   return 0;
 }
 

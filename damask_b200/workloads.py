@@ -92,6 +92,17 @@ def make(name: str, cells=None) -> tuple[RVE, Phase, list[LoadCase], Numerics]:
     return rve, phase, tension_x(t, N), numerics_default()
 
 
+def make_cut(name: str, cells) -> tuple[RVE, Phase, list[LoadCase], Numerics]:
+    """A smaller RVE of a workload at the workload's grain density (grains scaled by the cell
+    count, at least 2) with its seed, material, load and numerics: e.g. a 64^3 cut of the
+    256^3/2000-grain RVE has 31 grains."""
+    c, grains, seed, ph, t, N = WORKLOADS[name]
+    cells = tuple(int(x) for x in cells)
+    g = max(2, int(round(grains * np.prod(cells) / np.prod(c))))
+    rve = voronoi_rve(cells, SIZE_1MM, g, seed)
+    return rve, PHASES[ph](), tension_x(t, N), numerics_default()
+
+
 def material_yaml(rve: RVE, phase_name: str, phase: dict) -> dict:
     """material.yaml content (one constituent per material, isostrain homogenization)."""
     return {'homogenization': {'direct': {'N_constituents': 1, 'mechanical': {'type': 'isostrain'}}},

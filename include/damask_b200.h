@@ -158,7 +158,9 @@ int dmk_mech_forward(dmk_ctx* ctx, int cutBack, int guess, double dt, double dt_
                      const dmk_bc* deformation, const dmk_bc* stress, const double q_rot[4]);
 
 /* grid_mechanical_spectral_basic_solution, grid_mech_spectral_basic.f90:243-277.
-   The residual is iterated as a Richardson fixed point F <- F - r(F). */
+   The residual r(F) is driven to zero by the fixed-point iteration that dmk_numerics.snes_type
+   selects: Anderson-accelerated (the default, standing in for the reference's
+   -snes_type ngmres) or the Richardson iteration F <- F - r(F) (-snes_type nrichardson). */
 int dmk_mech_solution(dmk_ctx* ctx, dmk_solution_state* out);
 
 /* materialpoint_forward -> mechanical_forward, phase_mechanical.f90:987-1002 */
@@ -330,12 +332,12 @@ int dmk_timer_stop(dmk_ctx* ctx, double* ms);
    and its implicit device synchronisation are not allowed).  It allocates nothing: its
    partial sums live in a fixed 1.13 MiB device array that every GPU loading the library
    holds until the process exits.  n_voxels is limited to 16,777,216 (256^3); larger
-   sizes are rejected with DMK_ERR_ARG.  The first call on a device looks up that array's
-   device address (once per device, with the device current); make that first call
-   before any stream capture.  All calls share the array: calls that overlap on the GPU
-   (different streams or threads) race; each call overwrites what it uses, so no state
-   carries over.  stream: a cudaStream_t, or NULL for the default stream; the call waits
-   for the result. */
+   sizes are rejected with DMK_ERR_ARG.  Every call looks up that array's device address on the
+   current device (cudaGetSymbolAddress); the first lookup on a device loads the library's device
+   code there, so make the first call on each device before any stream capture.  All calls share
+   the array: calls that overlap on the GPU (different streams or threads) race; each call
+   overwrites what it uses, so no state carries over.  stream: a cudaStream_t, or NULL for the
+   default stream; the call copies the result to `mean` and synchronises `stream` before it returns. */
 int dmk_field_mean_noalloc(const double* field, int64_t n_voxels, double mean[9], void* stream);
 
 void dmk_destroy(dmk_ctx* ctx);

@@ -2,7 +2,7 @@
 
 Run here (where the reference tree is mounted), not on the test machines:
 
-    python tests/golden/make_golden.py /root/reference
+    python tests/golden/make_golden.py <path of the reference's source tree>
 
 The reference package is imported piecewise: its optional I/O dependencies
 (h5py, vtk, matplotlib) are replaced by inert stand-ins because none of the
@@ -87,4 +87,6 @@ def main(root: str) -> None:
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit(f'usage: python {sys.argv[0]} <path of the reference source tree>')
+    main(sys.argv[1])

@@ -2,7 +2,7 @@
 
 Run here (where the reference tree is mounted), not on the test machines:
 
-    python tests/golden/make_golden_17grains.py /root/reference
+    python tests/golden/make_golden_17grains.py <path of the reference's source tree>
 
 Source: ``tests/integration/resources/plastic_detect_changes/`` of the reference, the
 inputs and stored result of ``tests/integration/test_plastic_detect_changes.py`` for
@@ -108,4 +108,6 @@ def main(root: str) -> None:
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit(f'usage: python {sys.argv[0]} <path of the reference source tree>')
+    main(sys.argv[1])

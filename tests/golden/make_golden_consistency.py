@@ -2,7 +2,7 @@
 
 Run here (where the reference tree is mounted), not on the test machines:
 
-    python tests/golden/make_golden_consistency.py /root/reference
+    python tests/golden/make_golden_consistency.py <path of the reference's source tree>
 
 Source: ``tests/integration/resources/grid_mech_consistency/`` of the reference, the inputs
 of ``tests/integration/test_grid_mech_consistency.py`` for the plastic case: the 4x4x4 grid of
@@ -40,4 +40,6 @@ def main(root: str) -> None:
 
 
 if __name__ == '__main__':
-    main(sys.argv[1] if len(sys.argv) > 1 else '/root/reference')
+    if len(sys.argv) != 2:
+        sys.exit(f'usage: python {sys.argv[0]} <path of the reference source tree>')
+    main(sys.argv[1])

@@ -8,13 +8,15 @@ the reference's own recipe: uniform seeds, Gaussian quaternions, periodic Vorono
   form (FP32 FFT/Gamma/field update, FP64 constitutive update and correction sweep), <P>
   within 1e-5 at every increment; the first two increments of the FP64 form against the oracle.
 """
+import os
+
 import numpy as np
 import pytest
 
 from damask_b200 import workloads
 from damask_b200.grid import SpectralBasic, run_load_cases
 
-from conftest import rel
+from conftest import assert_fields, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -30,7 +32,7 @@ def test_grid16_fcc_full_run(gpu, oracle_lib):
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < 1e-9, a.inc
     for name in ('P', 'F', 'F_p', 'L_p', 'xi_sl', 'gamma_sl', 'O'):
-        assert rel(g.get_field(name), o.get_field(name)) < 1e-9, name
+        assert_fields(g, o, [name], 1e-9)
     for a, b in zip(g.get_coords(), o.get_coords()):
         assert rel(a, b) < 1e-9
     g.close()
@@ -51,3 +53,68 @@ def test_grid64_fcc_mixed_against_fp64(gpu, oracle_lib):
     for a, b in zip(runs['fp64'][:2], so):
         assert a.iterations == b.iterations
         assert rel(a.P_av, b.P_av) < 1e-9
+
+
+class Counted:
+    """Wraps a solver so that the constitutive counters of every solution call are summed:
+    evaluations x voxels, state iterations, Newton iterations, residual evaluations."""
+
+    def __init__(self, s):
+        self.s, self.total = s, np.zeros(4, dtype=np.int64)
+
+    def __getattr__(self, k):
+        return getattr(self.s, k)
+
+    def solution(self):
+        out = self.s.solution()
+        self.total += self.s.counters()
+        return out
+
+
+def _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, n, names=('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl')):
+    g = Counted(SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num))
+    o = Counted(oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num,
+                                               threads=os.cpu_count() or 8))
+    sg = run_load_cases(g, lcs, max_increments=n)
+    so = run_load_cases(o, lcs, max_increments=n)
+    assert len(sg) == len(so) == n
+    assert [s.iterations for s in sg] == [s.iterations for s in so]
+    assert all(s.converged for s in sg)
+    for a, b in zip(sg, so):
+        assert rel(a.P_av, b.P_av) < 1e-9, a.inc
+    # equal constitutive work: evaluations, state iterations and Newton iterations in total
+    assert list(g.total) == list(o.total), (g.total, o.total)
+    assert_fields(g, o, names, 1e-9)
+    g.s.close()
+    return sg, g.total
+
+
+@pytest.mark.parametrize('workload', ['grid256_bcc24_2000g', 'grid256_bcc48_2000g'])
+def test_headline_workload_cut_fp64_against_oracle(gpu, oracle_lib, workload):
+    """A 64^3 cut of the 256^3 bench RVE (same seed, same grain density: 31 grains) and material,
+    three increments of the tension load (the third in the plastic range), FP64 CUDA path against
+    the oracle: <P> per increment, per-voxel P, F, F_p, L_p, S, xi, gamma (both metrics), equal
+    fixed-point iteration counts and equal Newton / state iteration totals."""
+    rve, phase, lcs, num = workloads.make_cut(workload, (64, 64, 64))
+    sg, tot = _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, 3)
+    print(f'{workload} 64^3 cut: iterations {[s.iterations for s in sg]}, counters {list(tot)}')
+
+
+def test_grid64_fcc_ten_increments_against_oracle(gpu, oracle_lib):
+    """The 64^3 / 200-grain fcc workload, FP64 CUDA path against the oracle over its first ten
+    increments (elastic-plastic transition included)."""
+    rve, phase, lcs, num = workloads.make('grid64_fcc_200g')
+    _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, 10)
+
+
+def test_anderson_depth_30(gpu, oracle_lib):
+    """The fixed point at PETSc's default NGMRES history depth (m = 30) on the 16^3 fcc workload:
+    the CUDA path and the oracle take the same iterations; the counts are printed next to the
+    m = 8 default's."""
+    rve, phase, lcs, num = workloads.make('grid16_fcc_20g')
+    its = {}
+    for m in (30, 8):
+        num.anderson_m = m
+        sg, _ = _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, 10)
+        its[m] = [s.iterations for s in sg]
+    print(f'fixed-point iterations per increment, m=30: {its[30]}; m=8: {its[8]}')

@@ -10,7 +10,7 @@ import pytest
 from damask_b200 import synthetic, workloads
 from damask_b200.grid import SpectralBasic, run_load_cases
 
-from conftest import rel
+from conftest import assert_fields, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -71,7 +71,7 @@ def test_constitutive_response_and_tangent(gpu, oracle_lib, phase):
     assert rel(Pg, Po) < TOL and rel(Pavg, Pavo) < TOL
     assert rel(Cvg, Cvo) < TOL and rel(Cmg, Cmo) < TOL
     for name in ('F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'F_e'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     assert rel(g.dPdF(1.0), o.dPdF(1.0)) < TOL
     it = g.iteration_counts()
     assert it[:, 0].min() >= 1 and it[:, 1].min() >= 1 and np.all(it[:, 3] == 0)
@@ -130,7 +130,7 @@ def test_solver_parity(gpu, oracle_lib, case):
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < TOL
     for name in ('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl', 'O'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     assert rel(g.aims()['C_volAvg'], o.aims()['C_volAvg']) < TOL
     # coordinates of the last updateCoords (after every converged increment)
     for a, b in zip(g.get_coords(), o.get_coords()):
@@ -225,7 +225,7 @@ def test_quasi_2d_grids(gpu, oracle_lib, cells, solver):
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < TOL
     for name in ('P', 'F', 'F_p', 'xi_sl', 'gamma_sl'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     for a, b in zip(g.get_coords(), o.get_coords()):
         assert rel(a, b) < TOL
     g.close()
@@ -256,7 +256,7 @@ def test_boundary_condition_types(gpu, oracle_lib, load):
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < TOL
     for name in ('P', 'F', 'xi_sl'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     for k in ('F_aim', 'P_aim'):
         assert rel(g.aims()[k], o.aims()[k]) < TOL, k
     g.close()
@@ -325,7 +325,7 @@ def test_numerics_options(gpu, oracle_lib, option):
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < TOL
     for name in ('P', 'F', 'xi_sl'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     g.close()
 
 
@@ -364,5 +364,5 @@ def test_two_and_three_voxel_chunks(gpu, oracle_lib, cells):
     assert [s.iterations for s in sg] == [s.iterations for s in so]
     assert rel(sg[0].P_av, so[0].P_av) < TOL
     for name in ('P', 'xi_sl', 'gamma_sl'):
-        assert rel(g.get_field(name), o.get_field(name)) < TOL, name
+        assert_fields(g, o, [name], TOL)
     g.close()

@@ -45,6 +45,27 @@ def test_noalloc_mean_matches_constitutive_response(gpu):
     g.close()
 
 
+def test_noalloc_many_blocks_and_tail_allocates_nothing(gpu):
+    """A 33^3 field spans 36 partial-sum blocks of 1024 voxels, the last one partly filled:
+    the final sum over several block slots and the tail are exercised.  Repeated calls leave
+    the device's free memory unchanged (no allocation), and give the same mean each time."""
+    import torch
+    lib = _lib.load()
+    n = 33 ** 3
+    rng = np.random.default_rng(5)
+    host = rng.normal(size=(9, n)) * 1e8 + np.arange(9)[:, None] * 1e7
+    planes = torch.tensor(host, dtype=torch.float64, device='cuda')
+    torch.cuda.synchronize()
+    first = _mean_noalloc(lib, planes.data_ptr(), n)         # set-up happens here, before measuring
+    free0 = torch.cuda.mem_get_info()[0]
+    means = [_mean_noalloc(lib, planes.data_ptr(), n) for _ in range(20)]
+    torch.cuda.synchronize()
+    assert torch.cuda.mem_get_info()[0] == free0
+    ref = host.mean(axis=1)
+    assert np.abs(first - ref).max() / np.abs(ref).max() < TOL
+    assert all(np.array_equal(m, first) for m in means)      # fixed summation order
+
+
 def test_noalloc_rejects_oversized_grid(gpu):
     lib = _lib.load()
     out = np.zeros(9)
