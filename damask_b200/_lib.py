@@ -22,7 +22,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_phase_interaction', 'dmk_field_mean_noalloc', 'dmk_restart_write', 'dmk_restart_read',
            'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems', 'dmk_vti_open', 'dmk_vti_geometry',
            'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
-           'dmk_grid_run_ctx', 'dmk_fp64_peak']
+           'dmk_grid_run_ctx', 'dmk_fp64_peak', 'dmk_checkpoint_save', 'dmk_checkpoint_restore', 'dmk_adj_begin',
+           'dmk_adj_record', 'dmk_adj_step', 'dmk_adj_finish', 'dmk_adj_local_jacobian']
 
 _lib = None
 
@@ -88,6 +89,13 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_phase_schmid': (C.c_int, [C.POINTER(PhaseStruct), C.c_int, dp]),
         'dmk_phase_interaction': (C.c_int, [C.POINTER(PhaseStruct), dp]),
         'dmk_field_mean_noalloc': (C.c_int, [C.c_void_p, C.c_int64, dp, C.c_void_p]),
+        'dmk_checkpoint_save': (C.c_int, [vp, C.c_int]),
+        'dmk_checkpoint_restore': (C.c_int, [vp, C.c_int]),
+        'dmk_adj_begin': (C.c_int, [vp, C.c_int]),
+        'dmk_adj_record': (C.c_int, [vp, C.c_int]),
+        'dmk_adj_step': (C.c_int, [vp, C.c_int, dp, dp, ip]),
+        'dmk_adj_finish': (C.c_int, [vp, dp]),
+        'dmk_adj_local_jacobian': (C.c_int, [C.POINTER(PhaseStruct), C.c_double, dp, dp]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

@@ -117,7 +117,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         double s0[6];
 #pragma unroll
         for (int k = 0; k < 6; ++k) s0[k] = f.S0[k * N + v];
-        bad = dot_state_slots<NS>(pc, hs, s0, f.state0, N, v, xs, nullptr);
+        bad = dot_state_slots<NS>(pc, hs, s0, f.state0, N, v, xs, nullptr, 0);
 #pragma unroll 12
         for (int i = 0; i < NST; ++i) w.dot0[i * N + v] = xs[i * pass_threads<NS>()];
       }
@@ -135,7 +135,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
         for (int i = 0; i < NST; ++i) f.state[i * N + v] = f.state0[i * N + v];
         c.status = 3;
         c.phase = PH_CTRL;
-        advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
+        advance<NS>(pc, hs, nm, f, w, v, dt, c, xs, nullptr, 0);
       } else {
         const double dts = c.step * dt;
         double* D0 = w.D + v;                               // dotState generation 0
@@ -235,7 +235,7 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
     v = list_in[idx];
     VoxelCtl c;
     load_ctl(w, N, v, c);
-    advance<NS>(pc, hs, nm, f, w, v, dt, c, xs);
+    advance<NS>(pc, hs, nm, f, w, v, dt, c, xs, w.adg + v, N);
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
     if (!keep) finish_voxel(f, v, c);

@@ -324,17 +324,18 @@ __host__ __device__ constexpr int stress_slots() { return 3 * NS + 27; }
 
 // phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0) at the stored
 // stress and state of voxel v, written to this thread's slots: xi rates first, then
-// |dot_gamma|.  hs: the hardening matrix in shared memory.  adg_in (stride N), when given,
-// holds |dot_gamma| at this stress and state already (the kinetics of the converged
-// integrateStress); otherwise the kinetics are evaluated.  Returns true if any rate is NaN.
+// |dot_gamma|.  hs: the hardening matrix (shared memory, or device memory read with uniform
+// addresses).  adg_in (element s at adg_in[s * adg_stride]), when given, holds |dot_gamma| at
+// this stress and state already (the kinetics of the converged integrateStress); otherwise
+// the kinetics are evaluated.  Returns true if any rate is NaN.
 template <int NS>
 __device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double* __restrict__ hs, const double s6[6],
                                 const double* __restrict__ state, int64_t N, int64_t v, double* xs,
-                                const double* __restrict__ adg_in) {
+                                const double* adg_in, int64_t adg_stride) {
   double adg[NS];
   if (adg_in) {
 #pragma unroll
-    for (int s = 0; s < NS; ++s) adg[s] = adg_in[s * N];
+    for (int s = 0; s < NS; ++s) adg[s] = adg_in[s * adg_stride];
   } else {
 #pragma unroll
     for (int s = 0; s < NS; ++s) {
@@ -396,10 +397,12 @@ __device__ __forceinline__ double* dot_gen(const PassWork& w, int it, int NST, i
 // Advances voxel v through the control flow of phase_mechanical_constitutive and
 // integrateStateFPI until its next integrateStress (phase PH_STRESS) or its end
 // (PH_DONE).  Entered in PH_CTRL (substep control after an integration attempt) or
-// PH_DOT1 (state update after a successful integrateStress).
+// PH_DOT1 (state update after a successful integrateStress, whose |dot_gamma| is at
+// adg[s * adg_stride]).
 template <int NS>
 __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs, const Numerics& nm, const Fields& f,
-                        const PassWork& w, int64_t v, double dt, VoxelCtl& c, double* xs) {
+                        const PassWork& w, int64_t v, double dt, VoxelCtl& c, double* xs, const double* adg,
+                        int64_t adg_stride) {
   constexpr int NST = 2 * NS;
   const int64_t N = f.N;
   // every control step shrinks the substep or advances stepFrac; the bound only
@@ -452,7 +455,7 @@ __device__ void advance(const PhaseConst<NS>& pc, const double* __restrict__ hs,
       if (!after_stress)
 #pragma unroll
         for (int k = 0; k < 6; ++k) s6[k] = f.S[k * N + v];
-      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state, N, v, xs, after_stress ? w.adg + v : nullptr);
+      const bool bad = dot_state_slots<NS>(pc, hs, s6, f.state, N, v, xs, after_stress ? adg : nullptr, adg_stride);
       const double dts = c.step * dt;
       if (c.phase == PH_DOT0) {
         // integrateStateFPI:616-620

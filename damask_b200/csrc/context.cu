@@ -2,6 +2,7 @@
 // cuFFT plans, solver scalars) and the grid_mechanical_spectral_basic_* entry points.
 #include "../../include/damask_b200.h"
 #include "kernels.cuh"
+#include "adjoint.cuh"
 #include "lattice.h"
 
 #include <cufft.h>
@@ -10,6 +11,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -71,6 +73,7 @@ struct dmk_ctx {
   PhaseConst<24>* pc24 = nullptr;
   PhaseConst<48>* pc48 = nullptr;
   double* hmat = nullptr;        // slip-slip hardening matrix (NS x NS), read by the pass kernels
+  SysConst* sysc = nullptr;      // per-system constants of the Newton loop (NS entries)
   Numerics nm;
   Numerics2 nm2;
   GammaConst gc;
@@ -141,6 +144,30 @@ struct dmk_ctx {
   int* pcount = nullptr;         // [2 h + k]: entries appended to plist[h][k]
   int* hcount = nullptr;         // pinned host copies of the current counts of the chunks
   int64_t passes = 0;            // constitutive passes launched (all evaluations)
+
+  // device checkpoints (dmk_checkpoint_save / _restore): per slot, the per-voxel state and the
+  // device solver scalars in one device buffer, the host solver state in a host vector
+  struct Checkpoint {
+    double* dev = nullptr;
+    std::vector<double> host;
+  };
+  std::vector<Checkpoint> ckpts;
+
+  // adjoint of increments (dmk_adj_*)
+  int adj_slots = 0, adj_nx = 0, adj_nz = 0;
+  double* adj_pts = nullptr;       // per slot: the linearization point, 27 + 2 NS planes (F, Fp0, xi0, Lp, xi)
+  std::vector<double> adj_dt;      // per slot: time step of the increment
+  std::vector<std::array<int, 9>> adj_mask;   // per slot: stress mask of the load case (1 = not prescribed)
+  std::vector<char> adj_rec;       // per slot: recorded
+  double* adj_s = nullptr;         // 2 x (9 + NS) planes: state cotangent (Fp, xi), current and next
+  int adj_cur = 0;
+  double* adj_D = nullptr;         // nz x nx planes: the local Jacobians of the increment being reversed
+  double* adj_ws = nullptr;        // workspace of the local Jacobian, adj_chunk voxels
+  int64_t adj_chunk = 0;
+  double *adj_G = nullptr, *adj_lam = nullptr, *adj_sig = nullptr, *adj_w = nullptr;   // 9 planes each
+  double* adj_V = nullptr;         // Krylov basis: ADJ_KRYLOV_MAX + 1 fields of 9 planes
+  double* adj_part = nullptr;      // per-block partial sums
+  int* adj_bad = nullptr;          // voxels whose local Jacobian was singular
 };
 
 namespace {
@@ -286,6 +313,8 @@ void pad_host_phase(HostPhase& hp, int np) {
   hp.h0f.resize(np, 0.0);
   hp.xiinf.resize(np, 1.0);
   hp.xi0.resize(np, 1.0);
+  hp.fam.resize(np, -1);
+  hp.hfac.resize(np, 0.0);
   std::vector<double> h(size_t(np) * np, 0.0);
   for (int s = 0; s < ns; ++s)
     for (int k = 0; k < ns; ++k) h[size_t(s) * np + k] = hp.h[size_t(s) * ns + k];
@@ -334,6 +363,12 @@ void fill_phase_const(const HostPhase& hp, const double* hmat, PhaseConst<NS>& p
   }
   pc.atol_xi = hp.atol_xi;
   pc.atol_gamma = hp.atol_gamma;
+  for (int s = 0; s < NS; ++s) {
+    pc.fam[s] = hp.fam[s];
+    pc.hfac[s] = hp.hfac[s];
+  }
+  pc.nf = hp.nf;
+  std::memcpy(pc.th, hp.th, sizeof pc.th);
 }
 
 // host rotations (rotations.f90:282-339, P = -1)
@@ -595,15 +630,18 @@ void update_gamma_host(dmk_ctx* c, const double* C) {
 }
 
 // D2Z of the committed P, fused divergence + Gamma, Z2D into r (FP64 or FP32 spectral path)
-int spectral_pass(dmk_ctx* c, bool fp32, int do_gamma, int do_div, void* out) {
+// Gamma convolution (do_gamma, into out, DC from the device scalars' aim_rot) and divergence
+// partial sums (do_div) of the 9-plane field `in` (the stress P unless given).
+int spectral_pass(dmk_ctx* c, bool fp32, int do_gamma, int do_div, void* out, double* in = nullptr) {
   const double L[3] = {c->geom[0], c->geom[1], c->geom[2]};
+  if (!in) in = c->P;
   if (!fp32) {
-    CKF(cufftExecD2Z(c->plan_fwd, c->P, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
+    CKF(cufftExecD2Z(c->plan_fwd, in, reinterpret_cast<cufftDoubleComplex*>(c->spec)));
     CK(launch_gamma_div<double>(c->spec, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, do_gamma,
                                 do_div, c->stream));
     if (do_gamma) CKF(cufftExecZ2D(c->plan_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), static_cast<double*>(out)));
   } else {
-    CKL(launch_to_float(c->P, c->Pf, 9 * c->N, c->nsm, c->stream));
+    CKL(launch_to_float(in, c->Pf, 9 * c->N, c->nsm, c->stream));
     CKF(cufftExecR2C(c->plan_fwd_f, c->Pf, reinterpret_cast<cufftComplex*>(c->specf)));
     CK(launch_gamma_div<float>(c->specf, c->cells[0], c->cells[1], c->cells[2], L, c->gc, c->sc, c->div_partials, do_gamma,
                                do_div, c->stream));
@@ -956,6 +994,27 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     case 18: c->pc18 = new PhaseConst<18>(); fill_phase_const<18>(c->hp, c->hmat, *c->pc18); break;
     case 24: c->pc24 = new PhaseConst<24>(); fill_phase_const<24>(c->hp, c->hmat, *c->pc24); break;
     case 48: c->pc48 = new PhaseConst<48>(); fill_phase_const<48>(c->hp, c->hmat, *c->pc48); break;
+  }
+  {
+    // per-system constants of the Newton loop, staged into shared memory by the pass kernels
+    std::vector<SysConst> sys(c->NS);
+    for (int i = 0; i < c->NS; ++i) {
+      switch (c->NS) {
+        case 12: sys[i] = make_sys_const<12>(*c->pc12, i); break;
+        case 18: sys[i] = make_sys_const<18>(*c->pc18, i); break;
+        case 24: sys[i] = make_sys_const<24>(*c->pc24, i); break;
+        case 48: sys[i] = make_sys_const<48>(*c->pc48, i); break;
+      }
+    }
+    if (cudaMalloc(&c->sysc, sizeof(SysConst) * c->NS) != cudaSuccess ||
+        cudaMemcpy(c->sysc, sys.data(), sizeof(SysConst) * c->NS, cudaMemcpyHostToDevice) != cudaSuccess)
+      return bail(fail(DMK_ERR_CUDA, "copy of the per-system constants failed"));
+    switch (c->NS) {
+      case 12: c->pc12->sys = c->sysc; break;
+      case 18: c->pc18->sys = c->sysc; break;
+      case 24: c->pc24->sys = c->sysc; break;
+      case 48: c->pc48->sys = c->sysc; break;
+    }
   }
 
   const int NST = 2 * c->NS;
@@ -1687,6 +1746,12 @@ void dmk_destroy(dmk_ctx* c) {
                   (void*)c->pw, (void*)c->pctl, (void*)c->pcount, (void*)c->dot0, (void*)c->xp, (void*)c->xn, (void*)c->favg,
                   (void*)c->Ftau_last, (void*)c->Ftau_dot, (void*)c->Feval, (void*)c->curl_partials})
     if (p) cudaFree(p);
+  for (auto& ck : c->ckpts)
+    if (ck.dev) cudaFree(ck.dev);
+  for (void* p : {(void*)c->adj_pts, (void*)c->adj_s, (void*)c->adj_D, (void*)c->adj_ws, (void*)c->adj_G,
+                  (void*)c->adj_lam, (void*)c->adj_sig, (void*)c->adj_w, (void*)c->adj_V, (void*)c->adj_part,
+                  (void*)c->adj_bad})
+    if (p) cudaFree(p);
   for (auto& l : c->plist)
     for (int* p : l)
       if (p) cudaFree(p);
@@ -1706,7 +1771,379 @@ void dmk_destroy(dmk_ctx* c) {
   delete c->pc24;
   delete c->pc48;
   if (c->hmat) cudaFree(c->hmat);
+  if (c->sysc) cudaFree(c->sysc);
   delete c;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ checkpoints and the adjoint
+namespace {
+
+// The per-voxel buffers whose values carry from one increment to the next (basic scheme).
+std::vector<std::pair<double*, size_t>> state_buffers(dmk_ctx* c) {
+  const size_t N = size_t(c->N), NST = size_t(2 * c->NS);
+  return {{c->Fsol, 9 * N}, {c->Flast, 9 * N}, {c->Fdot, 9 * N}, {c->F, 9 * N},  {c->F0, 9 * N},
+          {c->Fp, 9 * N},   {c->Fp0, 9 * N},   {c->Lp, 9 * N},   {c->Lp0, 9 * N}, {c->S, 6 * N},
+          {c->S0, 6 * N},   {c->Fe, 9 * N},    {c->P, 9 * N},    {c->Pnew, 9 * N}, {c->state, NST * N},
+          {c->state0, NST * N}, {c->dot0, NST * N}};
+}
+constexpr size_t SC_DOUBLES = (sizeof(SolverScalars) + sizeof(double) - 1) / sizeof(double);
+
+// host solver state, packed in a fixed order
+template <bool SAVE>
+void pack_host(dmk_ctx* c, std::vector<double>& h) {
+  size_t o = 0;
+  auto io = [&](double* p, size_t n) {
+    if (SAVE) h.insert(h.end(), p, p + n);
+    else std::copy(h.begin() + o, h.begin() + o + n, p);
+    o += n;
+  };
+  io(c->F_aim, 9); io(c->F_aim_lastinc, 9); io(c->F_aimDot, 9); io(c->P_aim, 9); io(c->P_av, 9);
+  io(c->C_volAvg, 81); io(c->C_volAvgLastInc, 81); io(c->C_minMaxAvg, 81); io(c->C_minMaxAvgLastInc, 81);
+  io(c->Scomp, 81); io(c->C_gamma, 81); io(c->q_rot, 4); io(&c->dt, 1); io(c->h_aim, 9);
+  double ints[10];
+  for (int k = 0; k < 9; ++k) ints[k] = c->stress_mask[k];
+  ints[9] = c->dot0_valid ? 1.0 : 0.0;
+  io(ints, 10);
+  if (!SAVE) {
+    for (int k = 0; k < 9; ++k) c->stress_mask[k] = int(ints[k]);
+    c->dot0_valid = ints[9] != 0.0;
+  }
+}
+
+bool is_identity_rotation(const double* q) { return q[0] == 1.0 && q[1] == 0.0 && q[2] == 0.0 && q[3] == 0.0; }
+
+int adj_jacobians(dmk_ctx* c, int slot) {
+  const int64_t N = c->N;
+  const double* pts = c->adj_pts + size_t(slot) * size_t(27 + 2 * c->NS) * size_t(N);
+  CK(cudaMemsetAsync(c->adj_bad, 0, sizeof(int), c->stream));
+  for (int64_t v0 = 0; v0 < N; v0 += c->adj_chunk) {
+    const int64_t cnt = std::min<int64_t>(c->adj_chunk, N - v0);
+    const double dt = c->adj_dt[slot];
+    switch (c->NS) {
+      case 12: CKL(launch_adj_jacobian<12>(*c->pc12, dt, pts, N, v0, cnt, c->adj_ws, c->adj_D, c->adj_bad, c->stream)); break;
+      case 18: CKL(launch_adj_jacobian<18>(*c->pc18, dt, pts, N, v0, cnt, c->adj_ws, c->adj_D, c->adj_bad, c->stream)); break;
+      case 24: CKL(launch_adj_jacobian<24>(*c->pc24, dt, pts, N, v0, cnt, c->adj_ws, c->adj_D, c->adj_bad, c->stream)); break;
+      case 48: CKL(launch_adj_jacobian<48>(*c->pc48, dt, pts, N, v0, cnt, c->adj_ws, c->adj_D, c->adj_bad, c->stream)); break;
+    }
+  }
+  int bad = 0;
+  CK(cudaMemcpyAsync(&bad, c->adj_bad, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  if (bad) return fail(DMK_ERR_STATE, "adjoint: singular local Jacobian in " + std::to_string(bad) + " voxels");
+  return 0;
+}
+
+int adj_vjp(dmk_ctx* c, const double ell[9], const double* lam, int mode) {
+  const double* s_in = c->adj_s + size_t(c->adj_cur) * size_t(9 + c->NS) * size_t(c->N);
+  double* s_out = c->adj_s + size_t(1 - c->adj_cur) * size_t(9 + c->NS) * size_t(c->N);
+  switch (c->NS) {
+    case 12: CKL(launch_adj_vjp<12>(c->adj_D, c->N, c->adj_nx, ell, lam, s_in, c->adj_G, s_out, c->adj_part, mode, c->stream)); break;
+    case 18: CKL(launch_adj_vjp<18>(c->adj_D, c->N, c->adj_nx, ell, lam, s_in, c->adj_G, s_out, c->adj_part, mode, c->stream)); break;
+    case 24: CKL(launch_adj_vjp<24>(c->adj_D, c->N, c->adj_nx, ell, lam, s_in, c->adj_G, s_out, c->adj_part, mode, c->stream)); break;
+    case 48: CKL(launch_adj_vjp<48>(c->adj_D, c->N, c->adj_nx, ell, lam, s_in, c->adj_G, s_out, c->adj_part, mode, c->stream)); break;
+  }
+  return 0;
+}
+
+// fixed-order host sum of per-block partials: out[k] = sum_b part[b * K + k]
+int sum_partials(dmk_ctx* c, const double* dev, int nblocks, int K, double* out) {
+  std::vector<double> h(size_t(nblocks) * K);
+  CK(cudaMemcpyAsync(h.data(), dev, sizeof(double) * h.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int k = 0; k < K; ++k) out[k] = 0.0;
+  for (int b = 0; b < nblocks; ++b)
+    for (int k = 0; k < K; ++k) out[k] += h[size_t(b) * K + k];
+  return 0;
+}
+
+// y = M x (+ the affine part for G != null): sigma = K^T x - G, then the Gamma convolution of sigma
+// with the reference medium of the forward solver, whose average is replaced by S_m : <sigma>
+// (S_m: the masked compliance, non-zero on the stress-controlled components only).
+int adj_apply(dmk_ctx* c, const double* x, const double* G, const double* Sm, double* y) {
+  const int nb = adj_blocks(c->N);
+  CKL(launch_adj_sigma(c->adj_D, c->N, c->adj_nx, x, G, c->adj_sig, c->adj_part, c->stream));
+  double m9[9];
+  if (int rc = sum_partials(c, c->adj_part, nb, 9, m9)) return rc;
+  double dc[9];
+  for (int a = 0; a < 9; ++a) {
+    double s = 0.0;
+    for (int b = 0; b < 9; ++b) s += Sm[a + 9 * b] * m9[b] * c->wgt;
+    dc[a] = s;
+  }
+  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_rot), dc, 9 * sizeof(double),
+                     cudaMemcpyHostToDevice, c->stream));
+  return spectral_pass(c, false, 1, 0, y, c->adj_sig);
+}
+
+int adj_dots(dmk_ctx* c, const double* w, const double* V, int nv, double* out) {
+  CKL(launch_adj_mdot(w, V, 9 * c->N, nv, c->adj_part, c->nsm, c->stream));
+  return sum_partials(c, c->adj_part, adj_mdot_blocks(c->nsm), nv, out);
+}
+
+// Restarted GMRES (Saad & Schultz 1986) with classical Gram-Schmidt and one reorthogonalisation
+// for M lam = b, b = -(M 0 with G); lam starts at zero.  Returns the iterations in *its.
+int adj_solve(dmk_ctx* c, const double* Sm, double rtol, int* its, double* relres) {
+  const int m = ADJ_KRYLOV_MAX;
+  const int64_t n9 = 9 * c->N;
+  double* V = c->adj_V;
+  auto Vj = [&](int j) { return V + size_t(j) * size_t(n9); };
+  CK(cudaMemsetAsync(c->adj_lam, 0, sizeof(double) * n9, c->stream));
+  if (int rc = adj_apply(c, c->adj_lam, c->adj_G, Sm, c->adj_w)) return rc;   // w = -b
+  CKL(launch_adj_scale(Vj(0), c->adj_w, -1.0, n9, c->nsm, c->stream));
+  double beta2;
+  if (int rc = adj_dots(c, Vj(0), Vj(0), 1, &beta2)) return rc;
+  const double bnorm = std::sqrt(beta2);
+  double beta = bnorm;
+  *its = 0;
+  *relres = 0.0;
+  if (!(bnorm > 0.0)) return 0;
+  for (int restart = 0; restart < 40; ++restart) {
+    CKL(launch_adj_scale(Vj(0), Vj(0), 1.0 / beta, n9, c->nsm, c->stream));
+    std::vector<double> H(size_t(m + 1) * m, 0.0), g(m + 1, 0.0), cs(m, 0.0), sn(m, 0.0);
+    g[0] = beta;
+    int jend = 0;
+    double res = beta;
+    for (int j = 0; j < m; ++j) {
+      if (int rc = adj_apply(c, Vj(j), nullptr, Sm, c->adj_w)) return rc;
+      double h[ADJ_KRYLOV_MAX + 1], h2[ADJ_KRYLOV_MAX + 1], neg[ADJ_KRYLOV_MAX + 1];
+      if (int rc = adj_dots(c, c->adj_w, V, j + 1, h)) return rc;
+      for (int i = 0; i <= j; ++i) neg[i] = -h[i];
+      CKL(launch_adj_maxpy(c->adj_w, V, n9, j + 1, neg, c->nsm, c->stream));
+      if (int rc = adj_dots(c, c->adj_w, V, j + 1, h2)) return rc;
+      for (int i = 0; i <= j; ++i) { neg[i] = -h2[i]; h[i] += h2[i]; }
+      CKL(launch_adj_maxpy(c->adj_w, V, n9, j + 1, neg, c->nsm, c->stream));
+      double hn2;
+      if (int rc = adj_dots(c, c->adj_w, c->adj_w, 1, &hn2)) return rc;
+      const double hn = std::sqrt(hn2);
+      for (int i = 0; i <= j; ++i) H[size_t(i) * m + j] = h[i];
+      H[size_t(j + 1) * m + j] = hn;
+      // Givens rotations
+      for (int i = 0; i < j; ++i) {
+        const double a = H[size_t(i) * m + j], b = H[size_t(i + 1) * m + j];
+        H[size_t(i) * m + j] = cs[i] * a + sn[i] * b;
+        H[size_t(i + 1) * m + j] = -sn[i] * a + cs[i] * b;
+      }
+      const double a = H[size_t(j) * m + j], b = H[size_t(j + 1) * m + j];
+      const double r = std::hypot(a, b);
+      cs[j] = r > 0.0 ? a / r : 1.0;
+      sn[j] = r > 0.0 ? b / r : 0.0;
+      H[size_t(j) * m + j] = r;
+      H[size_t(j + 1) * m + j] = 0.0;
+      g[j + 1] = -sn[j] * g[j];
+      g[j] = cs[j] * g[j];
+      res = std::fabs(g[j + 1]);
+      ++*its;
+      jend = j + 1;
+      if (res <= rtol * bnorm || !(hn > 0.0)) break;
+      CKL(launch_adj_scale(Vj(j + 1), c->adj_w, 1.0 / hn, n9, c->nsm, c->stream));
+    }
+    // lam += V y, H y = g (upper triangular)
+    std::vector<double> yv(jend, 0.0);
+    for (int i = jend - 1; i >= 0; --i) {
+      double s = g[i];
+      for (int k = i + 1; k < jend; ++k) s -= H[size_t(i) * m + k] * yv[k];
+      yv[i] = s / H[size_t(i) * m + i];
+    }
+    CKL(launch_adj_maxpy(c->adj_lam, V, n9, jend, yv.data(), c->nsm, c->stream));
+    // true residual b - M lam
+    if (int rc = adj_apply(c, c->adj_lam, c->adj_G, Sm, c->adj_w)) return rc;
+    CKL(launch_adj_scale(Vj(0), c->adj_w, -1.0, n9, c->nsm, c->stream));
+    double r2;
+    if (int rc = adj_dots(c, Vj(0), Vj(0), 1, &r2)) return rc;
+    beta = std::sqrt(r2);
+    *relres = beta / bnorm;
+    if (beta <= rtol * bnorm || !(beta > 0.0)) return 0;
+  }
+  return fail(DMK_ERR_NOT_CONVERGED, "adjoint: the transposed equilibrium problem did not converge (relative residual " +
+                                         std::to_string(*relres) + ")");
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmk_checkpoint_save(dmk_ctx* c, int slot) {
+  if (!c || slot < 0) return fail(DMK_ERR_ARG, "checkpoint: null context or negative slot");
+  if (c->solver != 0) return fail(DMK_ERR_CONFIG, "checkpoints are implemented for the basic spectral scheme");
+  CK(cudaSetDevice(c->device));
+  if (size_t(slot) >= c->ckpts.size()) c->ckpts.resize(slot + 1);
+  auto& ck = c->ckpts[slot];
+  const auto bufs = state_buffers(c);
+  size_t total = SC_DOUBLES;
+  for (const auto& b : bufs) total += b.second;
+  if (!ck.dev)
+    if (int rc = dalloc(&ck.dev, total)) return rc;
+  size_t o = 0;
+  for (const auto& b : bufs) {
+    CK(cudaMemcpyAsync(ck.dev + o, b.first, sizeof(double) * b.second, cudaMemcpyDeviceToDevice, c->stream));
+    o += b.second;
+  }
+  CK(cudaMemcpyAsync(ck.dev + o, c->sc, sizeof(SolverScalars), cudaMemcpyDeviceToDevice, c->stream));
+  ck.host.clear();
+  pack_host<true>(c, ck.host);
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_checkpoint_restore(dmk_ctx* c, int slot) {
+  if (!c || slot < 0 || size_t(slot) >= c->ckpts.size() || !c->ckpts[slot].dev)
+    return fail(DMK_ERR_ARG, "checkpoint: no checkpoint in this slot");
+  CK(cudaSetDevice(c->device));
+  auto& ck = c->ckpts[slot];
+  size_t o = 0;
+  for (const auto& b : state_buffers(c)) {
+    CK(cudaMemcpyAsync(b.first, ck.dev + o, sizeof(double) * b.second, cudaMemcpyDeviceToDevice, c->stream));
+    o += b.second;
+  }
+  CK(cudaMemcpyAsync(c->sc, ck.dev + o, sizeof(SolverScalars), cudaMemcpyDeviceToDevice, c->stream));
+  pack_host<false>(c, ck.host);
+  update_gamma_host(c, c->C_gamma);
+  CK(cudaStreamSynchronize(c->stream));
+  return 0;
+}
+
+int dmk_adj_begin(dmk_ctx* c, int n_slots) {
+  if (!c || n_slots < 1) return fail(DMK_ERR_ARG, "adjoint: null context or no slots");
+  if (c->solver != 0) return fail(DMK_ERR_CONFIG, "the adjoint is implemented for the basic spectral scheme");
+  CK(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  const int NS = c->NS;
+  const int nf = c->hp.nf;
+  if (nf < 1 || nf > ADJ_MAX_FAMILIES) return fail(DMK_ERR_CONFIG, "adjoint: unsupported number of slip families");
+  if (n_slots != c->adj_slots) {
+    if (c->adj_pts) cudaFree(c->adj_pts);
+    c->adj_pts = nullptr;
+    if (int rc = dalloc(&c->adj_pts, size_t(n_slots) * size_t(27 + 2 * NS) * size_t(N))) return rc;
+    c->adj_slots = n_slots;
+  }
+  c->adj_nx = adj_nx(NS, nf);
+  c->adj_nz = adj_nz(NS);
+  if (!c->adj_s) {
+    const int64_t per = adj_ws_size(NS, nf);
+    c->adj_chunk = std::max<int64_t>(128, std::min<int64_t>(N, (int64_t(1) << 28) / (8 * per)));
+    const int nbv = std::max(adj_blocks(N) * 16, adj_mdot_blocks(c->nsm) * (ADJ_KRYLOV_MAX + 1));
+    if (int rc = dalloc(&c->adj_s, 2 * size_t(9 + NS) * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_D, size_t(c->adj_nz) * size_t(c->adj_nx) * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_ws, size_t(per) * size_t(c->adj_chunk))) return rc;
+    if (int rc = dalloc(&c->adj_G, 9 * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_lam, 9 * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_sig, 9 * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_w, 9 * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_V, size_t(ADJ_KRYLOV_MAX + 1) * 9 * size_t(N))) return rc;
+    if (int rc = dalloc(&c->adj_part, size_t(nbv))) return rc;
+    if (int rc = dalloc(&c->adj_bad, 1)) return rc;
+  }
+  c->adj_dt.assign(n_slots, 0.0);
+  c->adj_mask.assign(n_slots, std::array<int, 9>{});
+  c->adj_rec.assign(n_slots, 0);
+  c->adj_cur = 0;
+  CK(cudaMemsetAsync(c->adj_s, 0, sizeof(double) * 2 * size_t(9 + NS) * size_t(N), c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->iter_enabled = true;          // per-voxel substep counts, checked when an increment is recorded
+  return 0;
+}
+
+int dmk_adj_record(dmk_ctx* c, int slot) {
+  if (!c || slot < 0 || slot >= c->adj_slots) return fail(DMK_ERR_ARG, "adjoint: slot out of range (call dmk_adj_begin)");
+  CK(cudaSetDevice(c->device));
+  if (!is_identity_rotation(c->q_rot)) return fail(DMK_ERR_CONFIG, "adjoint: load-case rotation R must be the identity");
+  const int64_t N = c->N;
+  const int NS = c->NS;
+  // one substep per voxel (the local model is that of a single substep) and no failed voxel
+  std::vector<int> it(2 * size_t(N));
+  CK(cudaMemcpyAsync(it.data(), c->iter + 2 * N, sizeof(int) * 2 * N, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  for (int64_t v = 0; v < N; ++v) {
+    if (it[size_t(N + v)] != 0) return fail(DMK_ERR_STATE, "adjoint: the increment has failed voxels");
+    if (it[size_t(v)] != 1)
+      return fail(DMK_ERR_STATE, "adjoint: a voxel needed substeps in this increment (the adjoint covers single substeps)");
+  }
+  double* p = c->adj_pts + size_t(slot) * size_t(27 + 2 * NS) * size_t(N);
+  const size_t N9 = 9 * size_t(N), NN = size_t(NS) * size_t(N);
+  CK(cudaMemcpyAsync(p, c->F, sizeof(double) * N9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(p + N9, c->Fp0, sizeof(double) * N9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(p + 2 * N9, c->state0, sizeof(double) * NN, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(p + 2 * N9 + NN, c->Lp, sizeof(double) * N9, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaMemcpyAsync(p + 3 * N9 + NN, c->state, sizeof(double) * NN, cudaMemcpyDeviceToDevice, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->adj_dt[slot] = c->dt;
+  for (int k = 0; k < 9; ++k) c->adj_mask[slot][k] = c->stress_mask[k];
+  c->adj_rec[slot] = 1;
+  return 0;
+}
+
+int dmk_adj_step(dmk_ctx* c, int slot, const double P_av_bar[9], double theta_bar[20], int* iterations) {
+  if (!c || !P_av_bar || !theta_bar) return fail(DMK_ERR_ARG, "null argument");
+  if (slot < 0 || slot >= c->adj_slots || !c->adj_rec[slot]) return fail(DMK_ERR_ARG, "adjoint: slot not recorded");
+  CK(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  const int NS = c->NS;
+  const int nf = c->hp.nf;
+  if (int rc = adj_jacobians(c, slot)) return rc;
+  // masked compliance of the transposed average tangent (stress-controlled components only)
+  double CT[81], Sm[81];
+  for (int i = 0; i < 3; ++i) for (int j = 0; j < 3; ++j) for (int k = 0; k < 3; ++k) for (int l = 0; l < 3; ++l)
+    CT[k + 3 * l + 9 * i + 27 * j] = c->C_volAvg[i + 3 * j + 9 * k + 27 * l];
+  const double qI[4] = {1.0, 0.0, 0.0, 0.0};
+  if (int rc = masked_compliance(qI, c->adj_mask[slot].data(), CT, Sm)) return rc;
+  // G = (dP/dF)^T ell + (ds/dF)^T s_hat
+  if (int rc = adj_vjp(c, P_av_bar, nullptr, 0)) return rc;
+  int its = 0;
+  double relres = 0.0;
+  if (int rc = adj_solve(c, Sm, 1.0e-12, &its, &relres)) return rc;
+  if (iterations) *iterations = its;
+  // state cotangent of the increment start and the parameter cotangent
+  if (int rc = adj_vjp(c, P_av_bar, c->adj_lam, 1)) return rc;
+  double th[4 * ADJ_MAX_FAMILIES];
+  if (int rc = sum_partials(c, c->adj_part, adj_blocks(N), 4 * ADJ_MAX_FAMILIES, th)) return rc;
+  for (int p = 0; p < 4; ++p)
+    for (int f = 0; f < nf; ++f) theta_bar[(1 + p) * ADJ_MAX_FAMILIES + f] += th[p * nf + f] / double(N);
+  c->adj_cur = 1 - c->adj_cur;
+  (void)NS;
+  return 0;
+}
+
+int dmk_adj_finish(dmk_ctx* c, double theta_bar[20]) {
+  if (!c || !theta_bar) return fail(DMK_ERR_ARG, "null argument");
+  CK(cudaSetDevice(c->device));
+  const int64_t N = c->N;
+  const int NS = c->NSact;
+  std::vector<double> s(size_t(NS) * size_t(N));
+  const double* xi_bar = c->adj_s + size_t(c->adj_cur) * size_t(9 + c->NS) * size_t(N) + 9 * size_t(N);
+  CK(cudaMemcpyAsync(s.data(), xi_bar, sizeof(double) * s.size(), cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  // xi(t = 0) = xi_0 of the system's family in every voxel
+  for (int k = 0; k < NS; ++k) {
+    const int f = c->hp.fam[k];
+    if (f < 0) continue;
+    double t = 0.0;
+    for (int64_t v = 0; v < N; ++v) t += s[size_t(k) * size_t(N) + size_t(v)];
+    theta_bar[f] += t / double(N);
+  }
+  return 0;
+}
+
+int dmk_adj_local_jacobian(const dmk_phase* phase, double dt, const double* point, double* D) {
+  if (!phase || !point || !D) return fail(DMK_ERR_ARG, "null argument");
+  HostPhase hp;
+  std::string err;
+  if (build_host_phase(*phase, hp, err)) return fail(DMK_ERR_CONFIG, err);
+  const int np = padded_slip_count(hp.Ns);
+  if (!np) return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
+  pad_host_phase(hp, np);
+  switch (np) {
+    case 12: { auto pc = std::make_unique<PhaseConst<12>>(); fill_phase_const<12>(hp, hp.h.data(), *pc);
+               return host_local_jacobian<12>(*pc, hp.h.data(), dt, point, D) ? fail(DMK_ERR_STATE, "singular") : 0; }
+    case 18: { auto pc = std::make_unique<PhaseConst<18>>(); fill_phase_const<18>(hp, hp.h.data(), *pc);
+               return host_local_jacobian<18>(*pc, hp.h.data(), dt, point, D) ? fail(DMK_ERR_STATE, "singular") : 0; }
+    case 24: { auto pc = std::make_unique<PhaseConst<24>>(); fill_phase_const<24>(hp, hp.h.data(), *pc);
+               return host_local_jacobian<24>(*pc, hp.h.data(), dt, point, D) ? fail(DMK_ERR_STATE, "singular") : 0; }
+    case 48: { auto pc = std::make_unique<PhaseConst<48>>(); fill_phase_const<48>(hp, hp.h.data(), *pc);
+               return host_local_jacobian<48>(*pc, hp.h.data(), dt, point, D) ? fail(DMK_ERR_STATE, "singular") : 0; }
+  }
+  return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
 }
 
 }  // extern "C"

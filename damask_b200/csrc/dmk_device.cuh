@@ -14,6 +14,8 @@ namespace dmk {
 
 constexpr double TINY10 = 10.0 * 2.2250738585072014e-308;   // dEq0 threshold, prec.f90:131-143
 
+struct SysConst;
+
 // Per-phase constants, passed by value as a __grid_constant__ kernel parameter so
 // that every uniform access is served by the constant bank.
 template <int NS>
@@ -27,9 +29,15 @@ struct PhaseConst {
   double dn[NS][6];        // slip direction d and plane normal n (unit): P = d (x) n
   double dg0[NS], n[NS], a[NS], h0f[NS], xiinf[NS], ixiinf[NS];
   const double* hmat;      // slip-slip hardening matrix (NS x NS, row = reacting system) in device memory
+  const SysConst* sys;     // the per-system constants of the Newton loop (NS entries) in device memory
   int n_int[NS];           // stress exponent as integer if integral, else -1
   int a_int[NS];           // hardening exponent as integer if integral, else -1
   double atol_xi, atol_gamma;
+  // slip families (used by the adjoint's local model)
+  int fam[NS];             // family of system s, -1 for inert padding
+  double hfac[NS];         // h0f[s] = h_0 of the family * hfac[s]
+  int nf;                  // number of families
+  double th[4][4];         // per family: xi_inf, h_0, n, a (the parameters of the gradient)
 };
 
 struct Numerics {
@@ -185,26 +193,35 @@ struct SysConst {
   int pad[3];
 };
 
+// Host-side assembly of the per-system constants (the device copy is staged into shared memory
+// by stage_sys_const with coalesced 16-byte loads).
+template <int NS>
+__host__ __device__ inline SysConst make_sys_const(const PhaseConst<NS>& pc, int i) {
+  SysConst c;
+  for (int t = 0; t < 6; ++t) {
+    c.p6[t] = make_double2(pc.p6[0][i][t], pc.p6[1][i][t]);
+    c.q6[t] = make_double2(pc.q6[0][i][t], pc.q6[1][i][t]);
+  }
+  for (int k = 0; k < 4; ++k) c.P[k] = make_double2(pc.P[i][2 * k], pc.P[i][2 * k + 1]);
+  c.P[4] = make_double2(pc.P[i][8], 0.0);
+  c.dn[0] = make_double2(pc.dn[i][0], pc.dn[i][1]);
+  c.dn[1] = make_double2(pc.dn[i][2], pc.dn[i][3]);
+  c.dn[2] = make_double2(pc.dn[i][4], pc.dn[i][5]);
+  c.kin = make_double2(pc.dg0[i], pc.n[i]);
+  c.n_int = pc.n_int[i];
+  c.pad[0] = c.pad[1] = c.pad[2] = 0;
+  return c;
+}
+
+// Copies the NS per-system constants from device memory into shared memory: every thread of
+// the block moves 16-byte words of the contiguous array (no per-thread divergent reads of the
+// parameter space).
 template <int NS>
 __device__ __forceinline__ void stage_sys_const(const PhaseConst<NS>& pc, SysConst* sc) {
-  for (int i = threadIdx.x; i < NS; i += blockDim.x) {
-    SysConst c;
-#pragma unroll
-    for (int t = 0; t < 6; ++t) {
-      c.p6[t] = make_double2(pc.p6[0][i][t], pc.p6[1][i][t]);
-      c.q6[t] = make_double2(pc.q6[0][i][t], pc.q6[1][i][t]);
-    }
-#pragma unroll
-    for (int k = 0; k < 4; ++k) c.P[k] = make_double2(pc.P[i][2 * k], pc.P[i][2 * k + 1]);
-    c.P[4] = make_double2(pc.P[i][8], 0.0);
-    c.dn[0] = make_double2(pc.dn[i][0], pc.dn[i][1]);
-    c.dn[1] = make_double2(pc.dn[i][2], pc.dn[i][3]);
-    c.dn[2] = make_double2(pc.dn[i][4], pc.dn[i][5]);
-    c.kin = make_double2(pc.dg0[i], pc.n[i]);
-    c.n_int = pc.n_int[i];
-    c.pad[0] = c.pad[1] = c.pad[2] = 0;
-    sc[i] = c;
-  }
+  constexpr int WORDS = NS * int(sizeof(SysConst) / sizeof(double2));
+  const double2* __restrict__ src = reinterpret_cast<const double2*>(pc.sys);
+  double2* dst = reinterpret_cast<double2*>(sc);
+  for (int i = threadIdx.x; i < WORDS; i += blockDim.x) dst[i] = src[i];
 }
 
 // Hooke in Mandel notation with Fi = I: S = C66 : sym6(E), E = (Fe^T Fe - I)/2

