@@ -61,13 +61,15 @@ def gradient_numerics(num: Numerics | None = None) -> Numerics:
     derivatives to ~1e-5: divergence and stress-BC tolerances 1e-11 relative (absolute floors
     below them), Lp Newton 1e-11 relative with no absolute floor (the Newton residual's rounding
     floor lies near 1e-12), state iteration 1e-12 relative (more state iterations allowed),
-    Anderson history 16."""
+    Anderson history 30 and up to 300 fixed-point iterations (-snes_max_it 300, N_iter_max 300)."""
     n = copy.deepcopy(num) if num is not None else Numerics()
     n.eps_rel_div, n.eps_abs_div = 1.0e-11, 1.0e-12
     n.eps_rel_P, n.eps_abs_P = 1.0e-11, 1.0e-6
     n.eps_rel_Lp, n.eps_abs_Lp = 1.0e-11, 1.0e-30
     n.eps_rel_state, n.N_iter_state_max = 1.0e-12, 100
-    n.anderson_m = 16
+    n.anderson_m = 30
+    n.PETSc_options = (n.PETSc_options + ' -snes_max_it 300').strip()
+    n.N_iter_max = 300
     return n
 
 

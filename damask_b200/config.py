@@ -44,7 +44,7 @@ class NumericsStruct(C.Structure):
                 ('eps_abs_Li', C.c_double), ('f_update_jacobi_Li', C.c_int),
                 ('snes_type', C.c_int), ('anderson_m', C.c_int),
                 ('solver', C.c_int), ('alpha', C.c_double), ('beta', C.c_double),
-                ('eps_abs_curl', C.c_double), ('eps_rel_curl', C.c_double)]
+                ('eps_abs_curl', C.c_double), ('eps_rel_curl', C.c_double), ('snes_max_it', C.c_int)]
 
 
 class BCStruct(C.Structure):
@@ -253,6 +253,16 @@ class Numerics:
             return 1
         raise ValueError(f'unsupported -snes_type {kind}')
 
+    @property
+    def snes_max_it(self) -> int:
+        """PETSc's ``-snes_max_it`` from PETSc_options (PETSc's default 50)."""
+        toks = self.PETSc_options.split()
+        n = 50
+        for i, t in enumerate(toks[:-1]):
+            if t == '-snes_max_it':
+                n = int(toks[i + 1])
+        return n
+
     @classmethod
     def from_dict(cls, d: dict | None) -> 'Numerics':
         d = d or {}
@@ -343,6 +353,7 @@ class Numerics:
         s.eps_abs_Li = self.eps_abs_Lp if self.eps_abs_Li is None else self.eps_abs_Li
         s.f_update_jacobi_Li = int(self.f_update_jacobi_Lp if self.f_update_jacobi_Li is None else self.f_update_jacobi_Li)
         s.snes_type = self.snes_type
+        s.snes_max_it = self.snes_max_it
         s.anderson_m = int(self.anderson_m)
         s.solver = SOLVERS[self.solver]
         s.alpha, s.beta = float(self.alpha), float(self.beta)

@@ -744,7 +744,7 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
   if (c->num.update_gamma)
     if (int rc = set_polarization_scale(c)) return rc;
   const int64_t N = c->N, n18 = 18 * N;
-  const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
+  const int snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;   // PETSc -snes_max_it (default 50)
   const bool anderson = c->num.snes_type == 1;
   const int m = c->aa_m;
   const int nspec = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
@@ -1204,7 +1204,7 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
   CK(cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream));
   c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
   if (c->solver == 1) return solution_polarization(c, out);
-  const int snes_max_its = 50;          // PETSc SNES default maximum number of iterations
+  const int snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;   // PETSc -snes_max_it (default 50)
   const bool mixed = c->precision == DMK_PRECISION_MIXED;
   const bool anderson = c->num.snes_type == 1;
   const int m = c->aa_m;

@@ -96,6 +96,8 @@ typedef struct {
   int solver;
   double alpha, beta;          /* polarization parameters: 0 < alpha <= 2, 0 <= beta <= 2 */
   double eps_abs_curl, eps_rel_curl;   /* eps_abs_curl(F), eps_rel_curl(F) (polarization) */
+  int snes_max_it;             /* iteration cap of the fixed point: PETSc's -snes_max_it (default 50), which
+                                  the reference's PETSc_options can set; 0 means 50 */
 } dmk_numerics;
 
 /* tBCmech (grid_utilities.f90:35-39): values/mask column-major, mask 1 = 'x' */

@@ -1489,7 +1489,7 @@ int orc_mech_solution(orc_ctx* c, orc_solution* out) {
     update_gamma(c, c->C_minMaxAvg);
     if (pol) { c->C_scale = c->C_minMaxAvg; c->S_scale = inv_sym3333(c->C_minMaxAvg); }
   }
-  const int snes_max_its = 50;    // PETSc SNES default maximum number of iterations
+  const int snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;   // PETSc -snes_max_it (default 50)
   // iteration vector X: F (basic), or [F; F_tau] (polarization), with its residual r
   const long NX = pol ? 2 * c->N : c->N;
   std::vector<M3> X(NX), r(NX);

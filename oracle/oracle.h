@@ -59,6 +59,7 @@ typedef struct {
   int solver;                  /* 0 spectral_basic, 1 spectral_polarization */
   double alpha, beta;          /* polarization scheme parameters */
   double eps_abs_curl, eps_rel_curl;
+  int snes_max_it;           /* PETSc -snes_max_it (0: PETSc's default 50) */
 } orc_numerics;
 
 typedef struct {
