@@ -289,14 +289,63 @@ def mechanical_solver(name: str):
     return {'spectral_basic': SpectralBasic, 'spectral_polarization': SpectralPolarization}[name]
 
 
-def save_restart(path, data: dict, increment: int) -> None:
-    """Restart data and the increment they belong to, in one .npz container."""
-    np.savez(path, increment=increment, **data)
+def save_restart(path, data: dict, increment: int, phase_name: str = 'phase', homogenization_name: str = 'SX') -> None:
+    """The restart file <job>_restart.hdf5 in the reference's layout: the solver group of
+    grid_mech_spectral_basic.f90:378-416 (F, F_lastinc per voxel; P_aim, F_aim, F_aim_lastinc,
+    F_aimDot; C_volAvg, C_volAvgLastInc, C_minMaxAvg; the polarization scheme adds F_tau and
+    F_tau_lastinc, grid_mech_spectral_polarization.f90:412-415), the phase group of
+    mechanical_restartWrite (phase_mechanical.f90:1248-1261: omega_plastic, F, F_p, F_i, L_p, L_i)
+    and the homogenization group (homogenization.f90:492-517, no state for one constituent).
+    Fortran arrays (3,3,N) are HDF5 datasets of shape (N,3,3), as libhdf5 stores them.  The
+    increment is kept as the root attribute 'restart_increment' (the reference's driver takes it
+    from its command line)."""
+    from .dadf5 import H5Writer
+    N = np.asarray(data['F']).shape[0]
+
+    def t33n(a):
+        return np.ascontiguousarray(np.asarray(a, dtype=np.float64).reshape(N, 3, 3))
+
+    with H5Writer(path) as w:
+        w.dataset('solver/F', t33n(data['F']))
+        w.dataset('solver/F_lastinc', t33n(data['F_lastinc']))
+        for k in ('P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot'):
+            w.dataset(f'solver/{k}', np.asarray(data[k], dtype=np.float64).reshape(3, 3))
+        for k in ('C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg'):
+            w.dataset(f'solver/{k}', np.asarray(data[k], dtype=np.float64).reshape(3, 3, 3, 3))
+        for k in ('F_tau', 'F_tau_lastinc'):
+            if k in data:
+                w.dataset(f'solver/{k}', t33n(data[k]))
+        g = f'phase/{phase_name}'
+        w.dataset(f'{g}/omega_plastic', np.ascontiguousarray(data['omega_plastic'], dtype=np.float64))
+        w.dataset(f'{g}/F', t33n(data['F_phase']))
+        w.dataset(f'{g}/F_p', t33n(data['F_p']))
+        w.dataset(f'{g}/F_i', np.tile(np.eye(3), (N, 1, 1)))
+        w.dataset(f'{g}/L_p', t33n(data['L_p']))
+        w.dataset(f'{g}/L_i', np.zeros((N, 3, 3)))
+        w.group(f'homogenization/{homogenization_name}')
+        w.attrs('/', {'restart_increment': np.int64(increment)})
 
 
-def load_restart(path) -> tuple[dict, int]:
-    z = np.load(path)
-    return {k: z[k] for k in z.files if k != 'increment'}, int(z['increment'])
+def load_restart(path, phase_name: str = 'phase') -> tuple[dict, int]:
+    """The restart data of save_restart (or of the reference's restart file, whose increment is
+    then 0: the caller knows it) as the arrays of SpectralBasic.restart_read."""
+    from .h5read import DADF5
+    f = DADF5(path)
+    d = {'F': f.read('solver/F'), 'F_lastinc': f.read('solver/F_lastinc')}
+    N = d['F'].shape[0]
+    d = {k: v.reshape(N, 9) for k, v in d.items()}
+    for k in ('P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot', 'C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg'):
+        d[k] = f.read(f'solver/{k}').reshape(-1)
+    for k in ('F_tau', 'F_tau_lastinc'):
+        if k in f.keys('solver'):
+            d[k] = f.read(f'solver/{k}').reshape(N, 9)
+    g = f'phase/{phase_name}'
+    d['omega_plastic'] = f.read(f'{g}/omega_plastic')
+    d['F_phase'] = f.read(f'{g}/F').reshape(N, 9)
+    d['F_p'] = f.read(f'{g}/F_p').reshape(N, 9)
+    d['L_p'] = f.read(f'{g}/L_p').reshape(N, 9)
+    inc = f.attrs('').get('restart_increment', 0)
+    return d, int(np.asarray(inc).reshape(-1)[0]) if np.size(inc) else 0
 
 
 class NotConverged(RuntimeError):

@@ -1,4 +1,5 @@
-"""Minimal reader for the HDF5 result files (DADF5) that DAMASK writes, for tests only.
+"""Minimal reader for HDF5 files: the result (DADF5) and restart files that DAMASK writes, and the
+files of damask_b200.dadf5's writer (restart files of the Python host).
 
 It covers the subset that libhdf5's defaults produce for these files: superblock
 version 0, version-1 object headers (with continuation blocks), groups stored as

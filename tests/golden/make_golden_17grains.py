@@ -35,7 +35,7 @@ HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE))
 sys.path.insert(0, str(HERE.parents[1]))
 
-from dadf5 import DADF5                      # noqa: E402
+from damask_b200.h5read import DADF5         # noqa: E402
 from damask_b200 import vti                  # noqa: E402
 
 

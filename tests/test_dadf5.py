@@ -6,7 +6,7 @@ import numpy as np
 
 from damask_b200.dadf5 import H5Writer, ResultFile, slip_labels
 
-from golden.dadf5 import DADF5
+from damask_b200.h5read import DADF5
 
 
 def test_writer_roundtrip(tmp_path):

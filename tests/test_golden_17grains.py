@@ -19,7 +19,7 @@ import yaml
 from damask_b200 import config, dadf5, vti
 from damask_b200.grid import run_load_cases
 
-from golden.dadf5 import DADF5
+from damask_b200.h5read import DADF5
 
 GOLD = Path(__file__).resolve().parent / 'golden' / 'golden_17grains_bcc.npz'
 

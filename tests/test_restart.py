@@ -7,9 +7,8 @@ import pytest
 from damask_b200 import synthetic, workloads
 from damask_b200.grid import IncrementDriver, SpectralBasic, load_restart, save_restart
 
-pytestmark = pytest.mark.gpu
 
-
+@pytest.mark.gpu
 @pytest.mark.parametrize('solver', ['spectral_basic', 'spectral_polarization'])
 def test_restart_resumes_the_run(gpu, tmp_path, solver):
     rve = synthetic.voronoi_rve((8, 8, 8), workloads.SIZE_1MM, 6, 1)
@@ -21,12 +20,12 @@ def test_restart_resumes_the_run(gpu, tmp_path, solver):
     drv = IncrementDriver(a, lcs)
     for _ in range(4):
         drv.step()
-    save_restart(tmp_path / 'r.npz', a.restart_write(), drv.total)
+    save_restart(tmp_path / 'job_restart.hdf5', a.restart_write(), drv.total)
     ref = [r for _ in range(3) for r in drv.step()]
     xi_a, P_a = a.get_field('xi_sl'), a.get_field('P')
     a.close()
 
-    data, inc = load_restart(tmp_path / 'r.npz')
+    data, inc = load_restart(tmp_path / 'job_restart.hdf5')
     assert inc == 4
     b = SpectralBasic(*args)
     b.restart_read(data)
@@ -43,6 +42,7 @@ def test_restart_resumes_the_run(gpu, tmp_path, solver):
     b.close()
 
 
+@pytest.mark.gpu
 def test_restart_rejects_mismatched_data(gpu):
     rve = synthetic.voronoi_rve((4, 4, 4), workloads.SIZE_1MM, 2, 0)
     g = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, workloads.fcc_al(),
@@ -54,6 +54,7 @@ def test_restart_rejects_mismatched_data(gpu):
     g.close()
 
 
+@pytest.mark.gpu
 def test_restart_state_of_padded_phase(gpu):
     """A phase whose active slip systems run on a larger compiled count (cF N_sl [6] on 12) writes
     and reads omega_plastic with the active systems only (xi then gamma per voxel, sizeState = 2 Ns)."""
@@ -74,3 +75,34 @@ def test_restart_state_of_padded_phase(gpu):
     b.restart_read(d)
     assert np.array_equal(b.restart_write()['omega_plastic'], d['omega_plastic'])
     b.close()
+
+
+def test_restart_file_layout_and_round_trip(tmp_path):
+    """<job>_restart.hdf5 holds the reference's groups and datasets (solver, phase/<name>,
+    homogenization/<name>) with libhdf5's shapes for Fortran (3,3,N) arrays, and reads back
+    exactly (CPU only: synthetic restart data)."""
+    from damask_b200.h5read import DADF5
+    rng = np.random.default_rng(4)
+    N, ns = 30, 12
+    d = {k: rng.normal(size=(N, 9)) for k in ('F', 'F_lastinc', 'F_phase', 'F_p', 'L_p')}
+    d['omega_plastic'] = rng.normal(size=(N, 2 * ns))
+    for k in ('P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot'):
+        d[k] = rng.normal(size=9)
+    for k in ('C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg'):
+        d[k] = rng.normal(size=81)
+    p = tmp_path / 'job_restart.hdf5'
+    save_restart(p, d, 17, phase_name='Aluminum', homogenization_name='SX')
+    f = DADF5(p)
+    assert sorted(f.keys('')) == ['homogenization', 'phase', 'solver']
+    assert sorted(f.keys('solver')) == sorted(['F', 'F_lastinc', 'P_aim', 'F_aim', 'F_aim_lastinc', 'F_aimDot',
+                                               'C_volAvg', 'C_volAvgLastInc', 'C_minMaxAvg'])
+    assert sorted(f.keys('phase/Aluminum')) == sorted(['omega_plastic', 'F', 'F_p', 'F_i', 'L_p', 'L_i'])
+    assert f.keys('homogenization') == ['SX']
+    assert f.read('solver/F').shape == (N, 3, 3) and f.read('solver/C_volAvg').shape == (3, 3, 3, 3)
+    assert f.read('phase/Aluminum/omega_plastic').shape == (N, 2 * ns)
+    # Fortran order: F(i,j,e) is element [e, j, i]
+    assert f.read('solver/F')[3, 2, 1] == d['F'][3, 1 + 3 * 2]
+    back, inc = load_restart(p, phase_name='Aluminum')
+    assert inc == 17
+    for k, v in d.items():
+        assert np.array_equal(back[k], v), k
