@@ -27,28 +27,19 @@ __device__ __forceinline__ void finish_voxel(const Fields& f, int64_t v, const V
   if (c.status != 0) atomicMax(f.status, 2);               // STATUS_FAIL_PHASE_MECHANICAL
 }
 
-// warp-aggregated append of the continuing voxels (fast ones to the front of the list, slow ones
-// to its back) and of the iteration counters; every thread of the block reaches this point
-__device__ __forceinline__ void append_and_count(const Fields& f, const PassWork& w, bool keep, bool slow, int64_t v,
-                                                 int dstate, int dnewton) {
+// warp-aggregated append of the continuing voxels and of the iteration counters;
+// every thread of the block reaches this point
+__device__ __forceinline__ void append_and_count(const Fields& f, const PassWork& w, bool keep, int64_t v, int dstate,
+                                                 int dnewton) {
   const unsigned full = 0xffffffffu;
   const int lane = threadIdx.x & 31;
-  const unsigned lower = (1u << lane) - 1u;
-  const unsigned mf = __ballot_sync(full, keep && !slow);
-  const unsigned ms = __ballot_sync(full, keep && slow);
-  if (mf) {
-    const int leader = __ffs(mf) - 1;
+  const unsigned m = __ballot_sync(full, keep);
+  if (m) {
+    const int leader = __ffs(m) - 1;
     int base = 0;
-    if (lane == leader) base = atomicAdd(&w.count_out[0], __popc(mf));
+    if (lane == leader) base = atomicAdd(w.count_out, __popc(m));
     base = __shfl_sync(full, base, leader);
-    if (keep && !slow) w.list_out[base + __popc(mf & lower)] = int(v);
-  }
-  if (ms) {
-    const int leader = __ffs(ms) - 1;
-    int base = 0;
-    if (lane == leader) base = atomicAdd(&w.count_out[1], __popc(ms));
-    base = __shfl_sync(full, base, leader);
-    if (keep && slow) w.list_out[w.list_cap - 1 - (base + __popc(ms & lower))] = int(v);
+    if (keep) w.list_out[base + __popc(m & ((1u << lane) - 1u))] = int(v);
   }
   unsigned long long cs = dstate, cn = dnewton;
 #pragma unroll
@@ -77,7 +68,7 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
   __syncthreads();
   const int64_t v = v_begin + int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
-  bool keep = false, slow = false;
+  bool keep = false;
   if (v < v_end) {
     // F <- F - r (the Richardson/Anderson update of the previous evaluation), phase F
     double Fn[9];
@@ -160,10 +151,9 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
     }
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
-    slow = w.ctl[6 * N + v] > NEWTON_FAST;                 // as in the previous evaluation
     if (!keep) finish_voxel(f, v, c);
   }
-  append_and_count(f, w, keep, slow, v, 0, 0);
+  append_and_count(f, w, keep, v, 0, 0);
 }
 
 // one state iteration of every listed voxel: integrateStress (integrateStateFPI:626-629)
@@ -171,7 +161,7 @@ template <int NS>
 __global__ void __launch_bounds__(pass_threads<NS>())
 constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                            const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
-                           const int* __restrict__ list_in, int64_t n_in, int64_t n_fast) {
+                           const int* __restrict__ list_in, int64_t n_in) {
   extern __shared__ double2 smem2[];
   SysConst* sc = reinterpret_cast<SysConst*>(smem2);
   double* xs = reinterpret_cast<double*>(sc + NS) + threadIdx.x;
@@ -182,7 +172,7 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
   int dnewton = 0;
   const bool active = idx < n_in;
   if (active) {
-    const int64_t v = list_entry(list_in, idx, n_fast, w.list_cap);
+    const int64_t v = list_in[idx];
     const double step = w.sub[N + v];
     double Lp[9];
 #pragma unroll
@@ -211,7 +201,6 @@ constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gr
     w.ctl[2 * N + v] += 1;                                 // state iteration of this substep
     w.ctl[4 * N + v] += 1;                                 // state iterations, total
     w.ctl[5 * N + v] += dnewton;                           // Newton iterations, total
-    w.ctl[6 * N + v] = dnewton;                            // Newton iterations of this integrateStress
   }
   // iteration counters (warp aggregated)
   unsigned long long cs = active ? 1 : 0, cn = dnewton;
@@ -232,7 +221,7 @@ template <int NS>
 __global__ void __launch_bounds__(pass_threads<NS>(), 4)
 constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                             const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
-                            const int* __restrict__ list_in, int64_t n_in, int64_t n_fast) {
+                            const int* __restrict__ list_in, int64_t n_in) {
   extern __shared__ double slots[];
   double* hs = slots;
   double* xs = slots + NS * NS + threadIdx.x;
@@ -240,19 +229,18 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
   __syncthreads();
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const int64_t N = f.N;
-  bool keep = false, slow = false;
+  bool keep = false;
   int64_t v = 0;
   if (idx < n_in) {
-    v = list_entry(list_in, idx, n_fast, w.list_cap);
+    v = list_in[idx];
     VoxelCtl c;
     load_ctl(w, N, v, c);
     advance<NS>(pc, hs, nm, f, w, v, dt, c, xs, w.adg + v, N);
     store_ctl(w, N, v, c);
     keep = c.phase == PH_STRESS;
-    slow = w.ctl[6 * N + v] > NEWTON_FAST;
     if (!keep) finish_voxel(f, v, c);
   }
-  append_and_count(f, w, keep, slow, v, 0, 0);
+  append_and_count(f, w, keep, v, 0, 0);
 }
 
 template <int NS>
@@ -272,8 +260,7 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, int64_t n_fast,
-                                     cudaStream_t s) {
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
   const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * pass_threads<NS>() * sizeof(double);
   const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
@@ -282,8 +269,8 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
     e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_c));
   if (e != cudaSuccess) return e;
   const int nb = int((n_in + pass_threads<NS>() - 1) / pass_threads<NS>());
-  constitutive_stress_kernel<NS><<<nb, pass_threads<NS>(), smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in, n_fast);
-  constitutive_control_kernel<NS><<<nb, pass_threads<NS>(), smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in, n_fast);
+  constitutive_stress_kernel<NS><<<nb, pass_threads<NS>(), smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  constitutive_control_kernel<NS><<<nb, pass_threads<NS>(), smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in);
   return cudaGetLastError();
 }
 
@@ -292,8 +279,7 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
                                                      const PassWork&, double, int, int, int64_t, int64_t,          \
                                                      cudaStream_t);                                                 \
   template cudaError_t launch_constitutive_pass<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,           \
-                                                    const PassWork&, double, const int*, int64_t, int64_t,         \
-                                                    cudaStream_t);
+                                                    const PassWork&, double, const int*, int64_t, cudaStream_t);
 DMK_INSTANTIATE(12)
 DMK_INSTANTIATE(18)
 DMK_INSTANTIATE(24)

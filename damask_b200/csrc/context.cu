@@ -131,7 +131,7 @@ struct dmk_ctx {
   double *aa_dX = nullptr, *aa_dR = nullptr, *aa_Rprev = nullptr, *aa_partials = nullptr, *aa_out = nullptr;
   // constitutive pass scheme: per-voxel iteration state, voxel lists, pass counts
   double* pw = nullptr;          // Fs F0s Fp0s Lp0s (9 each), st0s dot last1 (2 NS each), stepFrac, step
-  int* pctl = nullptr;           // 7 planes of per-voxel control integers
+  int* pctl = nullptr;           // 6 planes of per-voxel control integers
   double* dot0 = nullptr;        // 2 NS planes: dotState at (S0, state0), see dot0_valid
   bool dot0_valid = false;       // dot0 holds the rates of the current increment-start values
   // The voxels are split into PASS_CHUNKS chunks whose pass loops run on their own streams,
@@ -141,9 +141,8 @@ struct dmk_ctx {
   cudaEvent_t fork = nullptr, join[PASS_CHUNKS] = {};
   int* plist[PASS_CHUNKS][2] = {};
   int nchunks = PASS_CHUNKS;     // chunks in use: fewer for small RVEs (one host sync per chunk and pass)
-  int64_t plist_len[PASS_CHUNKS] = {};   // capacity of plist[h][0] and plist[h][1]
-  int* pcount = nullptr;         // [4 h + 2 k + b]: entries appended to plist[h][k], front (b = 0) and back (b = 1)
-  int* hcount = nullptr;         // pinned host copies of the current counts of the chunks, [2 h + b]
+  int* pcount = nullptr;         // [2 h + k]: entries appended to plist[h][k]
+  int* hcount = nullptr;         // pinned host copies of the current counts of the chunks
   int64_t passes = 0;            // constitutive passes launched (all evaluations)
 
   // device checkpoints (dmk_checkpoint_save / _restore): per slot, the per-voxel state and the
@@ -200,8 +199,7 @@ PassWork pass_work(dmk_ctx* c, int half, int out) {
   w.sub = w.adg + int64_t(c->NS) * N;
   w.ctl = c->pctl;
   w.list_out = c->plist[half][out];
-  w.count_out = c->pcount + 4 * half + 2 * out;
-  w.list_cap = c->plist_len[half];
+  w.count_out = c->pcount + 2 * half + out;
   return w;
 }
 size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 7 * NS + 2); }
@@ -222,10 +220,10 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
   for (int h = 0; h < K; ++h) {
     // pass 0: restore and control up to the first integrateStress of every voxel of the chunk
     cur[h] = 0;
-    CK(cudaMemsetAsync(c->pcount + 4 * h, 0, 4 * sizeof(int), c->cstream[h]));
+    CK(cudaMemsetAsync(c->pcount + 2 * h, 0, 2 * sizeof(int), c->cstream[h]));
     CKL(launch_constitutive_begin<NS>(pc, c->nm, f, pass_work(c, h, 0), dt, apply, c->dot0_valid ? 1 : 0, lo[h], hi[h],
                                       c->cstream[h]));
-    CK(cudaMemcpyAsync(c->hcount + 2 * h, c->pcount + 4 * h, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
+    CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
     ++c->passes;
     active[h] = hi[h] > lo[h];
   }
@@ -236,19 +234,18 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
     for (int h = 0; h < K; ++h) {
       if (!active[h]) continue;
       CK(cudaStreamSynchronize(c->cstream[h]));
-      const int64_t n_fast = c->hcount[2 * h], n = n_fast + c->hcount[2 * h + 1];
+      const int64_t n = c->hcount[h];
       if (n == 0) { active[h] = false; continue; }
       any = true;
       // bounded by substeps x state iterations; a runaway count means corrupted control state
       if (++pass > 400000) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
       const int nxt = 1 - cur[h];
-      CK(cudaMemsetAsync(c->pcount + 4 * h + 2 * nxt, 0, 2 * sizeof(int), c->cstream[h]));
-      CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, h, nxt), dt, c->plist[h][cur[h]], n, n_fast,
+      CK(cudaMemsetAsync(c->pcount + 2 * h + nxt, 0, sizeof(int), c->cstream[h]));
+      CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, h, nxt), dt, c->plist[h][cur[h]], n,
                                        c->cstream[h]));
       ++c->launches;                                       // a pass is a stress and a control kernel
       ++c->passes;
-      CK(cudaMemcpyAsync(c->hcount + 2 * h, c->pcount + 4 * h + 2 * nxt, 2 * sizeof(int), cudaMemcpyDeviceToHost,
-                         c->cstream[h]));
+      CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h + nxt, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
       cur[h] = nxt;
     }
     if (!any) break;
@@ -1034,9 +1031,9 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
       (rc = dalloc(&c->div_partials, (size_t)gamma_div_blocks(cells[0], cells[1], cells[2]))) ||
       (rc = dalloc(&c->status, 1)) || (rc = dalloc(&c->iter, 4 * N)) || (rc = dalloc(&c->counters, 4)) ||
       (rc = dalloc(&c->sc, 1)) || (rc = dalloc(&c->tan_out, 245)) || (rc = dalloc(&c->tan_idx, 2)) ||
-      (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 7 * size_t(N))) ||
+      (rc = dalloc(&c->pw, pass_work_doubles(N, c->NS))) || (rc = dalloc(&c->pctl, 6 * size_t(N))) ||
       (rc = dalloc(&c->dot0, size_t(NST) * N)) ||
-      (rc = dalloc(&c->pcount, 4 * PASS_CHUNKS)) || (rc = dalloc(&c->xp, 3 * size_t(N))) ||
+      (rc = dalloc(&c->pcount, 2 * PASS_CHUNKS)) || (rc = dalloc(&c->xp, 3 * size_t(N))) ||
       (rc = dalloc(&c->xn, 3 * size_t(node_count(c)))) || (rc = dalloc(&c->favg, 9)))
     return bail(rc);
   // a chunk of at least 65536 voxels keeps a pass kernel wide enough to be worth its own stream
@@ -1044,12 +1041,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
   for (int h = 0; h < c->nchunks; ++h) {
     const size_t len = size_t(N * (h + 1) / c->nchunks - N * h / c->nchunks);
     if ((rc = dalloc(&c->plist[h][0], len)) || (rc = dalloc(&c->plist[h][1], len))) return bail(rc);
-    c->plist_len[h] = int64_t(len);
   }
-  // the Newton counts of the last stress integration start at zero (every voxel "fast")
-  if (cudaMemset(c->pctl, 0, sizeof(int) * 7 * size_t(N)) != cudaSuccess)
-    return bail(fail(DMK_ERR_CUDA, "cudaMemset of the control planes failed"));
-  if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), 2 * PASS_CHUNKS * sizeof(int)) != cudaSuccess) {
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), PASS_CHUNKS * sizeof(int)) != cudaSuccess) {
     c->hcount = nullptr;
     return bail(fail(DMK_ERR_CUDA, "cudaMallocHost failed"));
   }

@@ -87,21 +87,10 @@ struct PassWork {
   double* adg;     // NS: |dot_gamma| at the stress of the last converged integrateStress
   double* dot0;    // 2 NS: dotState at the increment-start stress and state (S0, state0)
   double* sub;     // 2: stepFrac (subFrac), step (subStep)
-  int* ctl;        // 7: phase, status, state iteration, substeps, state iterations total, Newton total,
-                   //    Newton iterations of the last integrateStress
-  int* list_out;   // voxels that continue into the next pass: fast ones from the front, slow ones from the back
-  int* count_out;  // [2]: entries appended to the front (fast) and to the back (slow) of list_out
-  int64_t list_cap;   // capacity of list_out (and of the list the pass reads)
+  int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
+  int* list_out;   // voxels that continue into the next pass
+  int* count_out;  // number of entries appended to list_out
 };
-
-// A voxel whose last integrateStress needed more Newton iterations than this goes to the slow end
-// of the next voxel list, so that the warps of a pass hold voxels of similar Newton counts.
-constexpr int NEWTON_FAST = 2;
-
-// entry idx of a voxel list holding n_fast entries at its front and the rest at its back
-__device__ __forceinline__ int64_t list_entry(const int* __restrict__ list, int64_t idx, int64_t n_fast, int64_t cap) {
-  return idx < n_fast ? list[idx] : list[cap - 1 - (idx - n_fast)];
-}
 
 enum : int { PH_CTRL = 0, PH_DOT0 = 1, PH_STRESS = 2, PH_DOT1 = 3, PH_DONE = 4 };
 

@@ -83,8 +83,7 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
                                       int64_t v_end, cudaStream_t s);
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, int64_t n_fast,
-                                     cudaStream_t s);
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
 cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s);
 cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s);
 cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int nparts, double wgt, const int* status,
