@@ -289,13 +289,63 @@ def _json_default(o):
     raise TypeError(type(o))
 
 
+BATCH_JOBS = 512                         # RVEs of the batched workload definition
+BATCH_RVES, BATCH_INCREMENTS = 128, 10   # the bounded batched sample of the default bench line
+
+
+def batch_sample(n_rves: int, increments: int, local: int = 0) -> dict:
+    """The batched workload's first n_rves RVEs (edges 8..32, 5..100 grains, random-axis tension or
+    simple shear), their first `increments` increments, as one batch of the library (FP64): updates/s
+    over the wall time of the run (the host's increment loops included, context set-up not) and over
+    the device time of the batched solutions."""
+    from damask_b200 import workloads
+    from damask_b200.batch import DeviceBatch
+    jobs = workloads.batched_jobs(BATCH_JOBS)[:n_rves]
+    voxels = sum(j[0].n_cells for j in jobs)
+    t0 = time.perf_counter()
+    db = DeviceBatch(jobs, max_increments=increments, device=local)
+    setup = time.perf_counter() - t0
+    clocks = ClockSampler(local)
+    clocks.start()
+    seconds = db.run()
+    clk = clocks.stop()
+    st = db.stats()
+    updates = sum(db.updates)
+    incs = sum(len(r) for r in db.results)
+    out = {'workload': f'first {n_rves} RVEs of batched{BATCH_JOBS} (edges {{8,12,16,24,32}}, 5..100 grains, '
+                       'random-axis tension or simple shear 1e-3/s), '
+                       + (f'increments 1..{increments} of each' if increments < 40 else 'all 40 increments'),
+           'value': updates / seconds, 'unit': 'updates/s', 'device_value': updates / (db.device_ms * 1e-3),
+           'seconds': seconds, 'device_seconds': db.device_ms * 1e-3, 'setup_seconds': setup,
+           'rves': n_rves, 'voxels': voxels, 'increments': incs, 'updates': updates,
+           'batched_solutions': db.batch_calls, 'graphs': st['graphs'], 'passes': st['passes'],
+           'fixed_point_iterations': st['iterations'], 'dtype': 'f64', 'clocks': clk,
+           'how': 'one dmk_batch_solution per round of solution requests: per fixed-point iteration one CUDA '
+                  'graph (constitutive passes of all active RVEs, device-side while loop), one cuFFT plan pair '
+                  'per edge size, batched aim / Gamma / convergence / Anderson kernels'}
+    db.close()
+    return out
+
+
 def run_batch(args) -> None:
     """Batched workload: independent RVEs (edges 8..32, 5..100 grains, random-axis tension or
-    simple shear, 40 increments to 4 %), all increments of every RVE, mixed precision; one
-    context per RVE on its own streams, host threads issue the RVEs concurrently."""
+    simple shear, 40 increments to 4 %), all increments of every RVE.  Default: one batch of the
+    library (FP64, shared launches); --batch-engine threads: one context per RVE on its own streams,
+    host threads issue the RVEs concurrently (mixed precision)."""
     import torch
     from damask_b200 import workloads
     from damask_b200.batch import BatchRunner
+    if args.batch_engine == 'device':
+        torch.cuda.synchronize()
+        b = batch_sample(args.batch, 40)
+        line = {'metric': 'batched RVE material-point updates/s (wall clock of the increment loops)',
+                'value': b['value'], 'unit': 'updates/s', 'n_gpus': 1, 'steps': b['increments'], 'warmup': 0,
+                'ms_per_step': 1e3 * b['seconds'] / max(1, b['increments']), 'higher_is_better': True,
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'config': {'workload': b['workload'], 'rves': args.batch, 'voxels': b['voxels'], 'engine': 'dmk_batch'},
+                'batched': b, 'clocks': b['clocks']}
+        print(json.dumps(line, default=_json_default), flush=True)
+        return
     jobs = workloads.batched_jobs(args.batch)
     voxels = sum(j[0].n_cells for j in jobs)
     torch.cuda.synchronize()
@@ -388,6 +438,9 @@ def main():
                     help='measure the batched workload instead: this many independent RVEs (512 in the '
                          'workload definition), one JSON line of its own')
     ap.add_argument('--batch-threads', type=int, default=48)
+    ap.add_argument('--batch-engine', choices=['device', 'threads'], default='device',
+                    help='--batch: one batch of the library (shared launches) or host threads over contexts')
+    ap.add_argument('--no-batched', action='store_true', help='leave out the batched key of the bench line')
     ap.add_argument('--derivative', choices=['continuous', 'central_difference', 'FWBW_difference'],
                     default='continuous', help='solver.grid.FFT.derivative (testing and profiling only)')
     ap.add_argument('--workload', choices=['grid256_bcc24_2000g', 'grid256_bcc48_2000g'], default=WORKLOAD,
@@ -430,6 +483,9 @@ def main():
         dist.destroy_process_group()
     if rank != 0:
         return
+    batched = None
+    if world == 1 and cells is None and not args.no_batched:
+        batched = batch_sample(BATCH_RVES, BATCH_INCREMENTS, local)
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         s = cpu_sample(steps=CPU_STEPS, warmup=warmup, workload=args.workload)
@@ -467,6 +523,8 @@ def main():
                          'increments_timed': f'{BCC48_WARMUP + 1}..{BCC48_WARMUP + BCC48_STEPS}',
                          's_per_increment': b48['s_per_increment'], 'roofline_fp64': b48['roofline']['fp64'],
                          'clocks': b48['mixed']['clocks']}
+    if batched is not None:
+        line['batched'] = batched
     print(json.dumps(line, default=_json_default), flush=True)
 
 

@@ -23,7 +23,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_get_coords', 'dmk_curl_rms', 'dmk_phase_slip_systems', 'dmk_vti_open', 'dmk_vti_geometry',
            'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
            'dmk_grid_run_ctx', 'dmk_fp64_peak', 'dmk_checkpoint_save', 'dmk_checkpoint_restore', 'dmk_adj_begin',
-           'dmk_adj_record', 'dmk_adj_step', 'dmk_adj_finish', 'dmk_adj_local_jacobian']
+           'dmk_adj_record', 'dmk_adj_step', 'dmk_adj_finish', 'dmk_adj_local_jacobian', 'dmk_batch_create',
+           'dmk_batch_solution', 'dmk_batch_stats', 'dmk_batch_destroy']
 
 _lib = None
 
@@ -96,6 +97,10 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_adj_step': (C.c_int, [vp, C.c_int, dp, dp, ip]),
         'dmk_adj_finish': (C.c_int, [vp, dp]),
         'dmk_adj_local_jacobian': (C.c_int, [C.POINTER(PhaseStruct), C.c_double, dp, dp]),
+        'dmk_batch_create': (C.c_int, [C.POINTER(vp), C.POINTER(vp), C.c_int]),
+        'dmk_batch_solution': (C.c_int, [vp, ip, C.c_int, C.POINTER(SolutionStruct)]),
+        'dmk_batch_stats': (C.c_int, [vp, dp]),
+        'dmk_batch_destroy': (None, [vp]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

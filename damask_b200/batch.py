@@ -1,10 +1,16 @@
 """Many independent RVEs on one GPU.
 
-Each RVE is its own solver context (its fields, cuFFT plans and CUDA streams); a pool of host
-threads drives the RVEs' increment loops.  The library calls release the interpreter lock, so
-the RVEs' kernel sequences are issued concurrently on their own streams and overlap on the
-device, which keeps the GPU busy although a single small RVE (8^3 ... 32^3 cells) is bound by
-launch latency.  RVEs never exchange data; every RVE's results are those of a standalone run.
+DeviceBatch: every RVE is a solver context and all of them form one batch of the library
+(dmk_batch_*).  Each RVE's increment loop runs on the host up to the point where it needs a
+solution; the solutions of all waiting RVEs are computed together, with the fixed-point iterations
+of every RVE in shared launches (per iteration one CUDA graph for the constitutive evaluation of
+all active RVEs, one cuFFT plan pair per edge size, batched residual and Anderson kernels).  The
+RVEs never exchange data; every RVE's results are those of a standalone run.  It takes the basic
+scheme in the FP64 form with one phase for all RVEs.
+
+BatchRunner: one context per RVE on its own streams, driven by a pool of host threads (any
+scheme and precision; the library calls release the interpreter lock, so the RVEs' kernel
+sequences overlap on the device).
 """
 from __future__ import annotations
 
@@ -12,7 +18,13 @@ import threading
 import time
 from concurrent.futures import ThreadPoolExecutor
 
-from .grid import SpectralBasic, run_load_cases, run_load_cases_native
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .config import SolutionStruct
+from .grid import IncrementDriver, SpectralBasic, run_load_cases, run_load_cases_native
 
 
 class BatchRunner:
@@ -58,3 +70,96 @@ class BatchRunner:
             for f in [ex.submit(self._run_one, k, on_finish) for k in range(len(self.jobs))]:
                 f.result()
         return time.perf_counter() - t0
+
+
+class DeviceBatch:
+    """Run the jobs ``(rve, phase, loadcases, numerics)`` as one batch of the library.
+
+    All contexts are created up front (they hold device memory until :meth:`close`).  ``run``
+    advances every job's increment loop (``IncrementDriver.step_requests``) to its next solution
+    request, solves all requests with one ``dmk_batch_solution`` call, hands each job its solution
+    and repeats until every job has run its increments (all, or ``max_increments``).  Jobs may
+    cut back and so fall out of step with the others; each request is solved at its own job's
+    increment and time step."""
+
+    def __init__(self, jobs, max_increments: int | None = None, N_cutback_max: int = 3, device: int = 0):
+        self.jobs = list(jobs)
+        self.max_increments = max_increments
+        self.lib = _lib.load()
+        self.solvers = [SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num,
+                                      precision='fp64', device=device) for rve, phase, _, num in self.jobs]
+        self.drivers = [IncrementDriver(s, lcs, N_cutback_max) for s, (_, _, lcs, _) in zip(self.solvers, self.jobs)]
+        self.results = [[] for _ in self.jobs]
+        self.updates = [0] * len(self.jobs)
+        self.batch_calls = 0
+        self.device_ms = 0.0              # device time of the batched solutions (dmk_batch_stats)
+        ctxs = (C.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
+        h = C.c_void_p()
+        _lib.check(self.lib.dmk_batch_create(C.byref(h), ctxs, len(self.solvers)))
+        self.handle = h
+        self._gens = [None] * len(self.jobs)
+
+    def _advance(self, k: int, sol) -> bool:
+        """Drive job k until it requests a solution (True) or has run its increments (False)."""
+        while True:
+            g = self._gens[k]
+            try:
+                if g is None:
+                    d = self.drivers[k]
+                    if d.done or (self.max_increments is not None and d.total >= self.max_increments):
+                        return False
+                    g = self._gens[k] = d.step_requests()
+                    g.send(None)
+                else:
+                    g.send(sol)
+                return True
+            except StopIteration as stop:
+                self.results[k].extend(stop.value or [])
+                self._gens[k] = None
+                sol = None
+
+    def solve(self, waiting: list[int]):
+        """One dmk_batch_solution call for the jobs in ``waiting``; their solution states."""
+        which = (C.c_int * len(waiting))(*waiting)
+        outs = (SolutionStruct * len(waiting))()
+        _lib.check(self.lib.dmk_batch_solution(self.handle, which, len(waiting), outs))
+        self.device_ms += self.stats()['solution_ms_last']
+        for k in waiting:
+            s = self.solvers[k]
+            c = s.counters()
+            s.total_counters += c
+            self.updates[k] += int(c[0])
+        return [outs[j] for j in range(len(waiting))]
+
+    def run(self, solve=None) -> float:
+        """Run every job; returns the wall time in seconds.  ``solve(waiting)`` replaces the
+        library call (it returns one solution state per listed job)."""
+        solve = solve or self.solve
+        t0 = time.perf_counter()
+        waiting = [k for k in range(len(self.jobs)) if self._advance(k, None)]
+        while waiting:
+            outs = solve(waiting)
+            self.batch_calls += 1
+            waiting = [k for k, sol in zip(waiting, outs) if self._advance(k, sol)]
+        return time.perf_counter() - t0
+
+    def stats(self) -> dict:
+        """Device ms of the constitutive graphs and of the whole last batched solution, graphs
+        launched, constitutive passes and fixed-point iterations so far."""
+        out = np.zeros(5)
+        _lib.check(self.lib.dmk_batch_stats(self.handle, out.ctypes.data_as(C.POINTER(C.c_double))))
+        return {'const_ms_last': out[0], 'solution_ms_last': out[1], 'graphs': int(out[2]), 'passes': int(out[3]),
+                'iterations': int(out[4])}
+
+    def close(self) -> None:
+        if getattr(self, 'handle', None):
+            self.lib.dmk_batch_destroy(self.handle)
+            self.handle = None
+        for s in getattr(self, 'solvers', []):
+            s.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

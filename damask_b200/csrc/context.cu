@@ -906,6 +906,53 @@ int solution_polarization(dmk_ctx* c, dmk_solution_state* out) {
   return 0;
 }
 
+// grid_mechanical_spectral_basic_solution before SNESsolve (grid_mech_spectral_basic.f90:259-262):
+// masked compliance, reference stiffness of Gamma, device scalars, counters
+int solution_prepare(dmk_ctx* c) {
+  int rc = masked_compliance(c->q_rot, c->stress_mask, c->C_volAvg, c->Scomp);
+  if (rc) return rc;
+  if (c->num.update_gamma) update_gamma_host(c, c->C_minMaxAvg);
+  if ((rc = upload_scalars(c, true))) return rc;
+  CK(cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream));
+  c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
+  return 0;
+}
+
+// grid_mechanical_spectral_basic_solution after SNESsolve (grid_mech_spectral_basic.f90:266-277):
+// the solution state, P_aim of the stress-controlled components, and the tangent of the converged
+// state (C_volAvg, C_minMaxAvg for the next increment); counters of the solve
+int solution_finish(dmk_ctx* c, const double F_aim[9], const double P_av[9], int totalIter, double err_div,
+                    double err_BC, int reason, int evals, dmk_solution_state* out) {
+  std::memcpy(c->F_aim, F_aim, sizeof c->F_aim);
+  std::memcpy(c->P_av, P_av, sizeof c->P_av);
+  out->converged = reason > 0;
+  out->iterationsNeeded = totalIter;
+  out->stagConverged = 1;
+  out->residualEvals = evals;
+  out->err_div = err_div;
+  out->err_BC = err_BC;
+  std::memcpy(out->P_av, P_av, sizeof out->P_av);
+  for (int k = 0; k < 9; ++k)
+    if (c->stress_mask[k]) c->P_aim[k] = c->P_av[k];
+  if (out->converged) {
+    CK(cudaEventRecord(c->ev[0], c->stream));
+    if (int rc = evaluate_tangent(c, c->dt, nullptr)) return rc;
+    CK(cudaEventRecord(c->ev[1], c->stream));
+    CK(cudaEventSynchronize(c->ev[1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+    c->last_ms[2] += ms;
+  }
+  unsigned long long hc[4];
+  CK(cudaMemcpyAsync(hc, c->counters, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaStreamSynchronize(c->stream));
+  c->last_counters[0] = int64_t(evals) * c->N;
+  c->last_counters[1] = int64_t(hc[1]);
+  c->last_counters[2] = int64_t(hc[2]);
+  c->last_counters[3] = evals;
+  return 0;
+}
+
 }  // namespace
 
 namespace dmk {
@@ -1061,7 +1108,8 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     return bail(rc);
   if (num->snes_type == 1) {
     c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
-    c->aa_blocks = c->nsm * 8;
+    // grid-stride blocks of the Anderson kernels: 8 per SM, fewer when the field is smaller
+    c->aa_blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(c->nsm) * 8, (nvec + 255) / 256)));
     if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * nvec)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * nvec)) ||
         (rc = dalloc(&c->aa_Rprev, nvec)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
         (rc = dalloc(&c->aa_out, 4 * AA_MAX)))
@@ -1197,12 +1245,8 @@ int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_ol
 
 int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
   if (!c || !out) return fail(DMK_ERR_ARG, "null argument");
-  int rc = masked_compliance(c->q_rot, c->stress_mask, c->C_volAvg, c->Scomp);
+  int rc = solution_prepare(c);
   if (rc) return rc;
-  if (c->num.update_gamma) update_gamma_host(c, c->C_minMaxAvg);
-  if ((rc = upload_scalars(c, true))) return rc;
-  CK(cudaMemsetAsync(c->counters, 0, 4 * sizeof(unsigned long long), c->stream));
-  c->last_ms[0] = c->last_ms[1] = c->last_ms[2] = 0.0;
   if (c->solver == 1) return solution_polarization(c, out);
   const int snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;   // PETSc -snes_max_it (default 50)
   const bool mixed = c->precision == DMK_PRECISION_MIXED;
@@ -1289,34 +1333,7 @@ int dmk_mech_solution(dmk_ctx* c, dmk_solution_state* out) {
     }
     reason = hs.reason;
   }
-  std::memcpy(c->F_aim, hs.F_aim, sizeof c->F_aim);
-  std::memcpy(c->P_av, hs.P_av, sizeof c->P_av);
-  out->converged = reason > 0;
-  out->iterationsNeeded = hs.totalIter;
-  out->stagConverged = 1;
-  out->residualEvals = evals;
-  out->err_div = hs.err_div;
-  out->err_BC = hs.err_BC;
-  std::memcpy(out->P_av, hs.P_av, sizeof out->P_av);
-  for (int k = 0; k < 9; ++k)
-    if (c->stress_mask[k]) c->P_aim[k] = c->P_av[k];
-  if (out->converged) {
-    CK(cudaEventRecord(c->ev[0], c->stream));
-    if ((rc = evaluate_tangent(c, c->dt, nullptr))) return rc;
-    CK(cudaEventRecord(c->ev[1], c->stream));
-    CK(cudaEventSynchronize(c->ev[1]));
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
-    c->last_ms[2] += ms;
-  }
-  unsigned long long hc[4];
-  CK(cudaMemcpyAsync(hc, c->counters, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  c->last_counters[0] = int64_t(evals) * c->N;
-  c->last_counters[1] = int64_t(hc[1]);
-  c->last_counters[2] = int64_t(hc[2]);
-  c->last_counters[3] = evals;
-  return 0;
+  return solution_finish(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, reason, evals, out);
 }
 
 int dmk_materialpoint_forward(dmk_ctx* c) {
@@ -2145,5 +2162,511 @@ int dmk_adj_local_jacobian(const dmk_phase* phase, double dt, const double* poin
   }
   return fail(DMK_ERR_CONFIG, "unsupported number of slip systems");
 }
+
+}  // extern "C"
+
+// ------------------------------------------------------------------ batches of contexts
+// The basic scheme's fixed point of many contexts (RVEs of one phase) in shared launches: per
+// iteration one CUDA graph runs the constitutive evaluation of every active context (its pass loop
+// is a device-side while node, so the host reads no voxel counts), then batched kernels and one
+// cuFFT plan per edge size form the residuals; the host reads the solver scalars of all contexts
+// once per iteration and makes the Anderson / Richardson decisions.
+
+struct dmk_batch {
+  int n = 0, NS = 0, device = 0, nsm = 148;
+  std::vector<dmk_ctx*> ctx;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int64_t n_items = 0;
+  // per-context tables of the constitutive kernels: one device block, one pinned host mirror
+  char* d_tab = nullptr;
+  char* h_tab = nullptr;
+  size_t tab_bytes = 0, o_f = 0, o_w = 0, o_dt = 0, o_dot0 = 0, o_apply = 0, o_active = 0;
+  int64_t* d_off = nullptr;
+  int* d_ctx_of = nullptr;
+  int* d_list[2] = {nullptr, nullptr};
+  int* d_count = nullptr;
+  int* d_status = nullptr;
+  int* d_iter = nullptr;
+  int* h_iter = nullptr;
+  // tables of the batched solver kernels
+  BatchCtx* d_bc = nullptr;
+  BatchCtx* h_bc = nullptr;
+  BatchAA* d_aa = nullptr;
+  BatchAA* h_aa = nullptr;
+  BatchScal* d_scal = nullptr;
+  BatchScal* h_scal = nullptr;
+  double* d_red = nullptr;       // partial sums of every context (sum9, divergence, Anderson)
+  double* d_dots = nullptr;      // Anderson inner products, 4 chunks of 2 AA_CHUNK per context
+  double* h_dots = nullptr;
+  struct Group {
+    int cells[3];
+    std::vector<int> members;
+    double* real = nullptr;
+    double* spec = nullptr;
+    cufftHandle fwd = 0, bwd = 0;
+  };
+  std::vector<Group> groups;
+  void* fft_work = nullptr;
+  int max_nconst = 0, max_nspec = 0, max_aa_blocks = 0;
+  int64_t max_n9 = 0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  double last_ms[2] = {0.0, 0.0};     // constitutive graphs, whole solution (device time)
+  int64_t graph_launches = 0, passes = 0, iterations = 0;
+};
+
+namespace {
+
+constexpr int BATCH_DOTS = 4 * 2 * AA_CHUNK;   // Anderson inner products per context (AA_MAX slots)
+
+void batch_free(dmk_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto& g : b->groups) {
+    if (g.fwd) cufftDestroy(g.fwd);
+    if (g.bwd) cufftDestroy(g.bwd);
+    if (g.real) cudaFree(g.real);
+    if (g.spec) cudaFree(g.spec);
+  }
+  for (void* p : {(void*)b->d_tab, (void*)b->d_off, (void*)b->d_ctx_of, (void*)b->d_list[0], (void*)b->d_list[1],
+                  (void*)b->d_count, (void*)b->d_status, (void*)b->d_iter, (void*)b->d_bc, (void*)b->d_aa,
+                  (void*)b->d_scal, (void*)b->d_red, (void*)b->d_dots, b->fft_work})
+    if (p) cudaFree(p);
+  for (void* p : {(void*)b->h_tab, (void*)b->h_iter, (void*)b->h_bc, (void*)b->h_aa, (void*)b->h_scal, (void*)b->h_dots})
+    if (p) cudaFreeHost(p);
+  for (auto e : b->ev)
+    if (e) cudaEventDestroy(e);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+template <int NS>
+const PhaseConst<NS>* phase_const_of(const dmk_ctx* c);
+template <> const PhaseConst<12>* phase_const_of<12>(const dmk_ctx* c) { return c->pc12; }
+template <> const PhaseConst<18>* phase_const_of<18>(const dmk_ctx* c) { return c->pc18; }
+template <> const PhaseConst<24>* phase_const_of<24>(const dmk_ctx* c) { return c->pc24; }
+template <> const PhaseConst<48>* phase_const_of<48>(const dmk_ctx* c) { return c->pc48; }
+
+// the phase constants of two contexts agree (their device pointers aside)
+template <int NS>
+bool same_phase_const(const dmk_ctx* a, const dmk_ctx* b) {
+  auto x = std::make_unique<PhaseConst<NS>>(*phase_const_of<NS>(a));
+  auto y = std::make_unique<PhaseConst<NS>>(*phase_const_of<NS>(b));
+  x->hmat = y->hmat = nullptr;
+  x->sys = y->sys = nullptr;
+  return std::memcmp(x.get(), y.get(), sizeof(PhaseConst<NS>)) == 0;
+}
+bool same_phase(const dmk_ctx* a, const dmk_ctx* b) {
+  if (a->NS != b->NS || a->hp.h != b->hp.h || std::memcmp(&a->nm, &b->nm, sizeof a->nm) != 0) return false;
+  switch (a->NS) {
+    case 12: return same_phase_const<12>(a, b);
+    case 18: return same_phase_const<18>(a, b);
+    case 24: return same_phase_const<24>(a, b);
+    case 48: return same_phase_const<48>(a, b);
+  }
+  return false;
+}
+
+template <int NS>
+cudaError_t batch_graph(dmk_batch* b, const BatchTables& t, const BatchPassBuffers& pb) {
+  const dmk_ctx* c0 = b->ctx[0];
+  return build_batch_pass_graph<NS>(*phase_const_of<NS>(c0), c0->nm, t, pb, b->nsm, b->stream, &b->graph);
+}
+
+int batch_build(dmk_batch* b) {
+  const int n = b->n;
+  CK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  for (auto& e : b->ev) CK(cudaEventCreate(&e));
+  // items: the voxels of all contexts, context after context
+  std::vector<int64_t> off(n + 1, 0);
+  for (int r = 0; r < n; ++r) off[r + 1] = off[r] + b->ctx[r]->N;
+  b->n_items = off[n];
+  if (b->n_items > INT32_MAX) return fail(DMK_ERR_ARG, "a batch holds at most 2^31 - 1 voxels");
+  std::vector<int> ctx_of(b->n_items);
+  for (int r = 0; r < n; ++r)
+    for (int64_t v = off[r]; v < off[r + 1]; ++v) ctx_of[v] = r;
+  int rc;
+  if ((rc = dalloc(&b->d_off, n + 1)) || (rc = dalloc(&b->d_ctx_of, b->n_items)) ||
+      (rc = dalloc(&b->d_list[0], b->n_items)) || (rc = dalloc(&b->d_list[1], b->n_items)) ||
+      (rc = dalloc(&b->d_count, 2)) || (rc = dalloc(&b->d_status, n)) || (rc = dalloc(&b->d_iter, 2)) ||
+      (rc = dalloc(&b->d_bc, n)) || (rc = dalloc(&b->d_aa, n)) || (rc = dalloc(&b->d_scal, n)) ||
+      (rc = dalloc(&b->d_dots, size_t(n) * BATCH_DOTS)))
+    return rc;
+  CK(cudaMemcpy(b->d_off, off.data(), sizeof(int64_t) * (n + 1), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(b->d_ctx_of, ctx_of.data(), sizeof(int) * b->n_items, cudaMemcpyHostToDevice));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_iter), 2 * sizeof(int)));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_bc), sizeof(BatchCtx) * n));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_aa), sizeof(BatchAA) * n));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_scal), sizeof(BatchScal) * n));
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_dots), sizeof(double) * n * BATCH_DOTS));
+  std::memset(b->h_bc, 0, sizeof(BatchCtx) * n);
+  std::memset(b->h_aa, 0, sizeof(BatchAA) * n);
+  // the tables of the constitutive kernels, 256-byte aligned sections of one block
+  auto sec = [&](size_t bytes) {
+    const size_t o = b->tab_bytes;
+    b->tab_bytes += (bytes + 255) / 256 * 256;
+    return o;
+  };
+  b->o_f = sec(sizeof(Fields) * n);
+  b->o_w = sec(sizeof(PassWork) * n);
+  b->o_dt = sec(sizeof(double) * n);
+  b->o_dot0 = sec(sizeof(int) * n);
+  b->o_apply = sec(sizeof(int) * n);
+  b->o_active = sec(n);
+  if ((rc = dalloc(&b->d_tab, b->tab_bytes))) return rc;
+  CK(cudaMallocHost(reinterpret_cast<void**>(&b->h_tab), b->tab_bytes));
+  std::memset(b->h_tab, 0, b->tab_bytes);
+  // per-context partial sums, and the static part of the solver kernels' table
+  size_t red = 0;
+  std::vector<size_t> o_part(n), o_div(n), o_aap(n);
+  for (int r = 0; r < n; ++r) {
+    dmk_ctx* c = b->ctx[r];
+    BatchCtx& x = b->h_bc[r];
+    x.N = c->N;
+    x.wgt = c->wgt;
+    for (int d = 0; d < 3; ++d) {
+      x.L[d] = c->geom[d];
+      x.n[d] = c->cells[d];
+    }
+    x.nconst = nblocks_const(c);
+    x.nspec = gamma_div_blocks(c->cells[0], c->cells[1], c->cells[2]);
+    x.aa_blocks = c->aa_blocks > 0 ? c->aa_blocks : 1;
+    b->max_nconst = std::max(b->max_nconst, x.nconst);
+    b->max_nspec = std::max(b->max_nspec, x.nspec);
+    b->max_aa_blocks = std::max(b->max_aa_blocks, x.aa_blocks);
+    b->max_n9 = std::max(b->max_n9, 9 * c->N);
+    o_part[r] = red;
+    red += size_t(9) * x.nconst;
+    o_div[r] = red;
+    red += size_t(x.nspec);
+    o_aap[r] = red;
+    red += size_t(x.aa_blocks) * 2 * AA_CHUNK;
+  }
+  if ((rc = dalloc(&b->d_red, red))) return rc;
+  for (int r = 0; r < n; ++r) {
+    BatchCtx& x = b->h_bc[r];
+    x.partials = b->d_red + o_part[r];
+    x.divp = b->d_red + o_div[r];
+    x.aa_partials = b->d_red + o_aap[r];
+    x.aa_out = b->d_dots + size_t(r) * BATCH_DOTS;
+    x.status = b->d_status + r;
+  }
+  // one cuFFT plan pair per edge size over the 9 components of all its contexts
+  for (int r = 0; r < n; ++r) {
+    const dmk_ctx* c = b->ctx[r];
+    auto it = std::find_if(b->groups.begin(), b->groups.end(), [&](const dmk_batch::Group& g) {
+      return g.cells[0] == c->cells[0] && g.cells[1] == c->cells[1] && g.cells[2] == c->cells[2];
+    });
+    if (it == b->groups.end()) {
+      b->groups.emplace_back();
+      it = b->groups.end() - 1;
+      for (int d = 0; d < 3; ++d) it->cells[d] = c->cells[d];
+    }
+    it->members.push_back(r);
+  }
+  size_t work = 0;
+  for (auto& g : b->groups) {
+    const int m = int(g.members.size());
+    const int64_t N = int64_t(g.cells[0]) * g.cells[1] * g.cells[2];
+    const int64_t plane = int64_t(g.cells[0] / 2 + 1) * g.cells[1] * g.cells[2];
+    if (int64_t(9) * m * plane * 2 > INT32_MAX) return fail(DMK_ERR_ARG, "edge group too large for one cuFFT plan");
+    if ((rc = dalloc(&g.real, size_t(9) * m * N)) || (rc = dalloc(&g.spec, size_t(18) * m * plane))) return rc;
+    int nn[3] = {g.cells[2], g.cells[1], g.cells[0]};
+    int inemb[3] = {g.cells[2], g.cells[1], g.cells[0]};
+    int onemb[3] = {g.cells[2], g.cells[1], g.cells[0] / 2 + 1};
+    size_t w1 = 0, w2 = 0;
+    CKF(cufftCreate(&g.fwd));
+    CKF(cufftCreate(&g.bwd));
+    CKF(cufftSetAutoAllocation(g.fwd, 0));
+    CKF(cufftSetAutoAllocation(g.bwd, 0));
+    CKF(cufftMakePlanMany(g.fwd, 3, nn, inemb, 1, int(N), onemb, 1, int(plane), CUFFT_D2Z, 9 * m, &w1));
+    CKF(cufftMakePlanMany(g.bwd, 3, nn, onemb, 1, int(plane), inemb, 1, int(N), CUFFT_Z2D, 9 * m, &w2));
+    work = std::max(work, std::max(w1, w2));
+    for (int k = 0; k < m; ++k) {
+      BatchCtx& x = b->h_bc[g.members[k]];
+      x.fft_real = g.real + size_t(9) * k * N;
+      x.fft_spec = g.spec + size_t(18) * k * plane;
+    }
+  }
+  if (work) CK(cudaMalloc(&b->fft_work, work));
+  for (auto& g : b->groups) {
+    CKF(cufftSetWorkArea(g.fwd, b->fft_work));
+    CKF(cufftSetWorkArea(g.bwd, b->fft_work));
+    CKF(cufftSetStream(g.fwd, b->stream));
+    CKF(cufftSetStream(g.bwd, b->stream));
+  }
+  // the constitutive evaluation of the batch as a graph over the tables
+  BatchTables t;
+  t.f = reinterpret_cast<const Fields*>(b->d_tab + b->o_f);
+  t.w = reinterpret_cast<const PassWork*>(b->d_tab + b->o_w);
+  t.dt = reinterpret_cast<const double*>(b->d_tab + b->o_dt);
+  t.off = b->d_off;
+  t.ctx_of = b->d_ctx_of;
+  t.active = reinterpret_cast<const unsigned char*>(b->d_tab + b->o_active);
+  t.use_dot0 = reinterpret_cast<const int*>(b->d_tab + b->o_dot0);
+  t.apply = reinterpret_cast<const int*>(b->d_tab + b->o_apply);
+  t.n_items = b->n_items;
+  BatchPassBuffers pb;
+  pb.list[0] = b->d_list[0];
+  pb.list[1] = b->d_list[1];
+  pb.count = b->d_count;
+  pb.status = b->d_status;
+  pb.n_ctx = n;
+  pb.iter = b->d_iter;
+  pb.max_passes = 400000;   // bounded by substeps x state iterations; more means corrupted control state
+  cudaError_t e = cudaErrorInvalidValue;
+  switch (b->NS) {
+    case 12: e = batch_graph<12>(b, t, pb); break;
+    case 18: e = batch_graph<18>(b, t, pb); break;
+    case 24: e = batch_graph<24>(b, t, pb); break;
+    case 48: e = batch_graph<48>(b, t, pb); break;
+  }
+  if (e != cudaSuccess) return fail(DMK_ERR_CUDA, std::string("batch graph: ") + cudaGetErrorString(e));
+  CK(cudaGraphInstantiate(&b->exec, b->graph, 0));
+  return 0;
+}
+
+// Fixed-point state of one context of a batched solve (the locals of dmk_mech_solution)
+struct BatchSolve {
+  int evals = 0, reason = 0, count = 0, new_slot = -1, it = 0, apply = 0, m = 0, snes_max_its = 50, nsl = 0;
+  bool anderson = false, first = true, active = false;
+  std::vector<double> G, bvec;
+  std::vector<int> slots_b;
+};
+
+int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_state* out) {
+  const int n = b->n;
+  std::vector<BatchSolve> st(n);
+  std::vector<int> pos(n, -1);
+  for (int k = 0; k < nw; ++k) {
+    const int r = which[k];
+    if (r < 0 || r >= n) return fail(DMK_ERR_ARG, "batch member index out of range");
+    if (pos[r] >= 0) return fail(DMK_ERR_ARG, "batch member listed twice");
+    pos[r] = k;
+  }
+  b->last_ms[0] = b->last_ms[1] = 0.0;
+  for (int k = 0; k < nw; ++k) {
+    const int r = which[k];
+    dmk_ctx* c = b->ctx[r];
+    if (int rc = solution_prepare(c)) return rc;
+    BatchSolve& S = st[r];
+    S.active = true;
+    S.snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;
+    S.anderson = c->num.snes_type == 1;
+    S.m = c->aa_m;
+    S.G.assign(size_t(S.m > 0 ? S.m : 1) * (S.m > 0 ? S.m : 1), 0.0);
+    // the batch's launches follow the context's queued work (forward, solver scalars)
+    CK(cudaEventRecord(c->fork, c->stream));
+    CK(cudaStreamWaitEvent(b->stream, c->fork, 0));
+  }
+  CK(cudaEventRecord(b->ev[0], b->stream));
+  Fields* hf = reinterpret_cast<Fields*>(b->h_tab + b->o_f);
+  PassWork* hw = reinterpret_cast<PassWork*>(b->h_tab + b->o_w);
+  double* hdt = reinterpret_cast<double*>(b->h_tab + b->o_dt);
+  int* hdot0 = reinterpret_cast<int*>(b->h_tab + b->o_dot0);
+  int* happly = reinterpret_cast<int*>(b->h_tab + b->o_apply);
+  unsigned char* hact = reinterpret_cast<unsigned char*>(b->h_tab + b->o_active);
+  for (;;) {
+    int nact = 0, nchunks = 0;
+    for (int r = 0; r < n; ++r) {
+      dmk_ctx* c = b->ctx[r];
+      BatchSolve& S = st[r];
+      BatchCtx& x = b->h_bc[r];
+      x.active = S.active ? 1 : 0;
+      hact[r] = S.active ? 1 : 0;
+      if (!S.active) continue;
+      ++nact;
+      Fields f = make_fields(c, S.apply ? c->r : nullptr);
+      f.status = b->d_status + r;
+      hf[r] = f;
+      hw[r] = pass_work(c, 0, 0);
+      hdt[r] = c->dt;
+      hdot0[r] = c->dot0_valid ? 1 : 0;
+      happly[r] = S.apply;
+      x.P = c->P;
+      x.Pnew = c->Pnew;
+      x.r = c->r;
+      x.X = c->Fsol;
+      x.Rprev = c->aa_Rprev;
+      x.dX = c->aa_dX;
+      x.dR = c->aa_dR;
+      x.sc = c->sc;
+      x.nm2 = c->nm2;
+      x.gc = c->gc;
+      x.write_slot = -1;
+      x.nsl = 0;
+      S.nsl = 0;
+      if (S.anderson && S.new_slot >= 0) {
+        S.slots_b.clear();
+        const int mk = std::min(S.count, S.m);
+        for (int q = S.count - mk; q < S.count; ++q) S.slots_b.push_back(q % S.m);
+        S.nsl = int(S.slots_b.size());
+        x.write_slot = S.new_slot;
+        x.nsl = S.nsl;
+        for (int q = 0; q < S.nsl; ++q) x.slots[q] = S.slots_b[q];
+        nchunks = std::max(nchunks, (S.nsl + AA_CHUNK - 1) / AA_CHUNK);
+      }
+    }
+    if (nact == 0) break;
+    ++b->iterations;
+    CK(cudaMemcpyAsync(b->d_tab, b->h_tab, b->tab_bytes, cudaMemcpyHostToDevice, b->stream));
+    CK(cudaMemcpyAsync(b->d_bc, b->h_bc, sizeof(BatchCtx) * n, cudaMemcpyHostToDevice, b->stream));
+    // constitutive evaluation of every active context
+    CK(cudaEventRecord(b->ev[2], b->stream));
+    CK(cudaGraphLaunch(b->exec, b->stream));
+    CK(cudaEventRecord(b->ev[3], b->stream));
+    ++b->graph_launches;
+    // residuals: <P> and aim, Gamma convolution per edge group, convergence test, inner products
+    CK(launch_batch_aim(b->d_bc, n, b->max_nconst, b->stream));
+    CK(launch_batch_gather(b->d_bc, n, b->max_n9, b->stream));
+    for (auto& g : b->groups)
+      CKF(cufftExecD2Z(g.fwd, g.real, reinterpret_cast<cufftDoubleComplex*>(g.spec)));
+    CK(launch_batch_gamma(b->d_bc, n, b->max_nspec, b->stream));
+    for (auto& g : b->groups)
+      CKF(cufftExecZ2D(g.bwd, reinterpret_cast<cufftDoubleComplex*>(g.spec), g.real));
+    CK(launch_batch_scatter(b->d_bc, n, b->max_n9, b->stream));
+    CK(launch_batch_converge(b->d_bc, n, b->d_scal, b->stream));
+    for (int ch = 0; ch < nchunks; ++ch) CK(launch_batch_aa_dots(b->d_bc, n, b->max_aa_blocks, ch, b->stream));
+    CK(cudaMemcpyAsync(b->h_scal, b->d_scal, sizeof(BatchScal) * n, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaMemcpyAsync(b->h_iter, b->d_iter, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+    if (nchunks)
+      CK(cudaMemcpyAsync(b->h_dots, b->d_dots, sizeof(double) * n * BATCH_DOTS, cudaMemcpyDeviceToHost, b->stream));
+    CK(cudaStreamSynchronize(b->stream));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, b->ev[2], b->ev[3]));
+    b->last_ms[0] += ms;
+    b->passes += b->h_iter[0];
+    if (b->h_iter[1]) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
+    // decisions and Anderson updates
+    int naa = 0;
+    for (int r = 0; r < n; ++r) {
+      BatchSolve& S = st[r];
+      b->h_aa[r].active = 0;
+      if (!S.active) continue;
+      dmk_ctx* c = b->ctx[r];
+      const BatchScal& hs = b->h_scal[r];
+      if (hs.status == 0) std::swap(c->P, c->Pnew);
+      c->dot0_valid = true;
+      ++S.evals;
+      if (S.nsl > 0) {
+        const double* dots = b->h_dots + size_t(r) * BATCH_DOTS;
+        S.bvec.assign(S.nsl, 0.0);
+        for (int q = 0; q < S.nsl; ++q) {
+          const int ch = q / AA_CHUNK, k = q % AA_CHUNK;
+          const double gq = dots[ch * 2 * AA_CHUNK + k], bq = dots[ch * 2 * AA_CHUNK + AA_CHUNK + k];
+          S.G[size_t(S.new_slot) * S.m + S.slots_b[q]] = S.G[size_t(S.slots_b[q]) * S.m + S.new_slot] = gq;
+          S.bvec[q] = bq;
+        }
+      }
+      if (S.first && S.anderson) {   // b for the first Anderson step is empty (plain Richardson step)
+        S.bvec.clear();
+        S.slots_b.clear();
+      }
+      S.first = false;
+      S.reason = hs.reason;
+      if (S.reason == 0 && ++S.it > S.snes_max_its) S.reason = -1;
+      if (S.reason != 0) {
+        S.active = false;
+        continue;
+      }
+      if (!S.anderson) {
+        S.apply = 1;
+        continue;
+      }
+      std::vector<double> gam = anderson_coefficients(S.G, S.m, S.slots_b, S.bvec);
+      S.new_slot = S.count % S.m;
+      BatchAA& a = b->h_aa[r];
+      a.active = 1;
+      a.new_slot = S.new_slot;
+      a.u.n = int(S.slots_b.size());
+      for (int q = 0; q < AA_MAX; ++q) {
+        a.u.slot[q] = q < a.u.n ? S.slots_b[q] : 0;
+        a.u.gamma[q] = q < a.u.n ? gam[q] : 0.0;
+      }
+      ++S.count;
+      ++naa;
+    }
+    if (naa) {
+      CK(cudaMemcpyAsync(b->d_aa, b->h_aa, sizeof(BatchAA) * n, cudaMemcpyHostToDevice, b->stream));
+      CK(launch_batch_aa_update(b->d_bc, b->d_aa, n, b->max_aa_blocks, b->stream));
+    }
+  }
+  CK(cudaEventRecord(b->ev[1], b->stream));
+  CK(cudaEventSynchronize(b->ev[1]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+  b->last_ms[1] = ms;
+  // the contexts' own streams continue after the batch (tangent, forward of the next increment)
+  for (int k = 0; k < nw; ++k) {
+    const int r = which[k];
+    dmk_ctx* c = b->ctx[r];
+    CK(cudaStreamWaitEvent(c->stream, b->ev[1], 0));
+    const BatchScal& hs = b->h_scal[r];
+    if (int rc = solution_finish(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, st[r].reason,
+                                 st[r].evals, &out[k]))
+      return rc;
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmk_batch_create(dmk_batch** out, dmk_ctx* const* ctxs, int n) {
+  if (!out || !ctxs) return fail(DMK_ERR_ARG, "null argument");
+  *out = nullptr;
+  if (n < 1 || n > 65535) return fail(DMK_ERR_ARG, "a batch holds 1 to 65535 contexts");
+  for (int r = 0; r < n; ++r) {
+    const dmk_ctx* c = ctxs[r];
+    if (!c) return fail(DMK_ERR_ARG, "null context");
+    if (c->solver != 0) return fail(DMK_ERR_CONFIG, "batched solves run the basic scheme");
+    if (c->precision != DMK_PRECISION_FP64) return fail(DMK_ERR_CONFIG, "batched solves run the FP64 form");
+    if (c->device != ctxs[0]->device) return fail(DMK_ERR_ARG, "contexts of a batch share one device");
+    if (!same_phase(c, ctxs[0])) return fail(DMK_ERR_CONFIG, "contexts of a batch share one phase and its numerics");
+    for (int q = 0; q < r; ++q)
+      if (ctxs[q] == c) return fail(DMK_ERR_ARG, "context listed twice");
+  }
+  dmk_batch* b = new dmk_batch();
+  b->n = n;
+  b->ctx.assign(ctxs, ctxs + n);
+  b->NS = ctxs[0]->NS;
+  b->device = ctxs[0]->device;
+  b->nsm = ctxs[0]->nsm;
+  if (cudaSetDevice(b->device) != cudaSuccess) {
+    batch_free(b);
+    return fail(DMK_ERR_CUDA, "cudaSetDevice failed");
+  }
+  if (int rc = batch_build(b)) {
+    const std::string msg = g_err;
+    batch_free(b);
+    return fail(rc, msg);
+  }
+  *out = b;
+  return 0;
+}
+
+int dmk_batch_solution(dmk_batch* b, const int* which, int n_which, dmk_solution_state* out) {
+  if (!b || (n_which > 0 && (!which || !out))) return fail(DMK_ERR_ARG, "null argument");
+  if (n_which < 0 || n_which > b->n) return fail(DMK_ERR_ARG, "n_which out of range");
+  CK(cudaSetDevice(b->device));
+  return batch_solution_impl(b, which, n_which, out);
+}
+
+int dmk_batch_stats(dmk_batch* b, double out[5]) {
+  if (!b || !out) return fail(DMK_ERR_ARG, "null argument");
+  out[0] = b->last_ms[0];
+  out[1] = b->last_ms[1];
+  out[2] = double(b->graph_launches);
+  out[3] = double(b->passes);
+  out[4] = double(b->iterations);
+  return 0;
+}
+
+void dmk_batch_destroy(dmk_batch* b) { batch_free(b); }
 
 }  // extern "C"

@@ -15,9 +15,9 @@
 namespace dmk {
 
 // partial sums of a 9-plane field (used when the stale P field is kept after a failure)
-__global__ void __launch_bounds__(CONST_THREADS) sum9_kernel(const double* __restrict__ X, int64_t N, double* partials) {
+__device__ __forceinline__ void sum9_block(const double* __restrict__ X, int64_t N, double* partials, int bx) {
   __shared__ double red[9 * (CONST_THREADS / 32)];
-  const int64_t v = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t v = int64_t(bx) * blockDim.x + threadIdx.x;
   double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
   if (v < N)
 #pragma unroll
@@ -25,7 +25,10 @@ __global__ void __launch_bounds__(CONST_THREADS) sum9_kernel(const double* __res
   block_reduce_sum<9>(s, red);
   if (threadIdx.x == 0)
 #pragma unroll
-    for (int k = 0; k < 9; ++k) partials[int64_t(blockIdx.x) * 9 + k] = s[k];
+    for (int k = 0; k < 9; ++k) partials[int64_t(bx) * 9 + k] = s[k];
+}
+__global__ void __launch_bounds__(CONST_THREADS) sum9_kernel(const double* __restrict__ X, int64_t N, double* partials) {
+  sum9_block(X, N, partials, blockIdx.x);
 }
 cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s) {
   const int nb = int((N + CONST_THREADS - 1) / CONST_THREADS);
@@ -63,7 +66,7 @@ __device__ void rot33(const double* qin, const double* T, double* R, bool active
 // After the constitutive sweep: P_av = <P> (rotated to the load frame),
 // deltaF_aim = S : (P_av - P_aim), F_aim -= deltaF_aim, err_BC, and the rotated
 // aim for the DC term of the Gamma convolution (form_residual, grid_mech_spectral_basic.f90:503-519).
-__global__ void aim_kernel(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim) {
+__device__ __forceinline__ void aim_body(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim) {
   __shared__ double acc[9][32];
   const int t = threadIdx.x;
   for (int k = 0; k < 9; ++k) {
@@ -101,11 +104,14 @@ __global__ void aim_kernel(SolverScalars* sc, const double* partials, int nparts
   sc->err_BC = e;
   rot33(sc->q_rot, dF, sc->aim_rot, true);
 }
+__global__ void aim_kernel(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim) {
+  aim_body(sc, partials, nparts, wgt, update_aim);
+}
 
 // converged(), grid_mech_spectral_basic.f90:422-458, plus the SNES bookkeeping of the
 // Richardson iteration.  reason: 0 iterating, 1 converged, -1 diverged.
-__global__ void converge_kernel(SolverScalars* sc, const double* div_partials, int nparts, double wgt,
-                                const int* status, const Numerics2 nm2, int count_iteration) {
+__device__ __forceinline__ void converge_body(SolverScalars* sc, const double* div_partials, int nparts, double wgt,
+                                              const int* status, const Numerics2& nm2, int count_iteration) {
   __shared__ double acc[32];
   const int t = threadIdx.x;
   double s = 0.0;
@@ -132,6 +138,10 @@ __global__ void converge_kernel(SolverScalars* sc, const double* div_partials, i
   sc->status = *status;
   sc->reason = reason;
 }
+__global__ void converge_kernel(SolverScalars* sc, const double* div_partials, int nparts, double wgt,
+                                const int* status, const Numerics2 nm2, int count_iteration) {
+  converge_body(sc, div_partials, nparts, wgt, status, nm2, count_iteration);
+}
 
 cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s) {
   aim_kernel<<<1, 32, 0, s>>>(sc, partials, nparts, wgt, update_aim);
@@ -154,15 +164,15 @@ cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int n
 // and the even-grid Nyquist corner where all a_i vanish) are set to zero; k = 0 then
 // receives the aim.
 template <typename Real>
-__global__ void __launch_bounds__(SPEC_THREADS)
-gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
-                 const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
-                 double* __restrict__ div_partials, int do_gamma, int do_div) {
+__device__ __forceinline__ void
+gamma_div_block(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                 const GammaConst& gc, const SolverScalars* __restrict__ sc,
+                 double* __restrict__ div_partials, int do_gamma, int do_div, int bx) {
   __shared__ double red[SPEC_THREADS / 32];
   using C2 = typename std::conditional<sizeof(Real) == 8, double2, float2>::type;
   C2* S = reinterpret_cast<C2*>(spec);
   const int red0 = n0 / 2 + 1;
-  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t idx = int64_t(bx) * blockDim.x + threadIdx.x;
   double dsum = 0.0;
   if (idx < plane) {
     const int kx = int(idx % red0);
@@ -280,7 +290,7 @@ gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2,
     if (threadIdx.x == 0) {
       double s = 0.0;
       for (int w = 0; w < SPEC_THREADS / 32; ++w) s += red[w];
-      div_partials[blockIdx.x] = s;
+      div_partials[bx] = s;
     }
   }
 }
@@ -292,15 +302,15 @@ gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2,
 // arithmetic.  Points with |det Re K| <= 1e-16 are zero; k = 0 receives the aim.  The divergence
 // term is |P_hat conj(-xi) rescale|^2 with the same plane weights as gamma_div_kernel.
 template <typename Real>
-__global__ void __launch_bounds__(SPEC_THREADS)
-gamma_div_fwbw_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
-                      const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
-                      double* __restrict__ div_partials, int do_gamma, int do_div) {
+__device__ __forceinline__ void
+gamma_div_fwbw_block(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                      const GammaConst& gc, const SolverScalars* __restrict__ sc,
+                      double* __restrict__ div_partials, int do_gamma, int do_div, int bx) {
   __shared__ double red[SPEC_THREADS / 32];
   using C2 = typename std::conditional<sizeof(Real) == 8, double2, float2>::type;
   C2* S = reinterpret_cast<C2*>(spec);
   const int red0 = n0 / 2 + 1;
-  const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
+  const int64_t idx = int64_t(bx) * blockDim.x + threadIdx.x;
   double dsum = 0.0;
   if (idx < plane) {
     const int kx = int(idx % red0);
@@ -455,9 +465,24 @@ gamma_div_fwbw_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, in
     if (threadIdx.x == 0) {
       double s = 0.0;
       for (int w = 0; w < SPEC_THREADS / 32; ++w) s += red[w];
-      div_partials[blockIdx.x] = s;
+      div_partials[bx] = s;
     }
   }
+}
+
+template <typename Real>
+__global__ void __launch_bounds__(SPEC_THREADS)
+gamma_div_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                 const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
+                 double* __restrict__ div_partials, int do_gamma, int do_div) {
+  gamma_div_block<Real>(spec, plane, n0, n1, n2, L0, L1, L2, gc, sc, div_partials, do_gamma, do_div, blockIdx.x);
+}
+template <typename Real>
+__global__ void __launch_bounds__(SPEC_THREADS)
+gamma_div_fwbw_kernel(Real* __restrict__ spec, int64_t plane, int n0, int n1, int n2, double L0, double L1, double L2,
+                      const __grid_constant__ GammaConst gc, const SolverScalars* __restrict__ sc,
+                      double* __restrict__ div_partials, int do_gamma, int do_div) {
+  gamma_div_fwbw_block<Real>(spec, plane, n0, n1, n2, L0, L1, L2, gc, sc, div_partials, do_gamma, do_div, blockIdx.x);
 }
 
 template <typename Real>
@@ -736,26 +761,21 @@ namespace dmk {
 // After an evaluation with residual R: dR[slot] = R - Rprev (if write_slot >= 0), and the
 // inner products g_t = dR[slot].dR[t] and b_t = dR[t].R for up to AA_CHUNK history slots
 // per launch (per-block partial sums, reduced by the caller in block order).
-constexpr int AA_CHUNK = 8;
-struct AASlots {
-  int n;                 // slots in this chunk
-  int slot[AA_CHUNK];
-};
 
-__global__ void __launch_bounds__(256)
-aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, double* __restrict__ dR, int64_t n,
-               int write_slot, AASlots sl, double* __restrict__ partials) {
+__device__ __forceinline__ void aa_dots_block(const double* __restrict__ R, const double* __restrict__ Rprev,
+                                              double* __restrict__ dR, int64_t n, int write_slot, const AASlots& sl,
+                                              double* __restrict__ partials, int bx, int nb, bool write) {
   __shared__ double red[2 * AA_CHUNK][8];
   double g[AA_CHUNK], b[AA_CHUNK];
 #pragma unroll
   for (int q = 0; q < AA_CHUNK; ++q) { g[q] = 0.0; b[q] = 0.0; }
 #pragma unroll 2
-  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+  for (int64_t e = int64_t(bx) * blockDim.x + threadIdx.x; e < n; e += int64_t(nb) * blockDim.x) {
     const double r = R[e];
     double dn = 0.0;
     if (write_slot >= 0) {
       dn = r - Rprev[e];
-      if (blockIdx.y == 0) dR[int64_t(write_slot) * n + e] = dn;
+      if (write) dR[int64_t(write_slot) * n + e] = dn;
     }
 #pragma unroll
     for (int q = 0; q < AA_CHUNK; ++q) {
@@ -780,13 +800,18 @@ aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, d
   if (threadIdx.x < 2 * AA_CHUNK) {
     double s = 0.0;
     for (int w = 0; w < 8; ++w) s += red[threadIdx.x][w];
-    partials[int64_t(blockIdx.x) * 2 * AA_CHUNK + threadIdx.x] = s;
+    partials[int64_t(bx) * 2 * AA_CHUNK + threadIdx.x] = s;
   }
+}
+__global__ void __launch_bounds__(256)
+aa_dots_kernel(const double* __restrict__ R, const double* __restrict__ Rprev, double* __restrict__ dR, int64_t n,
+               int write_slot, AASlots sl, double* __restrict__ partials) {
+  aa_dots_block(R, Rprev, dR, n, write_slot, sl, partials, blockIdx.x, gridDim.x, true);
 }
 
 // 16 lanes per output, each summing every 16th block partial, then a fixed-order combine
-__global__ void __launch_bounds__(256) aa_reduce_kernel(const double* __restrict__ partials, int nblocks,
-                                                        double* __restrict__ out) {
+__device__ __forceinline__ void aa_reduce_body(const double* __restrict__ partials, int nblocks,
+                                               double* __restrict__ out) {
   __shared__ double acc[16][2 * AA_CHUNK];
   const int t = threadIdx.x, q = t % (2 * AA_CHUNK), lane = t / (2 * AA_CHUNK);
   double s = 0.0;
@@ -798,6 +823,10 @@ __global__ void __launch_bounds__(256) aa_reduce_kernel(const double* __restrict
     for (int l = 0; l < 16; ++l) tot += acc[l][t];
     out[t] = tot;
   }
+}
+__global__ void __launch_bounds__(256) aa_reduce_kernel(const double* __restrict__ partials, int nblocks,
+                                                        double* __restrict__ out) {
+  aa_reduce_body(partials, nblocks, out);
 }
 
 cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,
@@ -820,17 +849,12 @@ cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int
 }
 
 // X <- X - R - sum_t gamma_t (dX[t] - dR[t]);  dX[new_slot] = X_new - X_old;  Rprev = R
-struct AAUpdate {
-  int n;
-  int slot[32];
-  double gamma[32];
-};
-__global__ void __launch_bounds__(256)
-aa_update_kernel(double* __restrict__ X, const double* __restrict__ R, double* __restrict__ Rprev,
-                 double* __restrict__ dX, const double* __restrict__ dR, int64_t n, int new_slot,
-                 const __grid_constant__ AAUpdate u) {
+__device__ __forceinline__ void aa_update_block(double* __restrict__ X, const double* __restrict__ R,
+                                                double* __restrict__ Rprev, double* __restrict__ dX,
+                                                const double* __restrict__ dR, int64_t n, int new_slot,
+                                                const AAUpdate& u, int bx, int nb) {
 #pragma unroll 2
-  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x) {
+  for (int64_t e = int64_t(bx) * blockDim.x + threadIdx.x; e < n; e += int64_t(nb) * blockDim.x) {
     const double x = X[e], r = R[e];
     double xn = x - r;
     for (int q = 0; q < u.n; ++q) {
@@ -842,12 +866,146 @@ aa_update_kernel(double* __restrict__ X, const double* __restrict__ R, double* _
     Rprev[e] = r;
   }
 }
+__global__ void __launch_bounds__(256)
+aa_update_kernel(double* __restrict__ X, const double* __restrict__ R, double* __restrict__ Rprev,
+                 double* __restrict__ dX, const double* __restrict__ dR, int64_t n, int new_slot,
+                 const __grid_constant__ AAUpdate u) {
+  aa_update_block(X, R, Rprev, dX, dR, n, new_slot, u, blockIdx.x, gridDim.x);
+}
 cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* dX, const double* dR, int64_t n,
                              int new_slot, const int* slots, const double* gamma, int nslots, int nblocks, cudaStream_t s) {
   AAUpdate u;
   u.n = nslots;
   for (int q = 0; q < 32; ++q) { u.slot[q] = q < nslots ? slots[q] : 0; u.gamma[q] = q < nslots ? gamma[q] : 0.0; }
   aa_update_kernel<<<nblocks, 256, 0, s>>>(X, R, Rprev, dX, dR, n, new_slot, u);
+  return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------ batches of contexts
+// Blocks beyond a context's own block count, and contexts not evaluated in this iteration, return
+// at once (uniformly per block, before any barrier).
+
+__global__ void __launch_bounds__(CONST_THREADS) batch_sum9_kernel(const BatchCtx* __restrict__ t) {
+  const BatchCtx& c = t[blockIdx.y];
+  if (!c.active || int(blockIdx.x) >= c.nconst) return;
+  sum9_block(*c.status == 0 ? c.Pnew : c.P, c.N, c.partials, blockIdx.x);
+}
+__global__ void batch_aim_kernel(const BatchCtx* __restrict__ t) {
+  const BatchCtx& c = t[blockIdx.x];
+  if (!c.active) return;
+  aim_body(c.sc, c.partials, c.nconst, c.wgt, 1);
+}
+cudaError_t launch_batch_aim(const BatchCtx* t, int n_ctx, int max_nconst, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  batch_sum9_kernel<<<dim3(max_nconst, n_ctx), CONST_THREADS, 0, s>>>(t);
+  batch_aim_kernel<<<n_ctx, 32, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+constexpr int BATCH_COPY_BLOCKS = 64;   // blocks per context of the gather and scatter copies
+__global__ void __launch_bounds__(256) batch_gather_kernel(const BatchCtx* __restrict__ t) {
+  const BatchCtx& c = t[blockIdx.y];
+  if (!c.active) return;
+  const double* __restrict__ src = *c.status == 0 ? c.Pnew : c.P;
+  double* __restrict__ dst = c.fft_real;
+  const int64_t n = 9 * c.N;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x)
+    dst[e] = src[e];
+}
+__global__ void __launch_bounds__(256) batch_scatter_kernel(const BatchCtx* __restrict__ t) {
+  const BatchCtx& c = t[blockIdx.y];
+  if (!c.active) return;
+  const double* __restrict__ src = c.fft_real;
+  double* __restrict__ dst = c.r;
+  const int64_t n = 9 * c.N;
+  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x)
+    dst[e] = src[e];
+}
+cudaError_t launch_batch_gather(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  const int nb = int(std::min<int64_t>(BATCH_COPY_BLOCKS, (max_n9 + 255) / 256));
+  batch_gather_kernel<<<dim3(nb, n_ctx), 256, 0, s>>>(t);
+  return cudaGetLastError();
+}
+cudaError_t launch_batch_scatter(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  const int nb = int(std::min<int64_t>(BATCH_COPY_BLOCKS, (max_n9 + 255) / 256));
+  batch_scatter_kernel<<<dim3(nb, n_ctx), 256, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(SPEC_THREADS) batch_gamma_kernel(const BatchCtx* __restrict__ t) {
+  const BatchCtx& c = t[blockIdx.y];
+  if (!c.active || int(blockIdx.x) >= c.nspec) return;
+  const int64_t plane = int64_t(c.n[0] / 2 + 1) * c.n[1] * c.n[2];
+  double* spec = static_cast<double*>(c.fft_spec);
+  if (c.gc.derivative == 2)
+    gamma_div_fwbw_block<double>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
+                                 blockIdx.x);
+  else
+    gamma_div_block<double>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
+                            blockIdx.x);
+}
+cudaError_t launch_batch_gamma(const BatchCtx* t, int n_ctx, int max_nspec, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  batch_gamma_kernel<<<dim3(max_nspec, n_ctx), SPEC_THREADS, 0, s>>>(t);
+  return cudaGetLastError();
+}
+
+__global__ void batch_converge_kernel(const BatchCtx* __restrict__ t, BatchScal* __restrict__ out) {
+  const BatchCtx& c = t[blockIdx.x];
+  if (!c.active) return;
+  converge_body(c.sc, c.divp, c.nspec, c.wgt, c.status, c.nm2, 1);
+  if (threadIdx.x != 0) return;
+  BatchScal& o = out[blockIdx.x];
+  const SolverScalars* sc = c.sc;
+  for (int k = 0; k < 9; ++k) {
+    o.P_av[k] = sc->P_av[k];
+    o.F_aim[k] = sc->F_aim[k];
+  }
+  o.err_div = sc->err_div;
+  o.err_BC = sc->err_BC;
+  o.totalIter = sc->totalIter;
+  o.reason = sc->reason;
+  o.status = sc->status;
+}
+cudaError_t launch_batch_converge(const BatchCtx* t, int n_ctx, BatchScal* out, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  batch_converge_kernel<<<n_ctx, 32, 0, s>>>(t, out);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) batch_aa_dots_kernel(const BatchCtx* __restrict__ t, int chunk) {
+  const BatchCtx& c = t[blockIdx.y];
+  if (!c.active || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl || int(blockIdx.x) >= c.aa_blocks) return;
+  AASlots sl;
+  sl.n = min(AA_CHUNK, c.nsl - chunk * AA_CHUNK);
+#pragma unroll
+  for (int q = 0; q < AA_CHUNK; ++q) sl.slot[q] = q < sl.n ? c.slots[chunk * AA_CHUNK + q] : 0;
+  aa_dots_block(c.r, c.Rprev, c.dR, 9 * c.N, c.write_slot, sl, c.aa_partials, blockIdx.x, c.aa_blocks, true);
+}
+__global__ void __launch_bounds__(256) batch_aa_reduce_kernel(const BatchCtx* __restrict__ t, int chunk) {
+  const BatchCtx& c = t[blockIdx.x];
+  if (!c.active || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl) return;
+  aa_reduce_body(c.aa_partials, c.aa_blocks, c.aa_out + chunk * 2 * AA_CHUNK);
+}
+cudaError_t launch_batch_aa_dots(const BatchCtx* t, int n_ctx, int max_blocks, int chunk, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  batch_aa_dots_kernel<<<dim3(max_blocks, n_ctx), 256, 0, s>>>(t, chunk);
+  batch_aa_reduce_kernel<<<n_ctx, 256, 0, s>>>(t, chunk);
+  return cudaGetLastError();
+}
+
+__global__ void __launch_bounds__(256) batch_aa_update_kernel(const BatchCtx* __restrict__ t,
+                                                              const BatchAA* __restrict__ u) {
+  const BatchCtx& c = t[blockIdx.y];
+  const BatchAA& a = u[blockIdx.y];
+  if (!a.active || int(blockIdx.x) >= c.aa_blocks) return;
+  aa_update_block(c.X, c.r, c.Rprev, c.dX, c.dR, 9 * c.N, a.new_slot, a.u, blockIdx.x, c.aa_blocks);
+}
+cudaError_t launch_batch_aa_update(const BatchCtx* t, const BatchAA* u, int n_ctx, int max_blocks, cudaStream_t s) {
+  if (n_ctx <= 0) return cudaSuccess;
+  batch_aa_update_kernel<<<dim3(max_blocks, n_ctx), 256, 0, s>>>(t, u);
   return cudaGetLastError();
 }
 

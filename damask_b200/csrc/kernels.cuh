@@ -84,6 +84,30 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
+// Tables of a batch of contexts of one phase (the constitutive passes of all of them in shared
+// launches): items are the voxels of all contexts, context after context.
+struct BatchTables {
+  const Fields* f;               // per context: its fields
+  const PassWork* w;             // per context: its pass work planes
+  const double* dt;              // per context: the time step of its current increment
+  const int64_t* off;            // per context: its first item (off[n_ctx] = n_items)
+  const int* ctx_of;             // per item: its context
+  const unsigned char* active;   // per context: evaluated in this launch
+  const int* use_dot0;           // per context: the increment-start rates are stored already
+  const int* apply;              // per context: fuse F <- F - r into the first pass
+  int64_t n_items;
+};
+struct BatchPassBuffers {
+  int* list[2];                  // item lists of the passes (n_items entries each)
+  int* count;                    // their 2 entry counts
+  int* status;                   // per context: worst status of the evaluation (Fields::status)
+  int n_ctx;
+  int* iter;                     // [0] passes run, [1] set when max_passes stopped the loop
+  int max_passes;
+};
+template <int NS>
+cudaError_t build_batch_pass_graph(const PhaseConst<NS>& pc, const Numerics& nm, const BatchTables& t,
+                                   const BatchPassBuffers& b, int nsm, cudaStream_t s, cudaGraph_t* out);
 cudaError_t launch_sum9(const double* X, int64_t N, double* partials, cudaStream_t s);
 cudaError_t launch_aim(SolverScalars* sc, const double* partials, int nparts, double wgt, int update_aim, cudaStream_t s);
 cudaError_t launch_converge(SolverScalars* sc, const double* div_partials, int nparts, double wgt, const int* status,
@@ -137,10 +161,76 @@ cudaError_t launch_coords(const double* u, const double* favg, const int n[3], c
 
 // Anderson acceleration of the fixed point (kernels.cu)
 constexpr int AA_MAX = 32;
+constexpr int AA_CHUNK = 8;    // history slots per inner-product launch
+struct AASlots {
+  int n;                       // slots in this chunk
+  int slot[AA_CHUNK];
+};
+struct AAUpdate {              // X <- X - R - sum_q gamma_q (dX[slot_q] - dR[slot_q])
+  int n;
+  int slot[AA_MAX];
+  double gamma[AA_MAX];
+};
 cudaError_t launch_aa_dots(const double* R, const double* Rprev, double* dR, int64_t n, int write_slot,
                            const int* slots, int nslots, double* partials, int nblocks, double* out, cudaStream_t s);
 cudaError_t launch_aa_update(double* X, const double* R, double* Rprev, double* dX, const double* dR, int64_t n,
                              int new_slot, const int* slots, const double* gamma, int nslots, int nblocks, cudaStream_t s);
+
+// ------------------------------------------------------------------ batches of contexts (kernels.cu)
+// The fixed-point iteration of many contexts (RVEs) in shared launches.  Each context is one entry
+// of a device table; a batched kernel takes its context from blockIdx.y (blockIdx.x for one block
+// per context) and keeps the block decomposition of the single-context kernel, so every context's
+// sums, spectra and updates are those of its standalone solve.
+struct BatchCtx {
+  const double* P;          // stress kept when the evaluation failed
+  const double* Pnew;       // stress of the evaluation, committed when its status is 0
+  const int* status;        // status of the evaluation
+  double* r;                // residual field (9 planes)
+  double* X;                // solver F (9 planes)
+  double* Rprev;            // Anderson: residual of the previous evaluation
+  double* dX;               // Anderson history
+  double* dR;
+  SolverScalars* sc;
+  double* partials;         // per block of CONST_THREADS voxels: 9 sums of the committed stress
+  double* divp;             // per Gamma block: divergence partial sums
+  double* aa_partials;      // per Anderson block: 2 AA_CHUNK partial sums
+  double* aa_out;           // per chunk: 2 AA_CHUNK sums (g then b)
+  double* fft_real;         // the context's 9 planes in its edge group's real buffer
+  void* fft_spec;           // the context's 9 spectra in the group's spectrum buffer
+  int64_t N;
+  double wgt;
+  double L[3];
+  int n[3];
+  int nconst, nspec, aa_blocks;
+  int active;               // evaluated in this fixed-point iteration
+  int write_slot;           // Anderson: slot of the new dR, -1 for none
+  int nsl;                  // Anderson: history slots of the inner products (oldest -> newest)
+  int slots[AA_MAX];
+  Numerics2 nm2;
+  GammaConst gc;
+};
+struct BatchAA {            // Anderson update of one context
+  int active, new_slot;
+  AAUpdate u;
+};
+struct BatchScal {          // solver scalars of one context, read back after each iteration
+  double P_av[9], F_aim[9];
+  double err_div, err_BC;
+  int totalIter, reason, status, pad;
+};
+// <P> of the committed stress and the aim update (sum9 + aim)
+cudaError_t launch_batch_aim(const BatchCtx* t, int n_ctx, int max_nconst, cudaStream_t s);
+// committed stress -> the group's real buffers (before the forward transforms)
+cudaError_t launch_batch_gather(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s);
+// Gamma convolution and divergence partial sums on the group spectra (FP64)
+cudaError_t launch_batch_gamma(const BatchCtx* t, int n_ctx, int max_nspec, cudaStream_t s);
+// the group's real buffers (after the inverse transforms) -> residual fields
+cudaError_t launch_batch_scatter(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s);
+// convergence test, and the scalars of every context into out
+cudaError_t launch_batch_converge(const BatchCtx* t, int n_ctx, BatchScal* out, cudaStream_t s);
+// Anderson inner products of one chunk of history slots (dots and their reduction)
+cudaError_t launch_batch_aa_dots(const BatchCtx* t, int n_ctx, int max_blocks, int chunk, cudaStream_t s);
+cudaError_t launch_batch_aa_update(const BatchCtx* t, const BatchAA* u, int n_ctx, int max_blocks, cudaStream_t s);
 
 // hand-written adjoint of an increment (adjoint.cu)
 constexpr int ADJ_KRYLOV_MAX = 30;   // restart length of the Krylov solve of the transposed equilibrium problem

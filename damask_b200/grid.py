@@ -407,6 +407,20 @@ class IncrementDriver:
             setattr(self, k, st[k])
 
     def step(self) -> list[IncrementStats]:
+        """One load-case increment with the solver's own solution call."""
+        gen = self.step_requests()
+        try:
+            gen.send(None)
+            while True:
+                gen.send(self.solver.solution())
+        except StopIteration as stop:
+            return stop.value
+
+    def step_requests(self):
+        """The increment of :meth:`step` as a generator: it yields where the solver's solution is
+        needed (after forward and materialpoint_forward), is sent that solution, and returns the
+        converged (sub)increments.  A batch drives many drivers this way and solves their requests
+        together."""
         if self.done:
             return []
         lc = self.loadcases[self._l]
@@ -437,7 +451,7 @@ class IncrementDriver:
             self.solver.forward(self.cut_back, self._guess, self.Delta_t, Delta_t_prev, t_remaining, lc)
             if not self.cut_back:
                 self.solver.materialpoint_forward()
-            sol = self.solver.solution()
+            sol = yield
             if self.sync is not None:
                 self.sync()
             dt_wall = time.perf_counter() - t0

@@ -365,6 +365,25 @@ int dmk_adj_finish(dmk_ctx* ctx, double theta_bar[20]);
    family.  Ns is the compiled slip-system count (12, 18, 24 or 48). */
 int dmk_adj_local_jacobian(const dmk_phase* phase, double dt, const double* point, double* D);
 
+/* Batches of independent RVEs (no counterpart in the reference, which solves one grid per
+   process).  A batch takes contexts of one phase and one set of constitutive numerics, basic scheme,
+   FP64 form, on one device, and solves one increment of any subset of them together:
+   dmk_batch_solution does what dmk_mech_solution does for each listed context, with the
+   iterations of all of them in shared launches (per fixed-point iteration one CUDA graph for the
+   constitutive evaluation of every active context, one cuFFT plan pair per edge size, batched
+   aim / Gamma / convergence / Anderson kernels, one host read of the solver scalars).  Each
+   context's results equal those of its own dmk_mech_solution call.  The other calls
+   (dmk_mech_forward, dmk_materialpoint_forward, ...) stay per context and may put the members of a
+   batch at different increments and time steps.  A batch uses the contexts' memory: destroy it
+   before them.  which[k] indexes ctxs of dmk_batch_create; out[k] is its solution state. */
+typedef struct dmk_batch dmk_batch;
+int dmk_batch_create(dmk_batch** out, dmk_ctx* const* ctxs, int n);
+int dmk_batch_solution(dmk_batch* batch, const int* which, int n_which, dmk_solution_state* out);
+/* out: device ms of the constitutive graphs and of the whole last dmk_batch_solution, graphs
+   launched, constitutive passes and fixed-point iterations of the batch so far */
+int dmk_batch_stats(dmk_batch* batch, double out[5]);
+void dmk_batch_destroy(dmk_batch* batch);
+
 /* Volume average <f> of a 9-component field that the caller already holds in device
    memory (9 planes of n_voxels doubles: component c of voxel v at field[c*n_voxels + v]),
    written to mean[9] on the host.  No counterpart in the reference: it exists for hosts

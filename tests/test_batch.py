@@ -1,4 +1,6 @@
-"""The batched workload: many independent RVEs of uneven size on one GPU (damask_b200/batch.py)."""
+"""The batched workload: many independent RVEs of uneven size on one GPU (damask_b200/batch.py):
+the library's batch (shared launches, dmk_batch_*) and the host-thread runner, each against
+standalone runs of the same RVEs."""
 import numpy as np
 import pytest
 
@@ -45,3 +47,55 @@ def test_batch_equals_standalone_runs(gpu):
         assert rel(fields[k], s.get_field('P')) < 1e-12
         assert br.updates[k] == sum(r.residual_evals for r in ref) * s.N
         s.close()
+
+
+def _standalone(job, n):
+    from damask_b200.grid import SpectralBasic, run_load_cases
+    rve, phase, lcs, num = job
+    s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num)
+    stats = run_load_cases(s, lcs, max_increments=n)
+    return s, stats
+
+
+@pytest.mark.gpu
+def test_device_batch_equals_standalone_runs(gpu):
+    """Eight RVEs of four edge sizes in one batch of the library: per fixed-point iteration one CUDA
+    graph evaluates the constitutive update of every active RVE, one cuFFT plan pair per edge size
+    transforms them, batched kernels form aim, Gamma, convergence test and Anderson step.  The
+    members differ in what a batch must keep per RVE: one runs the Richardson iteration, one the
+    FWBW_difference derivative, one Anderson depth 12 (two chunks of inner products), one a
+    shorter load case with twice the time step (it leaves the batch early, so later calls solve
+    subsets).  Each RVE matches its standalone run: fixed-point iterations and residual
+    evaluations per increment, constitutive counters, <P> per increment within 1e-12 and the fields
+    within 1e-10: the batched cuFFT plans (9 x RVEs transforms per plan instead of 9) may round
+    differently, and the fixed point carries last-bit differences of the residual into the fields
+    (measured 1.1e-11 for the P field of a 32^3 member)."""
+    from damask_b200.batch import DeviceBatch
+    jobs = workloads.batched_jobs(8, seed=11)
+    jobs[1][3].PETSc_options = '-snes_type nrichardson'
+    jobs[2][3].derivative = 'FWBW_difference'
+    jobs[3][3].anderson_m = 12
+    rve, phase, _, num = jobs[4]
+    jobs[4] = (rve, phase, workloads.tension_along([1.0, 2.0, 2.0], 4.0, 2), num)
+    assert len({j[0].cells for j in jobs}) >= 3
+    n = 4
+    db = DeviceBatch(jobs, max_increments=n)
+    db.run()
+    st = db.stats()
+    assert st['graphs'] >= st['iterations'] > 0 and st['passes'] > 0
+    errs = {}
+    for k, job in enumerate(jobs):
+        s, ref = _standalone(job, n)
+        got = db.results[k]
+        assert len(got) == len(ref) == (2 if k == 4 else n)
+        assert [r.iterations for r in got] == [r.iterations for r in ref], k
+        assert [r.residual_evals for r in got] == [r.residual_evals for r in ref], k
+        for a, b in zip(got, ref):
+            assert rel(a.P_av, b.P_av) < 1e-12, (k, a.inc)
+        g = db.solvers[k]
+        assert np.array_equal(g.total_counters[:3], s.total_counters[:3]), (k, g.total_counters, s.total_counters)
+        errs[k] = {name: rel(g.get_field(name), s.get_field(name)) for name in ('P', 'F', 'F_p', 'xi_sl', 'gamma_sl')}
+        s.close()
+    db.close()
+    print('field differences batch vs standalone:', errs)
+    assert max(max(e.values()) for e in errs.values()) < 1e-10, errs

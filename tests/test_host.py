@@ -239,3 +239,56 @@ def test_sta_file(oracle_lib, tmp_path):
     assert [r[0] for r in rows] == [s.inc for s in stats] == [1, 2, 3]
     assert [r[4] for r in rows] == [s.iterations for s in stats] and all(r[3] for r in rows)
     assert abs(rows[-1][1] - 3.0) < 1e-12
+
+
+def test_driver_requests_match_step():
+    """IncrementDriver.step_requests (the generator a batch drives) takes the same steps as
+    step(): forward / materialpoint_forward calls, cutbacks and statistics."""
+    from damask_b200.grid import IncrementDriver
+    lc = workloads.tension_x(4.0, 4)
+    a = FakeSolver(fail_at=[1, 4])
+    ref = run_load_cases(a, lc)
+    b = FakeSolver(fail_at=[1, 4])
+    drv = IncrementDriver(b, lc)
+    got = []
+    while not drv.done:
+        gen = drv.step_requests()
+        try:
+            gen.send(None)
+            while True:
+                gen.send(b.solution())
+        except StopIteration as stop:
+            got.extend(stop.value)
+    assert a.calls == b.calls
+    assert [(s.inc, s.t, s.cutback_level) for s in got] == [(s.inc, s.t, s.cutback_level) for s in ref]
+
+
+def test_device_batch_scheduling():
+    """DeviceBatch.run with the batched solve replaced by scripted solvers: jobs with different
+    cutbacks and lengths fall out of step, each request goes to its own job, every job runs its
+    increments, and the jobs' call sequences equal their standalone runs."""
+    from damask_b200.batch import DeviceBatch
+    from damask_b200.grid import IncrementDriver
+    loads = [workloads.tension_x(4.0, 4), workloads.tension_x(2.0, 2), workloads.tension_x(4.0, 4)]
+    fails = [[1], [], [0, 3]]
+    db = object.__new__(DeviceBatch)
+    db.jobs = loads
+    db.max_increments = None
+    fakes = [FakeSolver(f) for f in fails]
+    db.drivers = [IncrementDriver(s, lc) for s, lc in zip(fakes, loads)]
+    db.results = [[] for _ in loads]
+    db.batch_calls = 0
+    db._gens = [None] * len(loads)
+    sizes = []
+
+    def solve(waiting):
+        sizes.append(len(waiting))
+        return [fakes[k].solution() for k in waiting]
+
+    db.run(solve=solve)
+    for k, (lc, f) in enumerate(zip(loads, fails)):
+        s = FakeSolver(f)
+        ref = run_load_cases(s, lc)
+        assert fakes[k].calls == s.calls
+        assert [(r.inc, r.t) for r in db.results[k]] == [(r.inc, r.t) for r in ref]
+    assert db.batch_calls == len(sizes) and sizes[0] == 3 and sizes[-1] < 3
