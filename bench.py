@@ -289,15 +289,97 @@ def _json_default(o):
     raise TypeError(type(o))
 
 
+def flop_sample(increments: int) -> None:
+    """The constitutive counters and the static FP64 FLOP count of the first increments of a 32^3 cut of
+    the bcc-24 workload (FP64), printed as one JSON line: the run that an ncu count of the FP64
+    instructions of the constitutive kernels checks the static model against."""
+    from damask_b200 import workloads
+    from damask_b200.grid import IncrementDriver, SpectralBasic
+    rve, phase, lcs, num = workloads.make_cut(WORKLOAD, (32, 32, 32))
+    s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision='fp64')
+    drv = IncrementDriver(s, lcs)
+    for _ in range(increments):
+        drv.step()
+    c = s.total_counters
+    print(json.dumps({'workload': f'{WORKLOAD} 32^3 cut', 'increments': increments, 'updates': int(c[0]),
+                      'state_iterations': int(c[1]), 'newton_iterations': int(c[2]), 'residual_evals': int(c[3]),
+                      'static_fp64_flop': constitutive_flops(phase.n_slip, c[2], c[1], c[0])}), flush=True)
+    s.close()
+
+
+def _timed_run(solver, lcs, n=None) -> dict:
+    """Wall time, device time and counters of the first n increments (all: None) of a solver."""
+    from damask_b200.grid import run_load_cases
+    t0 = time.perf_counter()
+    st = run_load_cases(solver, lcs, max_increments=n)
+    wall = time.perf_counter() - t0
+    upd = sum(r.residual_evals for r in st) * solver.N
+    out = {'increments': len(st), 'wall_s': wall, 's_per_increment': wall / max(1, len(st)), 'updates': upd,
+           'updates_per_s': upd / wall, 'iterations': [r.iterations for r in st][:8]}
+    if hasattr(solver, 'total_ms'):
+        dev = float(np.sum(solver.total_ms)) * 1e-3
+        out.update({'device_s': dev, 'device_updates_per_s': upd / dev if dev > 0 else None})
+    return out
+
+
+def config_times() -> None:
+    """Times of the specified configurations other than the headline, one JSON line each: the
+    16^3 fcc run (C0, 60 increments) and the 64^3 fcc run (C1, 100 increments) in FP64 and mixed on
+    the GPU, with the oracle on all host cores (C0 whole, C1 its first 3 increments); the adjoint
+    configuration (C3: 32^3, 50 grains, 50 increments, checkpoints every 10) forward and gradient on
+    the GPU, and 5 increments of its forward on the oracle."""
+    from damask_b200 import workloads
+    from damask_b200.adjoint import IncrementSequence, gradient_numerics, gradient_phase, theta_of
+    from damask_b200.grid import SpectralBasic
+    from oracle.oracle import OracleSpectralBasic
+    threads = os.cpu_count() or 1
+
+    def gpu(name, precision):
+        rve, phase, lcs, num = workloads.make(name)
+        s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision=precision)
+        r = _timed_run(s, lcs)
+        s.close()
+        return r
+
+    def cpu(name, n):
+        rve, phase, lcs, num = workloads.make(name)
+        o = OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, threads=threads)
+        r = _timed_run(o, lcs, n)
+        o.close()
+        return dict(r, cores=threads, kind='port')
+
+    for cfg, name, n_cpu in (('C0', 'grid16_fcc_20g', None), ('C1', 'grid64_fcc_200g', 3)):
+        line = {'config': cfg, 'workload': name, 'gpu_fp64': gpu(name, 'fp64'), 'gpu_mixed': gpu(name, 'mixed'),
+                'cpu': cpu(name, n_cpu)}
+        print(json.dumps(line, default=_json_default), flush=True)
+    rve, phase, lcs, num = workloads.make('grid32_fcc_50g')
+    phase, num = gradient_phase(phase), gradient_numerics(num)
+    seq = IncrementSequence(rve, phase, lcs, num, 50, k=10)
+    theta = theta_of(phase)
+    t0 = time.perf_counter()
+    curve = seq.run(theta)
+    t1 = time.perf_counter()
+    seq.gradient(np.ones_like(curve))
+    t2 = time.perf_counter()
+    seq.close()
+    o = OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, threads=threads)
+    c = _timed_run(o, lcs, 5)
+    o.close()
+    print(json.dumps({'config': 'C3', 'workload': 'grid32_fcc_50g, 50 increments, gradient numerics',
+                      'gpu_forward_s': t1 - t0, 'gpu_gradient_s': t2 - t1,
+                      'cpu_forward_5_increments': dict(c, cores=threads, kind='port')}, default=_json_default),
+          flush=True)
+
+
 BATCH_JOBS = 512                         # RVEs of the batched workload definition
 BATCH_RVES, BATCH_INCREMENTS = 128, 10   # the bounded batched sample of the default bench line
 
 
 def batch_sample(n_rves: int, increments: int, local: int = 0) -> dict:
     """The batched workload's first n_rves RVEs (edges 8..32, 5..100 grains, random-axis tension or
-    simple shear), their first `increments` increments, as one batch of the library (FP64): updates/s
-    over the wall time of the run (the host's increment loops included, context set-up not) and over
-    the device time of the batched solutions."""
+    simple shear), their first `increments` increments, as one batch of the library (FP64) driven by
+    its C++ batched increment loop: updates/s over the wall time of the run (the increment loops
+    included, context set-up not)."""
     from damask_b200 import workloads
     from damask_b200.batch import DeviceBatch
     jobs = workloads.batched_jobs(BATCH_JOBS)[:n_rves]
@@ -307,22 +389,23 @@ def batch_sample(n_rves: int, increments: int, local: int = 0) -> dict:
     setup = time.perf_counter() - t0
     clocks = ClockSampler(local)
     clocks.start()
-    seconds = db.run()
+    seconds = db.run_native()
     clk = clocks.stop()
+    if db.failed:
+        raise RuntimeError(f'batched RVEs {db.failed} did not converge')
     st = db.stats()
     updates = sum(db.updates)
     incs = sum(len(r) for r in db.results)
     out = {'workload': f'first {n_rves} RVEs of batched{BATCH_JOBS} (edges {{8,12,16,24,32}}, 5..100 grains, '
                        'random-axis tension or simple shear 1e-3/s), '
                        + (f'increments 1..{increments} of each' if increments < 40 else 'all 40 increments'),
-           'value': updates / seconds, 'unit': 'updates/s', 'device_value': updates / (db.device_ms * 1e-3),
-           'seconds': seconds, 'device_seconds': db.device_ms * 1e-3, 'setup_seconds': setup,
+           'value': updates / seconds, 'unit': 'updates/s', 'seconds': seconds, 'setup_seconds': setup,
            'rves': n_rves, 'voxels': voxels, 'increments': incs, 'updates': updates,
-           'batched_solutions': db.batch_calls, 'graphs': st['graphs'], 'passes': st['passes'],
+           'batched_solutions': st['solutions'], 'graphs': st['graphs'], 'passes': st['passes'],
            'fixed_point_iterations': st['iterations'], 'dtype': 'f64', 'clocks': clk,
-           'how': 'one dmk_batch_solution per round of solution requests: per fixed-point iteration one CUDA '
-                  'graph (constitutive passes of all active RVEs, device-side while loop), one cuFFT plan pair '
-                  'per edge size, batched aim / Gamma / convergence / Anderson kernels'}
+           'how': 'dmk_batch_run: one dmk_batch_solution per round of solution requests; per fixed-point '
+                  'iteration one CUDA graph (constitutive passes of all active RVEs, device-side while loop), '
+                  'one cuFFT plan pair per edge size, batched aim / Gamma / convergence / Anderson kernels'}
     db.close()
     return out
 
@@ -441,11 +524,18 @@ def main():
     ap.add_argument('--batch-engine', choices=['device', 'threads'], default='device',
                     help='--batch: one batch of the library (shared launches) or host threads over contexts')
     ap.add_argument('--no-batched', action='store_true', help='leave out the batched key of the bench line')
+    ap.add_argument('--configs', action='store_true', help='time the other specified configurations and exit')
+    ap.add_argument('--flop-sample', type=int, default=0,
+                    help='print the counters and static FLOP count of this many increments of a 32^3 cut and exit')
     ap.add_argument('--derivative', choices=['continuous', 'central_difference', 'FWBW_difference'],
                     default='continuous', help='solver.grid.FFT.derivative (testing and profiling only)')
     ap.add_argument('--workload', choices=['grid256_bcc24_2000g', 'grid256_bcc48_2000g'], default=WORKLOAD,
                     help='the headline bcc N_sl [12,12] RVE, or the same RVE with all three cI families (48 systems)')
     args = ap.parse_args()
+    if args.flop_sample:
+        return flop_sample(args.flop_sample)
+    if args.configs:
+        return config_times()
     if args.batch:
         return run_batch(args)
     world, rank, local = dist_setup()

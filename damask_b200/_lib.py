@@ -9,7 +9,7 @@ import ctypes as C
 import os
 from pathlib import Path
 
-from .config import (INCREMENT_CB, BCStruct, GridSolverStruct, LoadStepStruct, NumericsStruct, PhaseStruct,
+from .config import (BATCH_INCREMENT_CB, INCREMENT_CB, BCStruct, GridSolverStruct, LoadStepStruct, NumericsStruct, PhaseStruct,
                      RestartStruct, SolutionStruct)
 
 LIB_PATH = Path(__file__).resolve().parent / 'libdamask_b200.so'
@@ -24,7 +24,7 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
            'dmk_grid_run_ctx', 'dmk_fp64_peak', 'dmk_checkpoint_save', 'dmk_checkpoint_restore', 'dmk_adj_begin',
            'dmk_adj_record', 'dmk_adj_step', 'dmk_adj_finish', 'dmk_adj_local_jacobian', 'dmk_batch_create',
-           'dmk_batch_solution', 'dmk_batch_stats', 'dmk_batch_destroy']
+           'dmk_batch_solution', 'dmk_batch_stats', 'dmk_batch_destroy', 'dmk_batch_run']
 
 _lib = None
 
@@ -101,6 +101,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_batch_solution': (C.c_int, [vp, ip, C.c_int, C.POINTER(SolutionStruct)]),
         'dmk_batch_stats': (C.c_int, [vp, dp]),
         'dmk_batch_destroy': (None, [vp]),
+        'dmk_batch_run': (C.c_int, [vp, C.POINTER(C.POINTER(LoadStepStruct)), ip, C.c_int, C.c_int, BATCH_INCREMENT_CB,
+                                    C.c_void_p, ip]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

@@ -23,7 +23,7 @@ import ctypes as C
 import numpy as np
 
 from . import _lib
-from .config import SolutionStruct
+from .config import LoadStepStruct, SolutionStruct
 from .grid import IncrementDriver, SpectralBasic, run_load_cases, run_load_cases_native
 
 
@@ -90,7 +90,8 @@ class DeviceBatch:
                                       precision='fp64', device=device) for rve, phase, _, num in self.jobs]
         self.drivers = [IncrementDriver(s, lcs, N_cutback_max) for s, (_, _, lcs, _) in zip(self.solvers, self.jobs)]
         self.results = [[] for _ in self.jobs]
-        self.updates = [0] * len(self.jobs)
+        self.updates = [0] * len(self.jobs)   # material-point updates of the converged (sub)increments
+        self.failed: list[int] = []
         self.batch_calls = 0
         self.device_ms = 0.0              # device time of the batched solutions (dmk_batch_stats)
         ctxs = (C.c_void_p * len(self.solvers))(*[s.ctx.value for s in self.solvers])
@@ -124,11 +125,12 @@ class DeviceBatch:
         outs = (SolutionStruct * len(waiting))()
         _lib.check(self.lib.dmk_batch_solution(self.handle, which, len(waiting), outs))
         self.device_ms += self.stats()['solution_ms_last']
-        for k in waiting:
+        for j, k in enumerate(waiting):
             s = self.solvers[k]
             c = s.counters()
             s.total_counters += c
-            self.updates[k] += int(c[0])
+            if outs[j].converged:
+                self.updates[k] += int(c[0])
         return [outs[j] for j in range(len(waiting))]
 
     def run(self, solve=None) -> float:
@@ -143,13 +145,46 @@ class DeviceBatch:
             waiting = [k for k, sol in zip(waiting, outs) if self._advance(k, sol)]
         return time.perf_counter() - t0
 
+    def run_native(self, N_cutback_max: int = 3) -> float:
+        """Run every job through the library's C++ batched increment loop (dmk_batch_run): no
+        interpreter between the members' calls; the results and updates as :meth:`run` (the solvers'
+        ``total_counters`` are not kept).  Returns the wall time in seconds.  A job that does not
+        converge after the cutbacks stops; its index goes to ``failed``."""
+        from .config import BATCH_INCREMENT_CB, loadstep_structs
+        from .grid import IncrementStats
+        n = len(self.jobs)
+        steps = [loadstep_structs(lcs) for _, _, lcs, _ in self.jobs]
+        arr = (C.POINTER(LoadStepStruct) * n)(*[C.cast(s, C.POINTER(LoadStepStruct)) for s in steps])
+        counts = (C.c_int * n)(*[len(lcs) for _, _, lcs, _ in self.jobs])
+        status = (C.c_int * n)()
+        clock = [time.perf_counter()]
+
+        def cb(k, info_p, _user):
+            i = info_p.contents
+            now = time.perf_counter()
+            self.results[k].append(IncrementStats(i.inc, i.t, i.cutback_level, bool(i.converged), i.iterations,
+                                                  i.residual_evals, now - clock[0],
+                                                  np.array(i.P_av[:]).reshape(3, 3, order='F')))
+            clock[0] = now
+            self.updates[k] += i.residual_evals * self.solvers[k].N
+            return 0
+
+        cfn = BATCH_INCREMENT_CB(cb)
+        t0 = time.perf_counter()
+        _lib.check(self.lib.dmk_batch_run(self.handle, arr, counts, N_cutback_max, int(self.max_increments or 0), cfn,
+                                          None, status))
+        seconds = time.perf_counter() - t0
+        self.failed = [k for k in range(n) if status[k] != 0]
+        return seconds
+
     def stats(self) -> dict:
         """Device ms of the constitutive graphs and of the whole last batched solution, graphs
-        launched, constitutive passes and fixed-point iterations so far."""
-        out = np.zeros(5)
+        launched, constitutive passes, fixed-point iterations and batched solutions so far, and the
+        host ms of the last solution's set-up, iterations, and tangents with counters."""
+        out = np.zeros(9)
         _lib.check(self.lib.dmk_batch_stats(self.handle, out.ctypes.data_as(C.POINTER(C.c_double))))
         return {'const_ms_last': out[0], 'solution_ms_last': out[1], 'graphs': int(out[2]), 'passes': int(out[3]),
-                'iterations': int(out[4])}
+                'iterations': int(out[4]), 'solutions': int(out[5]), 'host_ms_last': out[6:9].tolist()}
 
     def close(self) -> None:
         if getattr(self, 'handle', None):

@@ -83,6 +83,7 @@ class SolutionStruct(C.Structure):
 
 
 INCREMENT_CB = C.CFUNCTYPE(C.c_int, C.POINTER(IncrementInfoStruct), C.c_void_p)
+BATCH_INCREMENT_CB = C.CFUNCTYPE(C.c_int, C.c_int, C.POINTER(IncrementInfoStruct), C.c_void_p)
 FORWARD_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double,
                          C.POINTER(BCStruct), C.POINTER(BCStruct), C.POINTER(C.c_double))
 SOLUTION_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.POINTER(SolutionStruct))

@@ -8,6 +8,7 @@
 #include <cufft.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -97,6 +98,7 @@ struct dmk_ctx {
   size_t scratch_len = 0;
   TangentOut tan{};
   double* tan_out = nullptr;    // 243 doubles
+  double* tan_host = nullptr;   // pinned: 243 doubles of tan_out, then the 4 counters (as unsigned long long)
   long long* tan_idx = nullptr;
   int tan_blocks = 0;
   void* fft_work = nullptr;
@@ -451,9 +453,12 @@ int masked_compliance(const double* q, const int* mask9 /* column-major, 1 = 'x'
   return 0;
 }
 
-int upload_scalars(dmk_ctx* c, bool reset_iter) {
+// the solver scalars of the host state, in one copy (with the forward's rotated rate and aim, when given)
+int upload_scalars(dmk_ctx* c, bool reset_iter, const double* avRate = nullptr, const double* aim_fwd = nullptr) {
   SolverScalars h;
   std::memset(&h, 0, sizeof h);
+  if (avRate) std::memcpy(h.avRate, avRate, sizeof h.avRate);
+  if (aim_fwd) std::memcpy(h.aim_fwd, aim_fwd, sizeof h.aim_fwd);
   std::memcpy(h.F_aim, c->F_aim, sizeof h.F_aim);
   std::memcpy(h.P_aim, c->P_aim, sizeof h.P_aim);
   std::memcpy(h.P_av, c->P_av, sizeof h.P_av);
@@ -545,9 +550,20 @@ int evaluate_constitutive(dmk_ctx* c, double dt, const double* r, int apply, int
 // dP/dF of every voxel from the stored state: C_volAvg and C_minMaxAvg (grid_utilities.f90:171-202)
 int ensure_scratch(dmk_ctx* c, int K);
 
+// C_volAvg and C_minMaxAvg from the tangent sums copied to tan_host
+void tangent_complete(dmk_ctx* c);
+int tangent_enqueue(dmk_ctx* c, double dt);
+void tangent_complete(dmk_ctx* c) {
+  const double* h = c->tan_host;
+  for (int k = 0; k < 81; ++k) {
+    c->C_volAvg[k] = h[k];
+    c->C_minMaxAvg[k] = 0.5 * (h[81 + k] + h[162 + k]);
+  }
+}
+
 // planes_ready: the dPdF planes and norms of the current state are in place (evaluate_tangent_planes),
 // only their reductions remain
-int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev, bool planes_ready = false) {
+int tangent_launch(dmk_ctx* c, double dt, double* per_voxel_dev, bool planes_ready) {
   Fields f = make_fields(c, nullptr);
   TangentOut o = c->tan;
   o.per_voxel = per_voxel_dev;
@@ -561,13 +577,15 @@ int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev, bool planes_r
   CKL(launch_tangent_finalize(o, c->tan_blocks, c->wgt, c->tan_out, c->tan_idx, 0, c->N, c->stream));
   c->launches += 2;   // reduce, finalize and first-index kernels
   CKL(run_pick(c, f, dt));
-  double h[243];
-  CK(cudaMemcpyAsync(h, c->tan_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+  CK(cudaMemcpyAsync(c->tan_host, c->tan_out, sizeof(double) * 243, cudaMemcpyDeviceToHost, c->stream));
+  return 0;
+}
+// the tangent queued on the context's stream; tangent_complete after the stream has finished
+int tangent_enqueue(dmk_ctx* c, double dt) { return tangent_launch(c, dt, nullptr, false); }
+int evaluate_tangent(dmk_ctx* c, double dt, double* per_voxel_dev, bool planes_ready = false) {
+  if (int rc = tangent_launch(c, dt, per_voxel_dev, planes_ready)) return rc;
   CK(cudaStreamSynchronize(c->stream));
-  for (int k = 0; k < 81; ++k) {
-    c->C_volAvg[k] = h[k];
-    c->C_minMaxAvg[k] = 0.5 * (h[81 + k] + h[162 + k]);
-  }
+  tangent_complete(c);
   return 0;
 }
 
@@ -920,9 +938,11 @@ int solution_prepare(dmk_ctx* c) {
 
 // grid_mechanical_spectral_basic_solution after SNESsolve (grid_mech_spectral_basic.f90:266-277):
 // the solution state, P_aim of the stress-controlled components, and the tangent of the converged
-// state (C_volAvg, C_minMaxAvg for the next increment); counters of the solve
-int solution_finish(dmk_ctx* c, const double F_aim[9], const double P_av[9], int totalIter, double err_div,
-                    double err_BC, int reason, int evals, dmk_solution_state* out) {
+// state (C_volAvg, C_minMaxAvg for the next increment); counters of the solve.  In two halves, so
+// that a batch queues the tangents of all its contexts before it waits for them: the first
+// queues the tangent and the counters' read-back, the second waits for them.
+int solution_finish_begin(dmk_ctx* c, const double F_aim[9], const double P_av[9], int totalIter, double err_div,
+                          double err_BC, int reason, int evals, dmk_solution_state* out) {
   std::memcpy(c->F_aim, F_aim, sizeof c->F_aim);
   std::memcpy(c->P_av, P_av, sizeof c->P_av);
   out->converged = reason > 0;
@@ -936,21 +956,33 @@ int solution_finish(dmk_ctx* c, const double F_aim[9], const double P_av[9], int
     if (c->stress_mask[k]) c->P_aim[k] = c->P_av[k];
   if (out->converged) {
     CK(cudaEventRecord(c->ev[0], c->stream));
-    if (int rc = evaluate_tangent(c, c->dt, nullptr)) return rc;
+    if (int rc = tangent_enqueue(c, c->dt)) return rc;
     CK(cudaEventRecord(c->ev[1], c->stream));
-    CK(cudaEventSynchronize(c->ev[1]));
+  }
+  CK(cudaMemcpyAsync(c->tan_host + 243, c->counters, 4 * sizeof(unsigned long long), cudaMemcpyDeviceToHost,
+                     c->stream));
+  c->last_counters[0] = int64_t(evals) * c->N;
+  c->last_counters[3] = evals;
+  return 0;
+}
+int solution_finish_end(dmk_ctx* c, const dmk_solution_state* out) {
+  CK(cudaStreamSynchronize(c->stream));
+  if (out->converged) {
+    tangent_complete(c);
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
     c->last_ms[2] += ms;
   }
   unsigned long long hc[4];
-  CK(cudaMemcpyAsync(hc, c->counters, sizeof hc, cudaMemcpyDeviceToHost, c->stream));
-  CK(cudaStreamSynchronize(c->stream));
-  c->last_counters[0] = int64_t(evals) * c->N;
+  std::memcpy(hc, c->tan_host + 243, sizeof hc);
   c->last_counters[1] = int64_t(hc[1]);
   c->last_counters[2] = int64_t(hc[2]);
-  c->last_counters[3] = evals;
   return 0;
+}
+int solution_finish(dmk_ctx* c, const double F_aim[9], const double P_av[9], int totalIter, double err_div,
+                    double err_BC, int reason, int evals, dmk_solution_state* out) {
+  if (int rc = solution_finish_begin(c, F_aim, P_av, totalIter, err_div, err_BC, reason, evals, out)) return rc;
+  return solution_finish_end(c, out);
 }
 
 }  // namespace
@@ -1093,6 +1125,10 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     c->hcount = nullptr;
     return bail(fail(DMK_ERR_CUDA, "cudaMallocHost failed"));
   }
+  if (cudaMallocHost(reinterpret_cast<void**>(&c->tan_host), 247 * sizeof(double)) != cudaSuccess) {
+    c->tan_host = nullptr;
+    return bail(fail(DMK_ERR_CUDA, "cudaMallocHost failed"));
+  }
   if (precision == DMK_PRECISION_MIXED)
     if ((rc = dalloc(&c->specf, 2 * 9 * plane)) || (rc = dalloc(&c->Pf, 9 * N))) return bail(rc);
   if (c->solver == 1) {
@@ -1224,12 +1260,8 @@ int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_ol
   for (int k = 0; k < 9; ++k) c->stress_mask[k] = stress->mask[k] ? 1 : 0;
   std::memcpy(c->q_rot, q_rot, sizeof c->q_rot);
   c->dt = dt;
-  int rc = upload_scalars(c, true);
+  int rc = upload_scalars(c, true, avRate, aim);
   if (rc) return rc;
-  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, avRate), avRate, sizeof avRate,
-                     cudaMemcpyHostToDevice, c->stream));
-  CK(cudaMemcpyAsync(reinterpret_cast<char*>(c->sc) + offsetof(SolverScalars, aim_fwd), aim, sizeof aim,
-                     cudaMemcpyHostToDevice, c->stream));
   const double* dsc = reinterpret_cast<const double*>(c->sc);
   CKL(launch_forward(c->Fsol, c->Flast, c->Fdot, c->N, cutBack, guess, dt, dt_old,
                     dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->partials, c->sums, c->wgt,
@@ -1239,7 +1271,6 @@ int dmk_mech_forward(dmk_ctx* c, int cutBack, int guess, double dt, double dt_ol
     CKL(launch_pol_forward_tau(c->Fsol, c->Ftau, c->Ftau_last, c->Ftau_dot, c->N, cutBack, guess, dt, dt_old,
                               dsc + offsetof(SolverScalars, avRate) / sizeof(double), c->polc, c->stream));
   }
-  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -1345,7 +1376,6 @@ int dmk_materialpoint_forward(dmk_ctx* c) {
   CK(cudaMemcpyAsync(c->S0, c->S, b6, cudaMemcpyDeviceToDevice, c->stream));
   CK(cudaMemcpyAsync(c->state0, c->state, bs, cudaMemcpyDeviceToDevice, c->stream));
   c->dot0_valid = false;                                   // new increment-start values
-  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -1452,7 +1482,6 @@ int dmk_mech_update_coords(dmk_ctx* c) {
   CKF(cufftExecZ2D(c->plan_vec_bwd, reinterpret_cast<cufftDoubleComplex*>(c->spec), c->scratch));
   CKL(launch_coords(c->scratch, c->favg, c->cells, step, c->wgt, c->xp, c->xn, c->stream));
   c->launches += 2;   // each launcher above issues two kernels
-  CK(cudaStreamSynchronize(c->stream));
   return 0;
 }
 
@@ -1773,6 +1802,7 @@ void dmk_destroy(dmk_ctx* c) {
     for (int* p : l)
       if (p) cudaFree(p);
   if (c->hcount) cudaFreeHost(c->hcount);
+  if (c->tan_host) cudaFreeHost(c->tan_host);
   for (auto e : c->ev)
     if (e) cudaEventDestroy(e);
   for (auto e : c->tev)
@@ -2213,7 +2243,8 @@ struct dmk_batch {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   double last_ms[2] = {0.0, 0.0};     // constitutive graphs, whole solution (device time)
-  int64_t graph_launches = 0, passes = 0, iterations = 0;
+  int64_t graph_launches = 0, passes = 0, iterations = 0, solutions = 0;
+  double host_ms[3] = {0.0, 0.0, 0.0};  // last solution, host time: set-up, iterations, tangents and counters
 };
 
 namespace {
@@ -2438,8 +2469,13 @@ struct BatchSolve {
   std::vector<int> slots_b;
 };
 
+double ms_since(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t0).count();
+}
+
 int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_state* out) {
   const int n = b->n;
+  auto t0 = std::chrono::steady_clock::now();
   std::vector<BatchSolve> st(n);
   std::vector<int> pos(n, -1);
   for (int k = 0; k < nw; ++k) {
@@ -2464,6 +2500,8 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
     CK(cudaStreamWaitEvent(b->stream, c->fork, 0));
   }
   CK(cudaEventRecord(b->ev[0], b->stream));
+  b->host_ms[0] = ms_since(t0);
+  t0 = std::chrono::steady_clock::now();
   Fields* hf = reinterpret_cast<Fields*>(b->h_tab + b->o_f);
   PassWork* hw = reinterpret_cast<PassWork*>(b->h_tab + b->o_w);
   double* hdt = reinterpret_cast<double*>(b->h_tab + b->o_dt);
@@ -2600,16 +2638,22 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
   b->last_ms[1] = ms;
-  // the contexts' own streams continue after the batch (tangent, forward of the next increment)
+  b->host_ms[1] = ms_since(t0);
+  t0 = std::chrono::steady_clock::now();
+  // the contexts' own streams continue after the batch (tangent, forward of the next increment);
+  // all tangents are queued before the first wait
   for (int k = 0; k < nw; ++k) {
     const int r = which[k];
     dmk_ctx* c = b->ctx[r];
     CK(cudaStreamWaitEvent(c->stream, b->ev[1], 0));
     const BatchScal& hs = b->h_scal[r];
-    if (int rc = solution_finish(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, st[r].reason,
-                                 st[r].evals, &out[k]))
+    if (int rc = solution_finish_begin(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, st[r].reason,
+                                       st[r].evals, &out[k]))
       return rc;
   }
+  for (int k = 0; k < nw; ++k)
+    if (int rc = solution_finish_end(b->ctx[which[k]], &out[k])) return rc;
+  b->host_ms[2] = ms_since(t0);
   return 0;
 }
 
@@ -2654,19 +2698,27 @@ int dmk_batch_solution(dmk_batch* b, const int* which, int n_which, dmk_solution
   if (!b || (n_which > 0 && (!which || !out))) return fail(DMK_ERR_ARG, "null argument");
   if (n_which < 0 || n_which > b->n) return fail(DMK_ERR_ARG, "n_which out of range");
   CK(cudaSetDevice(b->device));
+  ++b->solutions;
   return batch_solution_impl(b, which, n_which, out);
 }
 
-int dmk_batch_stats(dmk_batch* b, double out[5]) {
+int dmk_batch_stats(dmk_batch* b, double out[9]) {
   if (!b || !out) return fail(DMK_ERR_ARG, "null argument");
   out[0] = b->last_ms[0];
   out[1] = b->last_ms[1];
   out[2] = double(b->graph_launches);
   out[3] = double(b->passes);
   out[4] = double(b->iterations);
+  out[5] = double(b->solutions);
+  for (int k = 0; k < 3; ++k) out[6 + k] = b->host_ms[k];
   return 0;
 }
 
 void dmk_batch_destroy(dmk_batch* b) { batch_free(b); }
 
 }  // extern "C"
+
+namespace dmk {
+int batch_size(const dmk_batch* b) { return b ? b->n : 0; }
+dmk_ctx* batch_member(dmk_batch* b, int k) { return (b && k >= 0 && k < b->n) ? b->ctx[k] : nullptr; }
+}  // namespace dmk

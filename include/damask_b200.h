@@ -380,9 +380,22 @@ typedef struct dmk_batch dmk_batch;
 int dmk_batch_create(dmk_batch** out, dmk_ctx* const* ctxs, int n);
 int dmk_batch_solution(dmk_batch* batch, const int* which, int n_which, dmk_solution_state* out);
 /* out: device ms of the constitutive graphs and of the whole last dmk_batch_solution, graphs
-   launched, constitutive passes and fixed-point iterations of the batch so far */
-int dmk_batch_stats(dmk_batch* batch, double out[5]);
+   launched, constitutive passes, fixed-point iterations and dmk_batch_solution calls so far, and the
+   host ms of the last call's set-up, iterations, and tangents with counters */
+int dmk_batch_stats(dmk_batch* batch, double out[9]);
 void dmk_batch_destroy(dmk_batch* batch);
+/* The increment loops of all members of a batch, each as dmk_grid_run_ctx (no restart skipping),
+   with their solutions computed together: every round, each unfinished member runs up to its next
+   solution request (dmk_mech_forward, dmk_materialpoint_forward), one dmk_batch_solution solves
+   all requests, and each member goes on (dmk_mech_update_coords, cb, cutback).  Members may fall
+   out of step.  steps[k], n_steps[k]: the load steps of member k; max_increments <= 0: all.
+   cb(member, info, user) after every converged (sub)increment of a member (nonzero stops that
+   member).  status[k]: 0, or DMK_ERR_NOT_CONVERGED when member k did not converge after
+   N_cutback_max cutbacks (IO_error 950; it stops, the others go on).  Returns 0, or the first
+   error of the library, which stops all members. */
+typedef int (*dmk_batch_increment_cb)(int member, const dmk_increment_info* info, void* user);
+int dmk_batch_run(dmk_batch* batch, const dmk_loadstep* const* steps, const int* n_steps, int N_cutback_max,
+                  int max_increments, dmk_batch_increment_cb cb, void* user, int* status);
 
 /* Volume average <f> of a 9-component field that the caller already holds in device
    memory (9 planes of n_voxels doubles: component c of voxel v at field[c*n_voxels + v]),

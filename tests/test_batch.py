@@ -99,3 +99,26 @@ def test_device_batch_equals_standalone_runs(gpu):
     db.close()
     print('field differences batch vs standalone:', errs)
     assert max(max(e.values()) for e in errs.values()) < 1e-10, errs
+
+
+@pytest.mark.gpu
+def test_device_batch_native_loop_equals_python_loop(gpu):
+    """The library's batched increment loop (dmk_batch_run) takes the steps of the Python loop over
+    the same batch: the same converged increments, iteration counts and results, bit for bit."""
+    from damask_b200.batch import DeviceBatch
+    jobs = workloads.batched_jobs(5, seed=3)
+    a = DeviceBatch(jobs, max_increments=3)
+    a.run()
+    b = DeviceBatch(jobs, max_increments=3)
+    b.run_native()
+    assert not b.failed
+    for k in range(len(jobs)):
+        key = lambda r: (r.inc, r.t, r.cutback_level, r.iterations, r.residual_evals)
+        assert [key(r) for r in a.results[k]] == [key(r) for r in b.results[k]]
+        for x, y in zip(a.results[k], b.results[k]):
+            assert np.array_equal(x.P_av, y.P_av)
+        assert np.array_equal(a.solvers[k].get_field('P'), b.solvers[k].get_field('P'))
+        assert np.array_equal(a.solvers[k].get_coords()[1], b.solvers[k].get_coords()[1])
+    assert a.updates == b.updates
+    a.close()
+    b.close()
