@@ -303,7 +303,8 @@ def flop_sample(increments: int) -> None:
     c = s.total_counters
     print(json.dumps({'workload': f'{WORKLOAD} 32^3 cut', 'increments': increments, 'updates': int(c[0]),
                       'state_iterations': int(c[1]), 'newton_iterations': int(c[2]), 'residual_evals': int(c[3]),
-                      'static_fp64_flop': constitutive_flops(phase.n_slip, c[2], c[1], c[0])}), flush=True)
+                      'static_fp64_flop': float(constitutive_flops(phase.n_slip, c[2], c[1], c[0]))},
+                     default=_json_default), flush=True)
     s.close()
 
 
@@ -325,9 +326,10 @@ def _timed_run(solver, lcs, n=None) -> dict:
 def config_times() -> None:
     """Times of the specified configurations other than the headline, one JSON line each: the
     16^3 fcc run (C0, 60 increments) and the 64^3 fcc run (C1, 100 increments) in FP64 and mixed on
-    the GPU, with the oracle on all host cores (C0 whole, C1 its first 3 increments); the adjoint
-    configuration (C3: 32^3, 50 grains, 50 increments, checkpoints every 10) forward and gradient on
-    the GPU, and 5 increments of its forward on the oracle."""
+    the GPU, with the oracle on all host cores (C0 whole, C1 its first 3 increments); the batched
+    workload's first 16 RVEs on the oracle (C2; the GPU figure is the bench line's `batched` key and
+    `--batch 512`); the adjoint configuration (C3: 32^3, 50 grains, 50 increments, checkpoints every
+    10) forward and gradient on the GPU, and 5 increments of its forward on the oracle."""
     from damask_b200 import workloads
     from damask_b200.adjoint import IncrementSequence, gradient_numerics, gradient_phase, theta_of
     from damask_b200.grid import SpectralBasic
@@ -352,6 +354,17 @@ def config_times() -> None:
         line = {'config': cfg, 'workload': name, 'gpu_fp64': gpu(name, 'fp64'), 'gpu_mixed': gpu(name, 'mixed'),
                 'cpu': cpu(name, n_cpu)}
         print(json.dumps(line, default=_json_default), flush=True)
+    # C2 on the oracle: the first 16 RVEs of the batched workload one after the other, 5 increments each
+    upd, wall = 0, 0.0
+    for rve, phase, lcs, num in workloads.batched_jobs(BATCH_JOBS)[:16]:
+        o = OracleSpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, threads=threads)
+        r = _timed_run(o, lcs, 5)
+        o.close()
+        upd += r['updates']
+        wall += r['wall_s']
+    print(json.dumps({'config': 'C2', 'workload': 'first 16 RVEs of batched512, increments 1..5 of each, in sequence',
+                      'cpu': {'updates': upd, 'wall_s': wall, 'updates_per_s': upd / wall, 'cores': threads,
+                              'kind': 'port'}}, default=_json_default), flush=True)
     rve, phase, lcs, num = workloads.make('grid32_fcc_50g')
     phase, num = gradient_phase(phase), gradient_numerics(num)
     seq = IncrementSequence(rve, phase, lcs, num, 50, k=10)
