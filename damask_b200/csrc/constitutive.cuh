@@ -109,18 +109,19 @@ __device__ __forceinline__ bool qr_solve(double* A, double* b) {
 // F and Fp0 point at voxel v's planes (stride N); they are read at the start and again
 // for the final Fp / P so that no copy stays in registers through the Newton loop.
 // xs: this thread's shared-memory slots (stride pass_threads<NS>()): 1/xi (NS entries), the
-// Newton weights dt*dgamma (NS), |dot_gamma| of the last residual evaluation (NS), then
-// A, the last accepted Lp guess and the Newton step (9 each).  Lp (in/out) is the warm
-// start and, on success, the result; S, Fp, P and Fe are written only on success.
+// Newton weights dt*dgamma (NS), then A (9).  The voxel's planes (stride N) receive |dot_gamma|
+// of the last residual evaluation (adg_g; the state update after a converged integration reads
+// it), the last accepted Lp guess (lo_g) and the Newton step (dl_g): they are written once per
+// Newton iteration and read back rarely (line search, step), so they stay out of the shared
+// memory that bounds the kernel's occupancy.  Lp (in/out) is the warm start and, on success,
+// the result; S, Fp, P and Fe are written only on success.
 template <int NS>
 __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __restrict__ sc, const Numerics& nm,
                                 const double* Fg, const double* Fp0g, int64_t N, double* xs, double dt, double* Lp,
-                                double* S, double* Fp, double* Pout, double* Feout, int& newton) {
+                                double* S, double* Fp, double* Pout, double* Feout, int& newton,
+                                double* __restrict__ adg_g, double* __restrict__ lo_g, double* __restrict__ dl_g) {
   double* const sw = xs + NS * pass_threads<NS>();
-  double* const sg = xs + 2 * NS * pass_threads<NS>();
-  double* const sA = xs + 3 * NS * pass_threads<NS>();
-  double* const sLo = sA + 9 * pass_threads<NS>();
-  double* const sdL = sLo + 9 * pass_threads<NS>();
+  double* const sA = xs + 2 * NS * pass_threads<NS>();
   {
     double F[9], Fp0[9], invFp0[9], A[9];
 #pragma unroll
@@ -133,7 +134,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
 
   double Lg[9], B[9], s6[6];
 #pragma unroll
-  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; sLo[k * pass_threads<NS>()] = Lp[k]; sdL[k * pass_threads<NS>()] = 0.0; }
+  for (int k = 0; k < 9; ++k) { Lg[k] = Lp[k]; lo_g[k * N] = Lp[k]; dl_g[k * N] = 0.0; }
   double step = 1.0, res_old = 1.7976931348623157e308;
   int jaco = 0;
   for (int it = 1;; ++it) {
@@ -181,7 +182,7 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
       // P_nS sense of the derivative follows the sign of dot_gamma (phenopowerlaw.f90:327)
       if (!(g > 0.0)) neg |= SenseMask<NS>(1) << s;
       sw[s * pass_threads<NS>()] = dt * dg;
-      sg[s * pass_threads<NS>()] = fabs(g);
+      adg_g[s * N] = fabs(g);
       double2 P[5];
 #pragma unroll
       for (int k = 0; k < 5; ++k) P[k] = c.P[k];
@@ -199,12 +200,12 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
     if (nR < res_old) {
       res_old = nR;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) sLo[k * pass_threads<NS>()] = Lg[k];
+      for (int k = 0; k < 9; ++k) lo_g[k * N] = Lg[k];
       step = 1.0;
     } else {
       step = nm.r_linesearch_Lp * step;
 #pragma unroll
-      for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * pass_threads<NS>()], step, sLo[k * pass_threads<NS>()]);
+      for (int k = 0; k < 9; ++k) Lg[k] = fma(dl_g[k * N], step, lo_g[k * N]);
       continue;
     }
     if (jaco % nm.f_update_jacobi_Lp == 0) {
@@ -281,10 +282,10 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
         for (int k = 0; k < 9; ++k) X[k] = fma(cq, Ps[k], X[k]);
       }
 #pragma unroll
-      for (int k = 0; k < 9; ++k) sdL[k * pass_threads<NS>()] = X[k];
+      for (int k = 0; k < 9; ++k) dl_g[k * N] = X[k];
     }
 #pragma unroll
-    for (int k = 0; k < 9; ++k) Lg[k] = fma(sdL[k * pass_threads<NS>()], step, Lg[k]);
+    for (int k = 0; k < 9; ++k) Lg[k] = fma(dl_g[k * N], step, Lg[k]);
   }
   // Fp = (Fp0^-1 B)^-1 / det^(1/3); P = F Fp^-1 S Fp^-T; Fe = F Fp^-1  (:571-581)
   double F[9], invFpn[9], Fpn[9];
@@ -320,7 +321,7 @@ __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double
 // Slots of the stress kernel (stride pass_threads<NS>()): 1/xi [0, NS), Newton weights
 // [NS, 2NS), |dot_gamma| [2NS, 3NS), Newton 3x3 scratch [3NS, 3NS + 27).
 template <int NS>
-__host__ __device__ constexpr int stress_slots() { return 3 * NS + 27; }
+__host__ __device__ constexpr int stress_slots() { return 2 * NS + 9; }
 
 // phenopowerlaw_dotState (Fi = I => Mp = S; no twins => sumF = 0) at the stored
 // stress and state of voxel v, written to this thread's slots: xi rates first, then

@@ -199,12 +199,14 @@ PassWork pass_work(dmk_ctx* c, int half, int out) {
   w.adg = w.D + 2 * NST * N;
   w.dot0 = c->dot0;
   w.sub = w.adg + int64_t(c->NS) * N;
+  w.lo = w.sub + 2 * N;
+  w.dl = w.lo + 9 * N;
   w.ctl = c->pctl;
   w.list_out = c->plist[half][out];
   w.count_out = c->pcount + 2 * half + out;
   return w;
 }
-size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 7 * NS + 2); }
+size_t pass_work_doubles(int64_t N, int NS) { return size_t(N) * size_t(36 + 7 * NS + 2 + 18); }
 
 template <int NS>
 int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, double dt, int apply) {

@@ -87,6 +87,8 @@ struct PassWork {
   double* adg;     // NS: |dot_gamma| at the stress of the last converged integrateStress
   double* dot0;    // 2 NS: dotState at the increment-start stress and state (S0, state0)
   double* sub;     // 2: stepFrac (subFrac), step (subStep)
+  double* lo;      // 9: the last accepted Lp guess of the current integrateStress
+  double* dl;      // 9: its Newton step
   int* ctl;        // 6: phase, status, state iteration, substeps, state iterations total, Newton total
   int* list_out;   // voxels that continue into the next pass
   int* count_out;  // number of entries appended to list_out
