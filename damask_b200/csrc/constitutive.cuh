@@ -346,9 +346,12 @@ __device__ bool dot_state_slots(const PhaseConst<NS>& pc, const double* __restri
     }
   }
   bool bad = false;
+  // xi of every system into the slots first, so that the loads overlap
+#pragma unroll 8
+  for (int l = 0; l < NS; ++l) xs[l * pass_threads<NS>()] = state[l * N + v];
 #pragma unroll 2
   for (int l = 0; l < NS; ++l) {
-    const double x = fma(-state[l * N + v], pc.ixiinf[l], 1.0);  // 1 - xi/xi_inf
+    const double x = fma(-xs[l * pass_threads<NS>()], pc.ixiinf[l], 1.0);  // 1 - xi/xi_inf
     const double left = copysign(powr(fabs(x), pc.a[l], pc.a_int[l]), x);
     const double2* hrow = reinterpret_cast<const double2*>(hs + l * NS);
     double hg = 0.0;
