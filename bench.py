@@ -45,10 +45,11 @@ def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> 
     return newton * (264 + 56 * ns) + steps * (567 + 135 * ns) + state * (455 + 86 * ns) + updates * (89 * ns)
 
 
-# DRAM bytes that the constitutive kernels move per material-point update, by slip-system count,
-# from the ncu capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (64^3 cut of
-# the workload; the traffic grows with the number of voxels)
-TRAFFIC_BYTES_PER_UPDATE = {24: 9428}
+# DRAM bytes that one stress and one control launch move per voxel of a full pass, by slip-system
+# count, from the ncu capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (two
+# passes of a 65 536-voxel chunk: stress 568 B, control 2 114 B); a material-point update runs one
+# such pass per state iteration
+TRAFFIC_BYTES_PER_PASS = {24: 2682}
 
 # the 48-system RVE's window inside the default bench line (5.7 s per increment at 256^3)
 BCC48_WARMUP, BCC48_STEPS = 3, 3
@@ -488,7 +489,8 @@ def measure(workload, steps, warmup, world, rank, local, cells, solver, derivati
     achieved_gbs = bpu * mx['N'] / (avg_launch_ms * 1e-3) / 1e9
     flops = constitutive_flops(ns, mx['newton'], mx['state'], mx['updates'])
     fp64_tflops = flops / (mx['const_ms'] * 1e-3) / 1e12
-    traffic = TRAFFIC_BYTES_PER_UPDATE.get(ns)
+    per_pass = TRAFFIC_BYTES_PER_PASS.get(ns)
+    traffic = per_pass * mx['state'] / max(1, mx['updates']) if per_pass else None
     roofline = {
         'bound': 'fp64',
         'kernel': 'constitutive update (begin + stress/control pass kernels), one evaluation of all voxels',
@@ -497,7 +499,9 @@ def measure(workload, steps, warmup, world, rank, local, cells, solver, derivati
         'flops_per_update': flops / max(1, mx['updates']),
         'flop_source': 'static FP64 count of the kernels times the counted Newton / state iterations',
         'traffic': traffic * mx['N'] if traffic else None,
-        'traffic_source': f'ncu DRAM bytes per update at 64^3 ({ns} systems), times the voxels of one evaluation',
+        'traffic_source': f'ncu DRAM bytes of a stress and a control launch per voxel and pass at 64^3 ({ns} systems), '
+                          'times the passes (state iterations) per update and the voxels of one evaluation; '
+                          'the begin kernel is not included',
         'avg_launch_ms': avg_launch_ms,
         'hbm': {'achieved': achieved_gbs, 'peak': peaks['hbm_gbs'], 'unit': 'GB/s', 'frac': achieved_gbs / peaks['hbm_gbs'],
                 'peak_source': peaks['source'], 'bytes_per_update': bpu},

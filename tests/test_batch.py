@@ -122,3 +122,28 @@ def test_device_batch_native_loop_equals_python_loop(gpu):
     assert a.updates == b.updates
     a.close()
     b.close()
+
+
+@pytest.mark.gpu
+def test_device_batch_cutbacks_match_standalone(gpu):
+    """A member whose fixed point is capped at 8 iterations (-snes_max_it 8) fails increments and
+    cuts back while the others go on: both batched loops (Python and dmk_batch_run) reproduce its
+    standalone sequence of (sub)increments, time steps and cutback levels, and every member's
+    results."""
+    from damask_b200.batch import DeviceBatch
+    jobs = workloads.batched_jobs(4, seed=7)
+    jobs[1][3].PETSc_options = '-snes_max_it 8'
+    n = 4
+    refs = [_standalone(job, n) for job in jobs]
+    assert any(r.cutback_level > 0 for r in refs[1][1]), 'the capped member must cut back'
+    for native in (False, True):
+        db = DeviceBatch(jobs, max_increments=n)
+        db.run_native() if native else db.run()
+        for k, (s, ref) in enumerate(refs):
+            key = lambda r: (r.inc, round(r.t, 12), r.cutback_level, r.iterations, r.residual_evals)
+            assert [key(r) for r in db.results[k]] == [key(r) for r in ref], (native, k)
+            for a, b in zip(db.results[k], ref):
+                assert rel(a.P_av, b.P_av) < 1e-12, (native, k, a.inc)
+        db.close()
+    for s, _ in refs:
+        s.close()
