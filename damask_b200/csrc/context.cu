@@ -1146,8 +1146,9 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     return bail(rc);
   if (num->snes_type == 1) {
     c->aa_m = std::max(1, std::min(num->anderson_m, AA_MAX));
-    // grid-stride blocks of the Anderson kernels: 8 per SM, fewer when the field is smaller
-    c->aa_blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(c->nsm) * 8, (nvec + 255) / 256)));
+    // grid-stride blocks of the Anderson kernels: 8 per SM, fewer for smaller fields (at least 8
+    // elements per thread, so that a batch of small RVEs launches few idle blocks)
+    c->aa_blocks = int(std::max<int64_t>(1, std::min<int64_t>(int64_t(c->nsm) * 8, (nvec + 2047) / 2048)));
     if ((rc = dalloc(&c->aa_dX, size_t(c->aa_m) * nvec)) || (rc = dalloc(&c->aa_dR, size_t(c->aa_m) * nvec)) ||
         (rc = dalloc(&c->aa_Rprev, nvec)) || (rc = dalloc(&c->aa_partials, size_t(c->aa_blocks) * 2 * AA_CHUNK_HOST)) ||
         (rc = dalloc(&c->aa_out, 4 * AA_MAX)))
