@@ -16,9 +16,10 @@ HERE = Path(__file__).resolve().parent
 CSRC = HERE / 'csrc'
 LIB = HERE / 'libdamask_b200.so'
 SOURCES = ['kernels.cu', 'constitutive.cu', 'dpdf.cu', 'polarization.cu', 'adjoint.cu', 'context.cu', 'noalloc.cu',
-           'lattice.cpp',
+           'host_parallel.cu', 'lattice.cpp',
            'vti.cpp', 'driver.cpp']
-HEADERS = ['dmk_device.cuh', 'constitutive.cuh', 'kernels.cuh', 'adjoint.cuh', 'lattice.h', 'lattice_tables.h']
+HEADERS = ['dmk_device.cuh', 'constitutive.cuh', 'kernels.cuh', 'adjoint.cuh', 'lattice.h', 'lattice_tables.h',
+           'host_parallel.h']
 ARCH = ['-gencode', 'arch=compute_100a,code=sm_100a']
 
 

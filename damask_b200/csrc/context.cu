@@ -3,6 +3,7 @@
 #include "../../include/damask_b200.h"
 #include "kernels.cuh"
 #include "adjoint.cuh"
+#include "host_parallel.h"
 #include "lattice.h"
 
 #include <cufft.h>
@@ -2248,6 +2249,7 @@ struct dmk_batch {
   double last_ms[2] = {0.0, 0.0};     // constitutive graphs, whole solution (device time)
   int64_t graph_launches = 0, passes = 0, iterations = 0, solutions = 0;
   double host_ms[3] = {0.0, 0.0, 0.0};  // last solution, host time: set-up, iterations, tangents and counters
+  std::unique_ptr<HostPool> pool;        // host threads for the per-member calls
 };
 
 namespace {
@@ -2275,6 +2277,7 @@ void batch_free(dmk_batch* b) {
   for (auto e : b->ev)
     if (e) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
+  b->pool.reset();
   delete b;
 }
 
@@ -2488,7 +2491,8 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
     pos[r] = k;
   }
   b->last_ms[0] = b->last_ms[1] = 0.0;
-  for (int k = 0; k < nw; ++k) {
+  std::string msg;
+  int rc0 = b->pool->run(nw, [&](int k) -> int {
     const int r = which[k];
     dmk_ctx* c = b->ctx[r];
     if (int rc = solution_prepare(c)) return rc;
@@ -2501,7 +2505,9 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
     // the batch's launches follow the context's queued work (forward, solver scalars)
     CK(cudaEventRecord(c->fork, c->stream));
     CK(cudaStreamWaitEvent(b->stream, c->fork, 0));
-  }
+    return 0;
+  }, &msg);
+  if (rc0) return fail(rc0, msg);
   CK(cudaEventRecord(b->ev[0], b->stream));
   b->host_ms[0] = ms_since(t0);
   t0 = std::chrono::steady_clock::now();
@@ -2645,17 +2651,17 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
   t0 = std::chrono::steady_clock::now();
   // the contexts' own streams continue after the batch (tangent, forward of the next increment);
   // all tangents are queued before the first wait
-  for (int k = 0; k < nw; ++k) {
+  rc0 = b->pool->run(nw, [&](int k) -> int {
     const int r = which[k];
     dmk_ctx* c = b->ctx[r];
     CK(cudaStreamWaitEvent(c->stream, b->ev[1], 0));
     const BatchScal& hs = b->h_scal[r];
-    if (int rc = solution_finish_begin(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, st[r].reason,
-                                       st[r].evals, &out[k]))
-      return rc;
-  }
-  for (int k = 0; k < nw; ++k)
-    if (int rc = solution_finish_end(b->ctx[which[k]], &out[k])) return rc;
+    return solution_finish_begin(c, hs.F_aim, hs.P_av, hs.totalIter, hs.err_div, hs.err_BC, st[r].reason,
+                                 st[r].evals, &out[k]);
+  }, &msg);
+  if (rc0) return fail(rc0, msg);
+  rc0 = b->pool->run(nw, [&](int k) -> int { return solution_finish_end(b->ctx[which[k]], &out[k]); }, &msg);
+  if (rc0) return fail(rc0, msg);
   b->host_ms[2] = ms_since(t0);
   return 0;
 }
@@ -2684,6 +2690,12 @@ int dmk_batch_create(dmk_batch** out, dmk_ctx* const* ctxs, int n) {
   b->NS = ctxs[0]->NS;
   b->device = ctxs[0]->device;
   b->nsm = ctxs[0]->nsm;
+  {
+    // host threads for the per-member calls: one per 32 members, at most 7 besides the caller
+    const int hw = int(std::thread::hardware_concurrency());
+    const int workers = std::max(0, std::min({n / 32, 7, hw > 1 ? hw - 1 : 0}));
+    b->pool = std::make_unique<HostPool>(workers, b->device);
+  }
   if (cudaSetDevice(b->device) != cudaSuccess) {
     batch_free(b);
     return fail(DMK_ERR_CUDA, "cudaSetDevice failed");
@@ -2722,6 +2734,7 @@ void dmk_batch_destroy(dmk_batch* b) { batch_free(b); }
 }  // extern "C"
 
 namespace dmk {
+HostPool* batch_pool(dmk_batch* b) { return b ? b->pool.get() : nullptr; }
 int batch_size(const dmk_batch* b) { return b ? b->n : 0; }
 dmk_ctx* batch_member(dmk_batch* b, int k) { return (b && k >= 0 && k < b->n) ? b->ctx[k] : nullptr; }
 }  // namespace dmk

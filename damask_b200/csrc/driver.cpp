@@ -8,11 +8,13 @@
 #include <vector>
 
 #include "../../include/damask_b200.h"
+#include "host_parallel.h"
 
 namespace dmk {
 int record_error(int code, const std::string& msg);
 int batch_size(const dmk_batch* b);
 dmk_ctx* batch_member(dmk_batch* b, int k);
+HostPool* batch_pool(dmk_batch* b);
 }
 
 namespace {
@@ -105,24 +107,40 @@ int dmk_batch_run(dmk_batch* batch, const dmk_loadstep* const* steps, const int*
     m[k].steps = steps[k];
     m[k].n_steps = n_steps[k];
   }
-  std::vector<int> waiting, next;
-  for (int k = 0; k < n; ++k) {
-    const int rc = advance(m[k], dmk::batch_member(batch, k), max_increments);
-    if (rc < 0) return rc;
-    if (rc == 1) waiting.push_back(k);
-  }
+  // the members' own calls (forward, materialpoint_forward, coordinates) run on the batch's host
+  // threads; the callbacks run on this thread, in member order
+  dmk::HostPool* pool = dmk::batch_pool(batch);
+  std::string msg;
+  std::vector<int> waiting, next, state(n, 0);   // state: the result of advance (1: waiting)
+  auto advance_all = [&](const std::vector<int>& members) -> int {
+    return pool->run(int(members.size()), [&](int j) -> int {
+      const int k = members[j];
+      const int rc = advance(m[k], dmk::batch_member(batch, k), max_increments);
+      state[k] = rc;
+      return rc < 0 ? rc : 0;
+    }, &msg);
+  };
+  std::vector<int> all(n);
+  for (int k = 0; k < n; ++k) all[k] = k;
+  if (int rc = advance_all(all)) return dmk::record_error(rc, msg);
+  for (int k = 0; k < n; ++k)
+    if (state[k] == 1) waiting.push_back(k);
   std::vector<dmk_solution_state> sol;
   while (!waiting.empty()) {
     sol.assign(waiting.size(), dmk_solution_state{});
     if (int rc = dmk_batch_solution(batch, waiting.data(), int(waiting.size()), sol.data())) return rc;
+    // coordinates of the converged members
+    int rc = pool->run(int(waiting.size()), [&](int j) -> int {
+      return (sol[j].converged && sol[j].stagConverged) ? dmk_mech_update_coords(dmk::batch_member(batch, waiting[j]))
+                                                        : 0;
+    }, &msg);
+    if (rc) return dmk::record_error(rc, msg);
     next.clear();
     for (size_t j = 0; j < waiting.size(); ++j) {
       const int k = waiting[j];
       Member& s = m[k];
-      dmk_ctx* c = dmk::batch_member(batch, k);
       const dmk_solution_state& o = sol[j];
       if (o.converged && o.stagConverged) {
-        if (int rc = dmk_mech_update_coords(c)) return rc;
         s.Delta_t_prev = s.Delta_t;
         s.cutBack = false;
         s.guess = true;
@@ -141,10 +159,10 @@ int dmk_batch_run(dmk_batch* batch, const dmk_loadstep* const* steps, const int*
         status[k] = DMK_ERR_NOT_CONVERGED;
         s.done = true;
       }
-      const int rc = advance(s, c, max_increments);
-      if (rc < 0) return rc;
-      if (rc == 1) next.push_back(k);
     }
+    if ((rc = advance_all(waiting))) return dmk::record_error(rc, msg);
+    for (int k : waiting)
+      if (state[k] == 1) next.push_back(k);
     waiting.swap(next);
   }
   return 0;
