@@ -211,7 +211,24 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
         p_av.extend(r.P_av for r in recs)
         return recs, c, tm
 
-    for _ in range(warmup):
+    for _ in range(warmup - 1):
+        one_step()
+    # the last warm-up increment: the autotuner picks the stress-kernel variant and the voxel-chunk
+    # count between its forward and its solution (results unchanged; basic scheme only)
+    tuning = None
+    if solver_name == 'spectral_basic':
+        gen = drv.step_requests()
+        try:
+            gen.send(None)
+            try:
+                tuning = solver.autotune(reps=2)
+            except Exception as e:                   # not enough free memory for the state copy
+                tuning = {'skipped': str(e)}
+            while True:
+                gen.send(solver.solution())
+        except StopIteration as stop:
+            p_av.extend(r.P_av for r in stop.value)
+    else:
         one_step()
     # timed region: inputs resident in HBM, device time on the solver's stream.  Each step is
     # timed twice from the same increment: the increment itself (value) and, end to end through
@@ -244,7 +261,8 @@ def run_gpu(precision: str, steps: int, warmup: int, world: int, rank: int, loca
     upd_e2e = upd
     out = {'updates': upd, 'ms': ms, 'newton': newton, 'state': state, 'evals': evals, 'const_ms': const_ms,
            'launches': launches, 'clocks': clk, 'updates_e2e': upd_e2e, 'ms_e2e': ms_e2e, 'N': solver.N,
-           'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8, 'device_gb': device_gb}
+           'ns': phase.n_slip, 'p_av': p_av, 'd2h_bytes': solver.N * 9 * 8, 'device_gb': device_gb,
+           'tuning': tuning}
     solver.close()
     return out
 
@@ -611,7 +629,9 @@ def main():
                    'precision': 'mixed',
                    'parallelism': f'replicas x{world}',
                    'l2': f'inputs larger than L2 (device memory of the context {mx["device_gb"]:.1f} GB)',
-                   'increments_timed': f'{warmup + 1}..{warmup + args.steps}'},
+                   'increments_timed': f'{warmup + 1}..{warmup + args.steps}',
+                   'tuning': {p: headline[k]['tuning'] for p, k in (('mixed', 'mixed'), ('fp64', 'fp64_raw'))
+                              if headline.get(k)}},
         'fp64': headline['fp64'],
         's_per_increment': headline['s_per_increment'],
         'mixed_over_fp64': headline['mixed_over_fp64'],
@@ -629,7 +649,7 @@ def main():
                          'mixed_over_fp64': b48['mixed_over_fp64'], 'P_av_rel_err': b48['P_av_rel_err'],
                          'increments_timed': f'{BCC48_WARMUP + 1}..{BCC48_WARMUP + BCC48_STEPS}',
                          's_per_increment': b48['s_per_increment'], 'roofline_fp64': b48['roofline']['fp64'],
-                         'clocks': b48['mixed']['clocks']}
+                         'clocks': b48['mixed']['clocks'], 'tuning': b48['mixed'].get('tuning')}
     if batched is not None:
         line['batched'] = batched
     print(json.dumps(line, default=_json_default), flush=True)

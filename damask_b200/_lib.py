@@ -24,7 +24,8 @@ EXPORTS = ['dmk_mech_init', 'dmk_mech_forward', 'dmk_mech_solution', 'dmk_materi
            'dmk_vti_label', 'dmk_vti_read_int', 'dmk_vti_read_real', 'dmk_vti_close', 'dmk_grid_run',
            'dmk_grid_run_ctx', 'dmk_fp64_peak', 'dmk_checkpoint_save', 'dmk_checkpoint_restore', 'dmk_adj_begin',
            'dmk_adj_record', 'dmk_adj_step', 'dmk_adj_finish', 'dmk_adj_local_jacobian', 'dmk_batch_create',
-           'dmk_batch_solution', 'dmk_batch_stats', 'dmk_batch_destroy', 'dmk_batch_run']
+           'dmk_batch_solution', 'dmk_batch_stats', 'dmk_batch_destroy', 'dmk_batch_run', 'dmk_autotune',
+           'dmk_get_tuning', 'dmk_set_tuning']
 
 _lib = None
 
@@ -103,6 +104,9 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         'dmk_batch_destroy': (None, [vp]),
         'dmk_batch_run': (C.c_int, [vp, C.POINTER(C.POINTER(LoadStepStruct)), ip, C.c_int, C.c_int, BATCH_INCREMENT_CB,
                                     C.c_void_p, ip]),
+        'dmk_autotune': (C.c_int, [vp, C.c_int, dp, ip]),
+        'dmk_get_tuning': (C.c_int, [vp, ip, ip]),
+        'dmk_set_tuning': (C.c_int, [vp, C.c_int, C.c_int]),
         'dmk_destroy': (None, [vp]),
         'dmk_last_error': (C.c_char_p, []),
     }

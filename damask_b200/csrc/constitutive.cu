@@ -243,11 +243,13 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
   append(w.list_out, w.count_out, keep, v);
 }
 
-// one state iteration of every listed voxel: integrateStress (integrateStateFPI:626-629)
-// three blocks per SM up to 24 systems (168 registers, a few spilled; 67 KB of shared memory per
-// block at 24 systems): measured 5 % faster at 256^3 than two blocks without spills
-template <int NS>
-__global__ void __launch_bounds__(pass_threads<NS>(), NS > 24 ? 1 : 3)
+// one state iteration of every listed voxel: integrateStress (integrateStateFPI:626-629).
+// MINB: resident blocks per SM that the register allocation is bounded for (the variants the
+// autotuner chooses from, stress_variant_blocks); three up to 24 systems by default (168 registers,
+// a few spilled; 67 KB of shared memory per block at 24 systems): measured 5 % faster at 256^3 than
+// two blocks without spills
+template <int NS, int MINB>
+__global__ void __launch_bounds__(pass_threads<NS>(), MINB)
 constitutive_stress_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                            const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                            const int* __restrict__ list_in, int64_t n_in) {
@@ -399,18 +401,47 @@ cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& 
   return cudaGetLastError();
 }
 
+// stress kernel variants: up to 24 systems bounded for 3 (default), 2 or 4 resident blocks per SM;
+// 48 systems (64-thread blocks, three fit by shared memory) one variant
+int stress_variant_count(int ns) { return ns > 24 ? 1 : 3; }
+int stress_variant_blocks(int ns, int variant) {
+  if (ns > 24) return 1;
+  static const int blocks[3] = {3, 2, 4};
+  return blocks[variant >= 0 && variant < 3 ? variant : 0];
+}
+
+namespace {
+template <int NS, int MINB>
+cudaError_t launch_stress(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f, const PassWork& w, double dt,
+                          const int* list_in, int64_t n_in, int nb, size_t smem, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem));
+  if (e != cudaSuccess) return e;
+  constitutive_stress_kernel<NS, MINB><<<nb, pass_threads<NS>(), smem, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  return cudaGetLastError();
+}
+}  // namespace
+
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s) {
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s,
+                                     int variant) {
   const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * pass_threads<NS>() * sizeof(double);
   const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
-  cudaError_t e = cudaFuncSetAttribute(constitutive_stress_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       int(smem_s));
-  if (e == cudaSuccess)
-    e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(smem_c));
+  cudaError_t e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       int(smem_c));
   if (e != cudaSuccess) return e;
   const int nb = int((n_in + pass_threads<NS>() - 1) / pass_threads<NS>());
-  constitutive_stress_kernel<NS><<<nb, pass_threads<NS>(), smem_s, s>>>(pc, nm, f, w, dt, list_in, n_in);
+  if constexpr (NS > 24) {
+    e = launch_stress<NS, 1>(pc, nm, f, w, dt, list_in, n_in, nb, smem_s, s);
+  } else {
+    switch (stress_variant_blocks(NS, variant)) {
+      case 2: e = launch_stress<NS, 2>(pc, nm, f, w, dt, list_in, n_in, nb, smem_s, s); break;
+      case 4: e = launch_stress<NS, 4>(pc, nm, f, w, dt, list_in, n_in, nb, smem_s, s); break;
+      default: e = launch_stress<NS, 3>(pc, nm, f, w, dt, list_in, n_in, nb, smem_s, s); break;
+    }
+  }
+  if (e != cudaSuccess) return e;
   constitutive_control_kernel<NS><<<nb, pass_threads<NS>(), smem_c, s>>>(pc, nm, f, w, dt, list_in, n_in);
   return cudaGetLastError();
 }
@@ -507,7 +538,8 @@ cudaError_t build_batch_pass_graph(const PhaseConst<NS>& pc, const Numerics& nm,
                                                      const PassWork&, double, int, int, int64_t, int64_t,          \
                                                      cudaStream_t);                                                 \
   template cudaError_t launch_constitutive_pass<NS>(const PhaseConst<NS>&, const Numerics&, const Fields&,           \
-                                                    const PassWork&, double, const int*, int64_t, cudaStream_t);   \
+                                                    const PassWork&, double, const int*, int64_t, cudaStream_t,    \
+                                                    int);                                                          \
   template cudaError_t build_batch_pass_graph<NS>(const PhaseConst<NS>&, const Numerics&, const BatchTables&,    \
                                                   const BatchPassBuffers&, int, cudaStream_t, cudaGraph_t*);
 DMK_INSTANTIATE(12)

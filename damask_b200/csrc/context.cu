@@ -144,6 +144,7 @@ struct dmk_ctx {
   cudaEvent_t fork = nullptr, join[PASS_CHUNKS] = {};
   int* plist[PASS_CHUNKS][2] = {};
   int nchunks = PASS_CHUNKS;     // chunks in use: fewer for small RVEs (one host sync per chunk and pass)
+  int stress_variant = 0;        // register bound of the stress kernel (stress_variant_blocks); dmk_autotune
   int* pcount = nullptr;         // [2 h + k]: entries appended to plist[h][k]
   int* hcount = nullptr;         // pinned host copies of the current counts of the chunks
   int64_t passes = 0;            // constitutive passes launched (all evaluations)
@@ -247,7 +248,7 @@ int constitutive_passes(dmk_ctx* c, const PhaseConst<NS>& pc, const Fields& f, d
       const int nxt = 1 - cur[h];
       CK(cudaMemsetAsync(c->pcount + 2 * h + nxt, 0, sizeof(int), c->cstream[h]));
       CKL(launch_constitutive_pass<NS>(pc, c->nm, f, pass_work(c, h, nxt), dt, c->plist[h][cur[h]], n,
-                                       c->cstream[h]));
+                                       c->cstream[h], c->stress_variant));
       ++c->launches;                                       // a pass is a stress and a control kernel
       ++c->passes;
       CK(cudaMemcpyAsync(c->hcount + h, c->pcount + 2 * h + nxt, sizeof(int), cudaMemcpyDeviceToHost, c->cstream[h]));
@@ -1120,8 +1121,10 @@ int dmk_mech_init(dmk_ctx** out, const int cells[3], const double geomSize[3], c
     return bail(rc);
   // a chunk of at least 65536 voxels keeps a pass kernel wide enough to be worth its own stream
   c->nchunks = int(std::max<int64_t>(1, std::min<int64_t>(PASS_CHUNKS, N / 65536)));
-  for (int h = 0; h < c->nchunks; ++h) {
-    const size_t len = size_t(N * (h + 1) / c->nchunks - N * h / c->nchunks);
+  // voxel lists for every chunk count (the autotuner and dmk_set_tuning change it): chunk h of K
+  // chunks holds at most ceil(N / K) voxels and exists for K > h, so its lists hold ceil(N / (h + 1))
+  for (int h = 0; h < PASS_CHUNKS; ++h) {
+    const size_t len = size_t((N + h) / (h + 1));
     if ((rc = dalloc(&c->plist[h][0], len)) || (rc = dalloc(&c->plist[h][1], len))) return bail(rc);
   }
   if (cudaMallocHost(reinterpret_cast<void**>(&c->hcount), PASS_CHUNKS * sizeof(int)) != cudaSuccess) {
@@ -2738,3 +2741,115 @@ HostPool* batch_pool(dmk_batch* b) { return b ? b->pool.get() : nullptr; }
 int batch_size(const dmk_batch* b) { return b ? b->n : 0; }
 dmk_ctx* batch_member(dmk_batch* b, int k) { return (b && k >= 0 && k < b->n) ? b->ctx[k] : nullptr; }
 }  // namespace dmk
+
+// ------------------------------------------------------------------ autotuner
+// The constitutive evaluation at the context's current state (its solver F and time step), timed
+// for every stress-kernel variant (register bound for 2, 3 or 4 resident blocks per SM up to 24
+// slip systems) and voxel-chunk count (1, 2, 4); the fastest pair is kept.  The fields an
+// evaluation changes (Fp, Lp, S, Fe, state) are copied to a scratch buffer first and restored after
+// every trial, and the stress buffers are swapped back, so a solve after the tuning runs bit for bit
+// as without it (the variants and chunk counts change the schedule, not the arithmetic).
+
+namespace {
+
+std::vector<std::pair<double*, size_t>> tuning_buffers(dmk_ctx* c) {
+  const size_t N = size_t(c->N), NST = size_t(2 * c->NS);
+  return {{c->Fp, 9 * N}, {c->Lp, 9 * N}, {c->S, 6 * N}, {c->Fe, 9 * N}, {c->state, NST * N}};
+}
+
+int copy_buffers(dmk_ctx* c, double* scratch, bool save) {
+  size_t o = 0;
+  for (const auto& b : tuning_buffers(c)) {
+    CK(cudaMemcpyAsync(save ? scratch + o : b.first, save ? b.first : scratch + o, sizeof(double) * b.second,
+                       cudaMemcpyDeviceToDevice, c->stream));
+    o += b.second;
+  }
+  return 0;
+}
+
+int autotune_impl(dmk_ctx* c, int reps, double* report, int* n_report) {
+  size_t total = 0;
+  for (const auto& b : tuning_buffers(c)) total += b.second;
+  size_t free_b = 0, total_b = 0;
+  CK(cudaMemGetInfo(&free_b, &total_b));
+  if (total * sizeof(double) + (size_t(1) << 30) > free_b)
+    return fail(DMK_ERR_CUDA, "autotune: not enough free device memory for the state copy");
+  double* scratch = nullptr;
+  if (int rc = dalloc(&scratch, total)) return rc;
+  std::unique_ptr<double, void (*)(double*)> guard(scratch, [](double* p) { cudaFree(p); });
+  double* const P0 = c->P;
+  double* const Pn0 = c->Pnew;
+  const bool dot0_valid = c->dot0_valid;
+  const int variant0 = c->stress_variant, chunks0 = c->nchunks;
+  if (int rc = copy_buffers(c, scratch, true)) return rc;
+  const double ms0 = c->last_ms[0];
+  int best_v = variant0, best_k = chunks0, n = 0;
+  double best = 1e300;
+  const int nv = stress_variant_count(c->NS);
+  for (int v = 0; v < nv; ++v)
+    for (int k : {1, 2, 4}) {
+      if (k > PASS_CHUNKS) continue;
+      c->stress_variant = v;
+      c->nchunks = k;
+      double t = 1e300;
+      for (int r = 0; r < std::max(1, reps); ++r) {
+        const double before = c->last_ms[0];
+        int st = 0;
+        if (int rc = evaluate_constitutive(c, c->dt, nullptr, 0, &st)) return rc;
+        t = std::min(t, c->last_ms[0] - before);
+        c->P = P0;
+        c->Pnew = Pn0;
+        if (int rc = copy_buffers(c, scratch, false)) return rc;
+      }
+      if (report && n < 12) {
+        report[3 * n] = stress_variant_blocks(c->NS, v);
+        report[3 * n + 1] = k;
+        report[3 * n + 2] = t;
+      }
+      ++n;
+      if (t < best) {
+        best = t;
+        best_v = v;
+        best_k = k;
+      }
+    }
+  CK(cudaStreamSynchronize(c->stream));
+  c->stress_variant = best_v;
+  c->nchunks = best_k;
+  c->last_ms[0] = ms0;
+  (void)dot0_valid;   // the evaluation stores the increment-start rates the next one would compute
+  if (n_report) *n_report = std::min(n, 12);
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int dmk_autotune(dmk_ctx* c, int reps, double* report, int* n_report) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (c->solver != 0) return fail(DMK_ERR_CONFIG, "the autotuner runs on the basic spectral scheme");
+  CK(cudaSetDevice(c->device));
+  return autotune_impl(c, reps, report, n_report);
+}
+
+int dmk_get_tuning(dmk_ctx* c, int* stress_blocks, int* chunks) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (stress_blocks) *stress_blocks = stress_variant_blocks(c->NS, c->stress_variant);
+  if (chunks) *chunks = c->nchunks;
+  return 0;
+}
+
+int dmk_set_tuning(dmk_ctx* c, int stress_blocks, int chunks) {
+  if (!c) return fail(DMK_ERR_ARG, "null argument");
+  if (chunks < 1 || chunks > PASS_CHUNKS) return fail(DMK_ERR_ARG, "chunks must be 1 to 4");
+  int v = -1;
+  for (int k = 0; k < stress_variant_count(c->NS); ++k)
+    if (stress_variant_blocks(c->NS, k) == stress_blocks) v = k;
+  if (v < 0) return fail(DMK_ERR_ARG, "no stress-kernel variant for that block count");
+  c->stress_variant = v;
+  c->nchunks = chunks;
+  return 0;
+}
+
+}  // extern "C"

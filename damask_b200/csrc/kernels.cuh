@@ -81,9 +81,13 @@ template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                       const PassWork& w, double dt, int apply_update, int use_dot0, int64_t v_begin,
                                       int64_t v_end, cudaStream_t s);
+// variant: the stress kernel's register bound (stress_variant_blocks: resident blocks per SM)
 template <int NS>
 cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
-                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s);
+                                     const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s,
+                                     int variant = 0);
+int stress_variant_count(int ns);
+int stress_variant_blocks(int ns, int variant);
 // Tables of a batch of contexts of one phase (the constitutive passes of all of them in shared
 // launches): items are the voxels of all contexts, context after context.
 struct BatchTables {

@@ -106,6 +106,24 @@ class SpectralBasic:
     def materialpoint_forward(self) -> None:
         _lib.check(self.lib.dmk_materialpoint_forward(self.ctx))
 
+    def autotune(self, reps: int = 2) -> dict:
+        """dmk_autotune: time the constitutive evaluation at the current state for every stress-kernel
+        variant and voxel-chunk count and keep the fastest (results unchanged)."""
+        rep = np.zeros(36)
+        n = C.c_int()
+        _lib.check(self.lib.dmk_autotune(self.ctx, int(reps), _dp(rep), C.byref(n)))
+        return {'candidates': [(int(rep[3 * k]), int(rep[3 * k + 1]), float(rep[3 * k + 2])) for k in range(n.value)],
+                'chosen': self.tuning()}
+
+    def tuning(self) -> tuple[int, int]:
+        """(stress-kernel blocks per SM, voxel chunks) in use."""
+        b, k = C.c_int(), C.c_int()
+        _lib.check(self.lib.dmk_get_tuning(self.ctx, C.byref(b), C.byref(k)))
+        return b.value, k.value
+
+    def set_tuning(self, stress_blocks: int, chunks: int) -> None:
+        _lib.check(self.lib.dmk_set_tuning(self.ctx, int(stress_blocks), int(chunks)))
+
     def update_coords(self) -> None:
         _lib.check(self.lib.dmk_mech_update_coords(self.ctx))
 

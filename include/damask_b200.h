@@ -319,6 +319,18 @@ int dmk_grid_run_ctx(dmk_ctx* ctx, const dmk_loadstep* steps, int n_steps, int N
    denominator of the constitutive update's FP64 roofline. */
 int dmk_fp64_peak(int device, double* tflops);
 
+/* Autotuner (no counterpart in the reference): times the constitutive evaluation at the context's
+   current state (its solver F and time step; call it after dmk_mech_forward, before the solution)
+   for every stress-kernel variant (register bound for 2, 3 or 4 resident blocks per SM up to 24
+   slip systems; one variant at 48) and voxel-chunk count (1, 2, 4), best of `reps` runs each, and
+   keeps the fastest pair.  The fields an evaluation changes are restored after every trial, so the
+   solve continues bit for bit as without tuning.  Needs free device memory for a copy of Fp, Lp, S,
+   Fe and the state (fails with DMK_ERR_CUDA otherwise, leaving the settings).  report (optional, 36
+   doubles): per candidate (blocks per SM, chunks, ms); *n_report candidates.  Basic scheme only. */
+int dmk_autotune(dmk_ctx* ctx, int reps, double* report, int* n_report);
+int dmk_get_tuning(dmk_ctx* ctx, int* stress_blocks, int* chunks);
+int dmk_set_tuning(dmk_ctx* ctx, int stress_blocks, int chunks);
+
 /* Number of kernels of this library launched by the context so far. */
 int dmk_get_launches(dmk_ctx* ctx, int64_t* out);
 /* Device timer on the context's stream: CUDA events recorded at start and stop;
