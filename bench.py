@@ -407,17 +407,17 @@ BATCH_JOBS = 512                         # RVEs of the batched workload definiti
 BATCH_RVES, BATCH_INCREMENTS = 128, 10   # the bounded batched sample of the default bench line
 
 
-def batch_sample(n_rves: int, increments: int, local: int = 0) -> dict:
+def batch_sample(n_rves: int, increments: int, local: int = 0, precision: str = 'mixed') -> dict:
     """The batched workload's first n_rves RVEs (edges 8..32, 5..100 grains, random-axis tension or
-    simple shear), their first `increments` increments, as one batch of the library (FP64) driven by
-    its C++ batched increment loop: updates/s over the wall time of the run (the increment loops
-    included, context set-up not)."""
+    simple shear), their first `increments` increments, as one batch of the library (mixed form, as the
+    workload is specified) driven by its C++ batched increment loop: updates/s over the wall time of the
+    run (the increment loops included, context set-up not)."""
     from damask_b200 import workloads
     from damask_b200.batch import DeviceBatch
     jobs = workloads.batched_jobs(BATCH_JOBS)[:n_rves]
     voxels = sum(j[0].n_cells for j in jobs)
     t0 = time.perf_counter()
-    db = DeviceBatch(jobs, max_increments=increments, device=local)
+    db = DeviceBatch(jobs, max_increments=increments, device=local, precision=precision)
     setup = time.perf_counter() - t0
     clocks = ClockSampler(local)
     clocks.start()
@@ -434,7 +434,8 @@ def batch_sample(n_rves: int, increments: int, local: int = 0) -> dict:
            'value': updates / seconds, 'unit': 'updates/s', 'seconds': seconds, 'setup_seconds': setup,
            'rves': n_rves, 'voxels': voxels, 'increments': incs, 'updates': updates,
            'batched_solutions': st['solutions'], 'graphs': st['graphs'], 'passes': st['passes'],
-           'fixed_point_iterations': st['iterations'], 'dtype': 'f64', 'clocks': clk,
+           'fixed_point_iterations': st['iterations'],
+           'dtype': 'f64 constitutive, f32 spectral (mixed)' if precision == 'mixed' else 'f64', 'clocks': clk,
            'how': 'dmk_batch_run: one dmk_batch_solution per round of solution requests; per fixed-point '
                   'iteration one CUDA graph (constitutive passes of all active RVEs, device-side while loop), '
                   'one cuFFT plan pair per edge size, batched aim / Gamma / convergence / Anderson kernels'}
@@ -456,7 +457,7 @@ def run_batch(args) -> None:
         line = {'metric': 'batched RVE material-point updates/s (wall clock of the increment loops)',
                 'value': b['value'], 'unit': 'updates/s', 'n_gpus': 1, 'steps': b['increments'], 'warmup': 0,
                 'ms_per_step': 1e3 * b['seconds'] / max(1, b['increments']), 'higher_is_better': True,
-                'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f64', 'data': 'synthetic',
+                'scaling': 'weak', 'vs_baseline': None, 'dtype': b['dtype'], 'data': 'synthetic',
                 'config': {'workload': b['workload'], 'rves': args.batch, 'voxels': b['voxels'], 'engine': 'dmk_batch'},
                 'batched': b, 'clocks': b['clocks']}
         print(json.dumps(line, default=_json_default), flush=True)

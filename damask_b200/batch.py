@@ -6,7 +6,7 @@ solution; the solutions of all waiting RVEs are computed together, with the fixe
 of every RVE in shared launches (per iteration one CUDA graph for the constitutive evaluation of
 all active RVEs, one cuFFT plan pair per edge size, batched residual and Anderson kernels).  The
 RVEs never exchange data; every RVE's results are those of a standalone run.  It takes the basic
-scheme in the FP64 form with one phase for all RVEs.
+scheme (FP64 or mixed form) with one phase for all RVEs.
 
 BatchRunner: one context per RVE on its own streams, driven by a pool of host threads (any
 scheme and precision; the library calls release the interpreter lock, so the RVEs' kernel
@@ -82,12 +82,13 @@ class DeviceBatch:
     cut back and so fall out of step with the others; each request is solved at its own job's
     increment and time step."""
 
-    def __init__(self, jobs, max_increments: int | None = None, N_cutback_max: int = 3, device: int = 0):
+    def __init__(self, jobs, max_increments: int | None = None, N_cutback_max: int = 3, device: int = 0,
+                 precision: str = 'fp64'):
         self.jobs = list(jobs)
         self.max_increments = max_increments
         self.lib = _lib.load()
         self.solvers = [SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num,
-                                      precision='fp64', device=device) for rve, phase, _, num in self.jobs]
+                                      precision=precision, device=device) for rve, phase, _, num in self.jobs]
         self.drivers = [IncrementDriver(s, lcs, N_cutback_max) for s, (_, _, lcs, _) in zip(self.solvers, self.jobs)]
         self.results = [[] for _ in self.jobs]
         self.updates = [0] * len(self.jobs)   # material-point updates of the converged (sub)increments

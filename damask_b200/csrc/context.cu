@@ -2242,6 +2242,10 @@ struct dmk_batch {
     double* real = nullptr;
     double* spec = nullptr;
     cufftHandle fwd = 0, bwd = 0;
+    float* real_f = nullptr;       // the mixed form's FP32 buffers and plans (when a member is mixed)
+    float* spec_f = nullptr;
+    cufftHandle fwd_f = 0, bwd_f = 0;
+    bool run32 = false, run64 = false;   // transforms needed in the current spectral pass
   };
   std::vector<Group> groups;
   void* fft_work = nullptr;
@@ -2266,10 +2270,10 @@ void batch_free(dmk_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
   for (auto& g : b->groups) {
-    if (g.fwd) cufftDestroy(g.fwd);
-    if (g.bwd) cufftDestroy(g.bwd);
-    if (g.real) cudaFree(g.real);
-    if (g.spec) cudaFree(g.spec);
+    for (cufftHandle p : {g.fwd, g.bwd, g.fwd_f, g.bwd_f})
+      if (p) cufftDestroy(p);
+    for (void* p : {(void*)g.real, (void*)g.spec, (void*)g.real_f, (void*)g.spec_f})
+      if (p) cudaFree(p);
   }
   for (void* p : {(void*)b->d_tab, (void*)b->d_off, (void*)b->d_ctx_of, (void*)b->d_list[0], (void*)b->d_list[1],
                   (void*)b->d_count, (void*)b->d_status, (void*)b->d_iter, (void*)b->d_bc, (void*)b->d_aa,
@@ -2409,6 +2413,8 @@ int batch_build(dmk_batch* b) {
     it->members.push_back(r);
   }
   size_t work = 0;
+  bool any_mixed = false;
+  for (int r = 0; r < n; ++r) any_mixed |= b->ctx[r]->precision == DMK_PRECISION_MIXED;
   for (auto& g : b->groups) {
     const int m = int(g.members.size());
     const int64_t N = int64_t(g.cells[0]) * g.cells[1] * g.cells[2];
@@ -2426,19 +2432,31 @@ int batch_build(dmk_batch* b) {
     CKF(cufftMakePlanMany(g.fwd, 3, nn, inemb, 1, int(N), onemb, 1, int(plane), CUFFT_D2Z, 9 * m, &w1));
     CKF(cufftMakePlanMany(g.bwd, 3, nn, onemb, 1, int(plane), inemb, 1, int(N), CUFFT_Z2D, 9 * m, &w2));
     work = std::max(work, std::max(w1, w2));
+    if (any_mixed) {
+      if ((rc = dalloc(&g.real_f, size_t(9) * m * N)) || (rc = dalloc(&g.spec_f, size_t(18) * m * plane))) return rc;
+      CKF(cufftCreate(&g.fwd_f));
+      CKF(cufftCreate(&g.bwd_f));
+      CKF(cufftSetAutoAllocation(g.fwd_f, 0));
+      CKF(cufftSetAutoAllocation(g.bwd_f, 0));
+      CKF(cufftMakePlanMany(g.fwd_f, 3, nn, inemb, 1, int(N), onemb, 1, int(plane), CUFFT_R2C, 9 * m, &w1));
+      CKF(cufftMakePlanMany(g.bwd_f, 3, nn, onemb, 1, int(plane), inemb, 1, int(N), CUFFT_C2R, 9 * m, &w2));
+      work = std::max(work, std::max(w1, w2));
+    }
     for (int k = 0; k < m; ++k) {
       BatchCtx& x = b->h_bc[g.members[k]];
       x.fft_real = g.real + size_t(9) * k * N;
       x.fft_spec = g.spec + size_t(18) * k * plane;
+      x.fft_real_f = g.real_f ? g.real_f + size_t(9) * k * N : nullptr;
+      x.fft_spec_f = g.spec_f ? g.spec_f + size_t(18) * k * plane : nullptr;
     }
   }
   if (work) CK(cudaMalloc(&b->fft_work, work));
-  for (auto& g : b->groups) {
-    CKF(cufftSetWorkArea(g.fwd, b->fft_work));
-    CKF(cufftSetWorkArea(g.bwd, b->fft_work));
-    CKF(cufftSetStream(g.fwd, b->stream));
-    CKF(cufftSetStream(g.bwd, b->stream));
-  }
+  for (auto& g : b->groups)
+    for (cufftHandle p : {g.fwd, g.bwd, g.fwd_f, g.bwd_f})
+      if (p) {
+        CKF(cufftSetWorkArea(p, b->fft_work));
+        CKF(cufftSetStream(p, b->stream));
+      }
   // the constitutive evaluation of the batch as a graph over the tables
   BatchTables t;
   t.f = reinterpret_cast<const Fields*>(b->d_tab + b->o_f);
@@ -2474,6 +2492,7 @@ int batch_build(dmk_batch* b) {
 struct BatchSolve {
   int evals = 0, reason = 0, count = 0, new_slot = -1, it = 0, apply = 0, m = 0, snes_max_its = 50, nsl = 0;
   bool anderson = false, first = true, active = false;
+  bool fp32 = false;               // mixed form: the spectral pass runs in FP32 until it first converges
   std::vector<double> G, bvec;
   std::vector<int> slots_b;
 };
@@ -2503,6 +2522,7 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
     S.active = true;
     S.snes_max_its = c->num.snes_max_it > 0 ? c->num.snes_max_it : 50;
     S.anderson = c->num.snes_type == 1;
+    S.fp32 = c->precision == DMK_PRECISION_MIXED;
     S.m = c->aa_m;
     S.G.assign(size_t(S.m > 0 ? S.m : 1) * (S.m > 0 ? S.m : 1), 0.0);
     // the batch's launches follow the context's queued work (forward, solver scalars)
@@ -2527,6 +2547,8 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
       BatchSolve& S = st[r];
       BatchCtx& x = b->h_bc[r];
       x.active = S.active ? 1 : 0;
+      x.mode = S.active ? (S.fp32 ? 1 : 2) : 0;
+      x.count_iter = 1;
       hact[r] = S.active ? 1 : 0;
       if (!S.active) continue;
       ++nact;
@@ -2570,27 +2592,62 @@ int batch_solution_impl(dmk_batch* b, const int* which, int nw, dmk_solution_sta
     CK(cudaGraphLaunch(b->exec, b->stream));
     CK(cudaEventRecord(b->ev[3], b->stream));
     ++b->graph_launches;
-    // residuals: <P> and aim, Gamma convolution per edge group, convergence test, inner products
+    // residuals: <P> and aim, Gamma convolution per edge group (FP32 or FP64 by each context's
+    // mode), convergence test, inner products; the scalars of all contexts read back once
     CK(launch_batch_aim(b->d_bc, n, b->max_nconst, b->stream));
-    CK(launch_batch_gather(b->d_bc, n, b->max_n9, b->stream));
-    for (auto& g : b->groups)
-      CKF(cufftExecD2Z(g.fwd, g.real, reinterpret_cast<cufftDoubleComplex*>(g.spec)));
-    CK(launch_batch_gamma(b->d_bc, n, b->max_nspec, b->stream));
-    for (auto& g : b->groups)
-      CKF(cufftExecZ2D(g.bwd, reinterpret_cast<cufftDoubleComplex*>(g.spec), g.real));
-    CK(launch_batch_scatter(b->d_bc, n, b->max_n9, b->stream));
-    CK(launch_batch_converge(b->d_bc, n, b->d_scal, b->stream));
-    for (int ch = 0; ch < nchunks; ++ch) CK(launch_batch_aa_dots(b->d_bc, n, b->max_aa_blocks, ch, b->stream));
-    CK(cudaMemcpyAsync(b->h_scal, b->d_scal, sizeof(BatchScal) * n, cudaMemcpyDeviceToHost, b->stream));
-    CK(cudaMemcpyAsync(b->h_iter, b->d_iter, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
-    if (nchunks)
-      CK(cudaMemcpyAsync(b->h_dots, b->d_dots, sizeof(double) * n * BATCH_DOTS, cudaMemcpyDeviceToHost, b->stream));
-    CK(cudaStreamSynchronize(b->stream));
+    auto spectral = [&](int nch) -> int {
+      for (auto& g : b->groups) {
+        g.run32 = g.run64 = false;
+        for (int r : g.members) {
+          g.run32 |= b->h_bc[r].mode == 1;
+          g.run64 |= b->h_bc[r].mode == 2;
+        }
+      }
+      CK(launch_batch_gather(b->d_bc, n, b->max_n9, b->stream));
+      for (auto& g : b->groups) {
+        if (g.run32) CKF(cufftExecR2C(g.fwd_f, g.real_f, reinterpret_cast<cufftComplex*>(g.spec_f)));
+        if (g.run64) CKF(cufftExecD2Z(g.fwd, g.real, reinterpret_cast<cufftDoubleComplex*>(g.spec)));
+      }
+      CK(launch_batch_gamma<float>(b->d_bc, n, b->max_nspec, b->stream));
+      CK(launch_batch_gamma<double>(b->d_bc, n, b->max_nspec, b->stream));
+      for (auto& g : b->groups) {
+        if (g.run32) CKF(cufftExecC2R(g.bwd_f, reinterpret_cast<cufftComplex*>(g.spec_f), g.real_f));
+        if (g.run64) CKF(cufftExecZ2D(g.bwd, reinterpret_cast<cufftDoubleComplex*>(g.spec), g.real));
+      }
+      CK(launch_batch_scatter(b->d_bc, n, b->max_n9, b->stream));
+      CK(launch_batch_converge(b->d_bc, n, b->d_scal, b->stream));
+      for (int ch = 0; ch < nch; ++ch) CK(launch_batch_aa_dots(b->d_bc, n, b->max_aa_blocks, ch, b->stream));
+      CK(cudaMemcpyAsync(b->h_scal, b->d_scal, sizeof(BatchScal) * n, cudaMemcpyDeviceToHost, b->stream));
+      CK(cudaMemcpyAsync(b->h_iter, b->d_iter, 2 * sizeof(int), cudaMemcpyDeviceToHost, b->stream));
+      if (nch)
+        CK(cudaMemcpyAsync(b->h_dots, b->d_dots, sizeof(double) * n * BATCH_DOTS, cudaMemcpyDeviceToHost, b->stream));
+      CK(cudaStreamSynchronize(b->stream));
+      return 0;
+    };
+    if (int rc = spectral(nchunks)) return rc;
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, b->ev[2], b->ev[3]));
     b->last_ms[0] += ms;
     b->passes += b->h_iter[0];
     if (b->h_iter[1]) return fail(DMK_ERR_CUDA, "constitutive passes did not terminate");
+    // FP32 passes that meet the tolerance get a correction pass in FP64 on the same stress field;
+    // its residual, decision and inner products replace the FP32 ones (dmk_mech_solution's)
+    int ncorr = 0, nch1 = 0;
+    for (int r = 0; r < n; ++r) {
+      BatchCtx& x = b->h_bc[r];
+      const bool corr = x.mode == 1 && b->h_scal[r].reason == 1;
+      if (corr) {
+        st[r].fp32 = false;
+        ++ncorr;
+        if (x.write_slot >= 0) nch1 = std::max(nch1, (x.nsl + AA_CHUNK - 1) / AA_CHUNK);
+      }
+      x.mode = corr ? 2 : 0;
+      x.count_iter = 0;
+    }
+    if (ncorr) {
+      CK(cudaMemcpyAsync(b->d_bc, b->h_bc, sizeof(BatchCtx) * n, cudaMemcpyHostToDevice, b->stream));
+      if (int rc = spectral(nch1)) return rc;
+    }
     // decisions and Anderson updates
     int naa = 0;
     for (int r = 0; r < n; ++r) {
@@ -2681,7 +2738,6 @@ int dmk_batch_create(dmk_batch** out, dmk_ctx* const* ctxs, int n) {
     const dmk_ctx* c = ctxs[r];
     if (!c) return fail(DMK_ERR_ARG, "null context");
     if (c->solver != 0) return fail(DMK_ERR_CONFIG, "batched solves run the basic scheme");
-    if (c->precision != DMK_PRECISION_FP64) return fail(DMK_ERR_CONFIG, "batched solves run the FP64 form");
     if (c->device != ctxs[0]->device) return fail(DMK_ERR_ARG, "contexts of a batch share one device");
     if (!same_phase(c, ctxs[0])) return fail(DMK_ERR_CONFIG, "contexts of a batch share one phase and its numerics");
     for (int q = 0; q < r; ++q)

@@ -905,21 +905,31 @@ cudaError_t launch_batch_aim(const BatchCtx* t, int n_ctx, int max_nconst, cudaS
 constexpr int BATCH_COPY_BLOCKS = 64;   // blocks per context of the gather and scatter copies
 __global__ void __launch_bounds__(256) batch_gather_kernel(const BatchCtx* __restrict__ t) {
   const BatchCtx& c = t[blockIdx.y];
-  if (!c.active) return;
+  if (c.mode == 0) return;
   const double* __restrict__ src = *c.status == 0 ? c.Pnew : c.P;
-  double* __restrict__ dst = c.fft_real;
   const int64_t n = 9 * c.N;
-  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x)
-    dst[e] = src[e];
+  const int64_t e0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, de = int64_t(gridDim.x) * blockDim.x;
+  if (c.mode == 1) {
+    float* __restrict__ dst = c.fft_real_f;
+    for (int64_t e = e0; e < n; e += de) dst[e] = float(src[e]);
+  } else {
+    double* __restrict__ dst = c.fft_real;
+    for (int64_t e = e0; e < n; e += de) dst[e] = src[e];
+  }
 }
 __global__ void __launch_bounds__(256) batch_scatter_kernel(const BatchCtx* __restrict__ t) {
   const BatchCtx& c = t[blockIdx.y];
-  if (!c.active) return;
-  const double* __restrict__ src = c.fft_real;
+  if (c.mode == 0) return;
   double* __restrict__ dst = c.r;
   const int64_t n = 9 * c.N;
-  for (int64_t e = int64_t(blockIdx.x) * blockDim.x + threadIdx.x; e < n; e += int64_t(gridDim.x) * blockDim.x)
-    dst[e] = src[e];
+  const int64_t e0 = int64_t(blockIdx.x) * blockDim.x + threadIdx.x, de = int64_t(gridDim.x) * blockDim.x;
+  if (c.mode == 1) {
+    const float* __restrict__ src = c.fft_real_f;
+    for (int64_t e = e0; e < n; e += de) dst[e] = double(src[e]);
+  } else {
+    const double* __restrict__ src = c.fft_real;
+    for (int64_t e = e0; e < n; e += de) dst[e] = src[e];
+  }
 }
 cudaError_t launch_batch_gather(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s) {
   if (n_ctx <= 0) return cudaSuccess;
@@ -934,28 +944,32 @@ cudaError_t launch_batch_scatter(const BatchCtx* t, int n_ctx, int64_t max_n9, c
   return cudaGetLastError();
 }
 
+template <typename Real>
 __global__ void __launch_bounds__(SPEC_THREADS) batch_gamma_kernel(const BatchCtx* __restrict__ t) {
   const BatchCtx& c = t[blockIdx.y];
-  if (!c.active || int(blockIdx.x) >= c.nspec) return;
+  if (c.mode != (sizeof(Real) == 4 ? 1 : 2) || int(blockIdx.x) >= c.nspec) return;
   const int64_t plane = int64_t(c.n[0] / 2 + 1) * c.n[1] * c.n[2];
-  double* spec = static_cast<double*>(c.fft_spec);
+  Real* spec = static_cast<Real*>(sizeof(Real) == 4 ? c.fft_spec_f : c.fft_spec);
   if (c.gc.derivative == 2)
-    gamma_div_fwbw_block<double>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
-                                 blockIdx.x);
+    gamma_div_fwbw_block<Real>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
+                               blockIdx.x);
   else
-    gamma_div_block<double>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
-                            blockIdx.x);
+    gamma_div_block<Real>(spec, plane, c.n[0], c.n[1], c.n[2], c.L[0], c.L[1], c.L[2], c.gc, c.sc, c.divp, 1, 1,
+                          blockIdx.x);
 }
+template <typename Real>
 cudaError_t launch_batch_gamma(const BatchCtx* t, int n_ctx, int max_nspec, cudaStream_t s) {
   if (n_ctx <= 0) return cudaSuccess;
-  batch_gamma_kernel<<<dim3(max_nspec, n_ctx), SPEC_THREADS, 0, s>>>(t);
+  batch_gamma_kernel<Real><<<dim3(max_nspec, n_ctx), SPEC_THREADS, 0, s>>>(t);
   return cudaGetLastError();
 }
+template cudaError_t launch_batch_gamma<double>(const BatchCtx*, int, int, cudaStream_t);
+template cudaError_t launch_batch_gamma<float>(const BatchCtx*, int, int, cudaStream_t);
 
 __global__ void batch_converge_kernel(const BatchCtx* __restrict__ t, BatchScal* __restrict__ out) {
   const BatchCtx& c = t[blockIdx.x];
-  if (!c.active) return;
-  converge_body(c.sc, c.divp, c.nspec, c.wgt, c.status, c.nm2, 1);
+  if (c.mode == 0) return;
+  converge_body(c.sc, c.divp, c.nspec, c.wgt, c.status, c.nm2, c.count_iter);
   if (threadIdx.x != 0) return;
   BatchScal& o = out[blockIdx.x];
   const SolverScalars* sc = c.sc;
@@ -977,7 +991,7 @@ cudaError_t launch_batch_converge(const BatchCtx* t, int n_ctx, BatchScal* out, 
 
 __global__ void __launch_bounds__(256) batch_aa_dots_kernel(const BatchCtx* __restrict__ t, int chunk) {
   const BatchCtx& c = t[blockIdx.y];
-  if (!c.active || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl || int(blockIdx.x) >= c.aa_blocks) return;
+  if (c.mode == 0 || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl || int(blockIdx.x) >= c.aa_blocks) return;
   AASlots sl;
   sl.n = min(AA_CHUNK, c.nsl - chunk * AA_CHUNK);
 #pragma unroll
@@ -986,7 +1000,7 @@ __global__ void __launch_bounds__(256) batch_aa_dots_kernel(const BatchCtx* __re
 }
 __global__ void __launch_bounds__(256) batch_aa_reduce_kernel(const BatchCtx* __restrict__ t, int chunk) {
   const BatchCtx& c = t[blockIdx.x];
-  if (!c.active || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl) return;
+  if (c.mode == 0 || c.write_slot < 0 || chunk * AA_CHUNK >= c.nsl) return;
   aa_reduce_body(c.aa_partials, c.aa_blocks, c.aa_out + chunk * 2 * AA_CHUNK);
 }
 cudaError_t launch_batch_aa_dots(const BatchCtx* t, int n_ctx, int max_blocks, int chunk, cudaStream_t s) {

@@ -201,12 +201,16 @@ struct BatchCtx {
   double* aa_out;           // per chunk: 2 AA_CHUNK sums (g then b)
   double* fft_real;         // the context's 9 planes in its edge group's real buffer
   void* fft_spec;           // the context's 9 spectra in the group's spectrum buffer
+  float* fft_real_f;        // the same in FP32 (mixed form), or null
+  void* fft_spec_f;
   int64_t N;
   double wgt;
   double L[3];
   int n[3];
   int nconst, nspec, aa_blocks;
-  int active;               // evaluated in this fixed-point iteration
+  int active;               // evaluated in this fixed-point iteration (<P>, aim)
+  int mode;                 // its spectral pass now: 0 none, 1 FP32, 2 FP64
+  int count_iter;           // the convergence test counts an iteration (not in an FP64 correction pass)
   int write_slot;           // Anderson: slot of the new dR, -1 for none
   int nsl;                  // Anderson: history slots of the inner products (oldest -> newest)
   int slots[AA_MAX];
@@ -224,9 +228,11 @@ struct BatchScal {          // solver scalars of one context, read back after ea
 };
 // <P> of the committed stress and the aim update (sum9 + aim)
 cudaError_t launch_batch_aim(const BatchCtx* t, int n_ctx, int max_nconst, cudaStream_t s);
-// committed stress -> the group's real buffers (before the forward transforms)
+// committed stress -> the group's real buffers, FP32 or FP64 by each context's mode
 cudaError_t launch_batch_gather(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s);
-// Gamma convolution and divergence partial sums on the group spectra (FP64)
+// Gamma convolution and divergence partial sums on the group spectra of the contexts in mode 1
+// (Real = float) or 2 (double)
+template <typename Real>
 cudaError_t launch_batch_gamma(const BatchCtx* t, int n_ctx, int max_nspec, cudaStream_t s);
 // the group's real buffers (after the inverse transforms) -> residual fields
 cudaError_t launch_batch_scatter(const BatchCtx* t, int n_ctx, int64_t max_n9, cudaStream_t s);

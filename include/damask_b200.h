@@ -378,8 +378,9 @@ int dmk_adj_finish(dmk_ctx* ctx, double theta_bar[20]);
 int dmk_adj_local_jacobian(const dmk_phase* phase, double dt, const double* point, double* D);
 
 /* Batches of independent RVEs (no counterpart in the reference, which solves one grid per
-   process).  A batch takes contexts of one phase and one set of constitutive numerics, basic scheme,
-   FP64 form, on one device, and solves one increment of any subset of them together:
+   process).  A batch takes contexts of one phase and one set of constitutive numerics, basic scheme
+   (FP64 or mixed form, per context), on one device, and solves one increment of any subset of them
+   together:
    dmk_batch_solution does what dmk_mech_solution does for each listed context, with the
    iterations of all of them in shared launches (per fixed-point iteration one CUDA graph for the
    constitutive evaluation of every active context, one cuFFT plan pair per edge size, batched

@@ -147,3 +147,34 @@ def test_device_batch_cutbacks_match_standalone(gpu):
         db.close()
     for s, _ in refs:
         s.close()
+
+
+@pytest.mark.gpu
+def test_device_batch_mixed_form(gpu):
+    """The mixed form in a batch: FP32 spectral passes (cuFFT R2C/C2R plans per edge size) with the
+    FP64 correction pass of dmk_mech_solution for the members whose FP32 pass meets the tolerance.
+    Against standalone mixed runs: equal fixed-point iteration counts and <P> within 1e-6 (the FP32
+    transforms of the batched plans round differently from the per-RVE ones); against the batch's
+    FP64 form: <P> within 1e-5, the mixed form's bound."""
+    from damask_b200.batch import DeviceBatch
+    from damask_b200.grid import SpectralBasic, run_load_cases
+    jobs = workloads.batched_jobs(6, seed=5)
+    n = 3
+    mixed = DeviceBatch(jobs, max_increments=n, precision='mixed')
+    mixed.run_native()
+    fp64 = DeviceBatch(jobs, max_increments=n)
+    fp64.run_native()
+    worst = 0.0
+    for k, (rve, phase, lcs, num) in enumerate(jobs):
+        s = SpectralBasic(rve.cells, rve.size, rve.material, rve.quaternions, phase, num, precision='mixed')
+        ref = run_load_cases(s, lcs, max_increments=n)
+        got = mixed.results[k]
+        assert [r.iterations for r in got] == [r.iterations for r in ref], k
+        for a, b, c in zip(got, ref, fp64.results[k]):
+            assert rel(a.P_av, b.P_av) < 1e-6, (k, a.inc)
+            worst = max(worst, rel(a.P_av, c.P_av))
+        s.close()
+    assert worst < 1e-5
+    print(f'mixed batch vs FP64 batch: <P> within {worst:.2e}')
+    mixed.close()
+    fp64.close()
