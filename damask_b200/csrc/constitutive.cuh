@@ -319,7 +319,7 @@ __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double
 }
 
 // Slots of the stress kernel (stride pass_threads<NS>()): 1/xi [0, NS), Newton weights
-// [NS, 2NS), |dot_gamma| [2NS, 3NS), Newton 3x3 scratch [3NS, 3NS + 27).
+// [NS, 2NS), A = F Fp0^-1 [2NS, 2NS + 9).
 template <int NS>
 __host__ __device__ constexpr int stress_slots() { return 2 * NS + 9; }
 
