@@ -234,9 +234,12 @@ constitutive_begin_kernel(const __grid_constant__ PhaseConst<NS> pc, const __gri
                           const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                           int apply_update, int use_dot0, int64_t v_begin, int64_t v_end) {
   extern __shared__ double slots[];
-  double* hs = slots;
-  double* xs = slots + NS * NS + threadIdx.x;
-  stage_hardening<NS>(pc, hs);
+  const double* hs = pc.hmat;
+  double* xs = slots + hard_smem_doubles<NS>() + threadIdx.x;
+  if constexpr (hard_smem_doubles<NS>() > 0) {
+    stage_hardening<NS>(pc, slots);
+    hs = slots;
+  }
   __syncthreads();
   const int64_t v = v_begin + int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   const bool keep = v < v_end && begin_voxel<NS>(pc, hs, xs, nm, f, w, v, dt, apply_update, use_dot0);
@@ -272,9 +275,12 @@ constitutive_control_kernel(const __grid_constant__ PhaseConst<NS> pc, const __g
                             const __grid_constant__ Fields f, const __grid_constant__ PassWork w, double dt,
                             const int* __restrict__ list_in, int64_t n_in) {
   extern __shared__ double slots[];
-  double* hs = slots;
-  double* xs = slots + NS * NS + threadIdx.x;
-  stage_hardening<NS>(pc, hs);
+  const double* hs = pc.hmat;
+  double* xs = slots + hard_smem_doubles<NS>() + threadIdx.x;
+  if constexpr (hard_smem_doubles<NS>() > 0) {
+    stage_hardening<NS>(pc, slots);
+    hs = slots;
+  }
   __syncthreads();
   const int64_t idx = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   int64_t v = 0;
@@ -298,9 +304,12 @@ __global__ void __launch_bounds__(pass_threads<NS>(), 4)
 constitutive_begin_batch_kernel(const __grid_constant__ PhaseConst<NS> pc, const __grid_constant__ Numerics nm,
                                 const __grid_constant__ BatchTables t, int* list_out, int* count_out) {
   extern __shared__ double slots[];
-  double* hs = slots;
-  double* xs = slots + NS * NS + threadIdx.x;
-  stage_hardening<NS>(pc, hs);
+  const double* hs = pc.hmat;
+  double* xs = slots + hard_smem_doubles<NS>() + threadIdx.x;
+  if constexpr (hard_smem_doubles<NS>() > 0) {
+    stage_hardening<NS>(pc, slots);
+    hs = slots;
+  }
   __syncthreads();
   const int64_t g = int64_t(blockIdx.x) * blockDim.x + threadIdx.x;
   bool keep = false;
@@ -346,9 +355,12 @@ constitutive_control_batch_kernel(const __grid_constant__ PhaseConst<NS> pc, con
   const int64_t first = int64_t(blockIdx.x) * blockDim.x;
   if (first >= n_in) return;
   extern __shared__ double slots[];
-  double* hs = slots;
-  double* xs = slots + NS * NS + threadIdx.x;
-  stage_hardening<NS>(pc, hs);
+  const double* hs = pc.hmat;
+  double* xs = slots + hard_smem_doubles<NS>() + threadIdx.x;
+  if constexpr (hard_smem_doubles<NS>() > 0) {
+    stage_hardening<NS>(pc, slots);
+    hs = slots;
+  }
   __syncthreads();
   for (int64_t base = first; base < n_in; base += int64_t(gridDim.x) * blockDim.x) {
     const int64_t idx = base + threadIdx.x;
@@ -390,7 +402,7 @@ template <int NS>
 cudaError_t launch_constitutive_begin(const PhaseConst<NS>& pc, const Numerics& nm, const Fields& f,
                                       const PassWork& w, double dt, int apply_update, int use_dot0, int64_t v_begin,
                                       int64_t v_end, cudaStream_t s) {
-  const size_t smem = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
+  const size_t smem = (hard_smem_doubles<NS>() + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem));
   if (e != cudaSuccess) return e;
@@ -427,7 +439,7 @@ cudaError_t launch_constitutive_pass(const PhaseConst<NS>& pc, const Numerics& n
                                      const PassWork& w, double dt, const int* list_in, int64_t n_in, cudaStream_t s,
                                      int variant) {
   const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * pass_threads<NS>() * sizeof(double);
-  const size_t smem_c = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
+  const size_t smem_c = (hard_smem_doubles<NS>() + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   cudaError_t e = cudaFuncSetAttribute(constitutive_control_kernel<NS>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        int(smem_c));
   if (e != cudaSuccess) return e;
@@ -463,7 +475,7 @@ int resident_blocks(const void* fn, size_t smem, int nsm, int64_t n_items) {
 template <int NS>
 cudaError_t build_batch_pass_graph(const PhaseConst<NS>& pc, const Numerics& nm, const BatchTables& t,
                                    const BatchPassBuffers& b, int nsm, cudaStream_t s, cudaGraph_t* out) {
-  const size_t smem_b = (size_t(NS) * NS + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
+  const size_t smem_b = (hard_smem_doubles<NS>() + size_t(2 * NS) * pass_threads<NS>()) * sizeof(double);
   const size_t smem_s = size_t(NS) * sizeof(SysConst) + size_t(stress_slots<NS>()) * pass_threads<NS>() * sizeof(double);
   const size_t smem_c = smem_b;
   cudaError_t e = cudaFuncSetAttribute(constitutive_begin_batch_kernel<NS>,

@@ -313,6 +313,12 @@ __device__ int integrate_stress(const PhaseConst<NS>& pc, const SysConst* __rest
 
 // Hardening matrix staged in shared memory once per block (row = reacting system),
 // read with uniform addresses (broadcast) in the control kernels.
+// doubles of shared memory for the hardening matrix: staged up to 24 systems; at 48 (18 KB) the
+// control and begin kernels read it from device memory (uniform addresses, L1 resident), so that
+// four 64-thread blocks fit per SM instead of three
+template <int NS>
+__host__ __device__ constexpr size_t hard_smem_doubles() { return NS <= 24 ? size_t(NS) * NS : 0; }
+
 template <int NS>
 __device__ __forceinline__ void stage_hardening(const PhaseConst<NS>& pc, double* hs) {
   for (int i = threadIdx.x; i < NS * NS; i += blockDim.x) hs[i] = pc.hmat[i];
