@@ -650,6 +650,7 @@ def main():
                          'mixed_over_fp64': b48['mixed_over_fp64'], 'P_av_rel_err': b48['P_av_rel_err'],
                          'increments_timed': f'{BCC48_WARMUP + 1}..{BCC48_WARMUP + BCC48_STEPS}',
                          's_per_increment': b48['s_per_increment'], 'roofline_fp64': b48['roofline']['fp64'],
+                         'traffic': b48['roofline']['traffic'], 'traffic_source': b48['roofline']['traffic_source'],
                          'clocks': b48['mixed']['clocks'], 'tuning': b48['mixed'].get('tuning')}
     if batched is not None:
         line['batched'] = batched
