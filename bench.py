@@ -46,10 +46,11 @@ def constitutive_flops(ns: int, newton: float, state: float, updates: float) -> 
 
 
 # DRAM bytes that one stress and one control launch move per voxel of a full pass, by slip-system
-# count, from the ncu capture summarised in profiles/constitutive_passes_64cubed_bcc24.txt (two
-# passes of a 65 536-voxel chunk: stress 568 B, control 2 114 B); a material-point update runs one
-# such pass per state iteration
-TRAFFIC_BYTES_PER_PASS = {24: 2682}
+# count, from the ncu captures summarised in profiles/constitutive_passes_64cubed_bcc24.txt and
+# _bcc48.txt (two passes of a 65 536-voxel chunk each; 24 systems: stress 568 B, control 2 114 B;
+# 48 systems: stress 794 B, control 4 840 B); a material-point update runs one such pass per state
+# iteration
+TRAFFIC_BYTES_PER_PASS = {24: 2682, 48: 5634}
 
 # the 48-system RVE's window inside the default bench line (5.7 s per increment at 256^3)
 BCC48_WARMUP, BCC48_STEPS = 3, 3
